@@ -1,0 +1,342 @@
+"""Benchmark: bidirectional path tracing paths/s on one B200.
+
+Workload (the configuration the headline metric is quoted on): the 4-space
+Cornell box with a 3-sphere hull mesh (20,000 points on S^3, ~135k
+3-simplex facets), a rotated 4-parallelotope and one 3-parallelotope light,
+64-bin spectral colour, a 64x64x64 voxel screen, 16 requested samples per
+voxel (27 rendered: the stratified sampler rounds up to 3^3), maximum path
+depth 6.  Inputs are synthetic, generated from fixed seeds
+(math_b200/scenes.py).
+
+One step is one painter pass: every voxel's 27 paths traced, connected and
+folded into the pixel estimator (7,077,888 paths).  `value` is paths/s over
+the timed steps on the device (CUDA events on the painter's stream, L2
+flushed between steps), `e2e` the same through the C ABI with the image read
+back to host memory every step.  `--impl reference` runs the reference's own
+CPU painter (compiled from its sources, oracle/_ref) on this machine's host
+cores on a bounded slab of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = {"scene": "cornell4d", "screen": [64, 64, 64], "spp": 16, "max_depth": 6,
+            "points": 20000, "color": "spectrum64"}
+REFERENCE_SLAB = [64, 64, 4]  # bounded sample of the same scene for the CPU painter
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="nbpt", choices=["nbpt", "reference"])
+    p.add_argument("--precision", default="float", choices=["float", "double"])
+    p.add_argument("--small", action="store_true", help="a small configuration for smoke runs")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def scene_desc(small: bool):
+    from math_b200 import scenes
+
+    if small:
+        return scenes.cornell_4d(size=(16, 16, 16), points=2000)
+    return scenes.cornell_4d(size=tuple(WORKLOAD["screen"]), points=WORKLOAD["points"])
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+
+        def read():
+            for line in self.proc.stdout:
+                self.rows.append([x.strip() for x in line.split(",")])
+
+        self.thread = threading.Thread(target=read, daemon=True)
+        self.thread.start()
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) < 9:
+                continue
+            for name, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(small: bool, seconds_hint: float = 20.0) -> dict:
+    """The reference's own painter (create_painter, BPT, float, spectrum),
+    unmodified, on the host cores: one pass over a bounded slab of the
+    workload's screen."""
+    from math_b200 import scenes
+    from oracle import oracle
+
+    if not oracle.available():
+        return {"value": None, "unit": "paths/s", "cores": 0, "kind": "reference",
+                "sample": "oracle library not built"}
+    slab = [16, 16, 2] if small else REFERENCE_SLAB
+    desc = scenes.cornell_4d(size=tuple(slab), points=2000 if small else WORKLOAD["points"])
+    # the same camera as the full screen: the slab is the centre of the
+    # full screen's first two axes at full resolution, a few voxels thick
+    s = oracle.Scene(desc, "float", True)
+    cores = os.cpu_count() or 1
+    stats, _ = s.paint(WORKLOAD["spp"], WORKLOAD["max_depth"], passes=1, threads=cores)
+    value = stats["sample_count"] / stats["pass_duration"]
+    return {"value": value, "unit": "paths/s", "cores": cores, "kind": "reference",
+            "sample": (f"one pass of the reference painter over a {slab[0]}x{slab[1]}x{slab[2]} slab "
+                       f"({stats['sample_count']} paths, {stats['pass_duration']:.2f} s, "
+                       f"ray_count {stats['ray_count']})")}
+
+
+def record_bytes(n: int, precision: str) -> dict:
+    t = 8 if precision == "double" else 4
+    return {"node": 2 * n * t + 8, "facet": n * (n + 1) * t + 4, "shape": n * (n + 1) * t}
+
+
+def run_reference(args, rank: int):
+    if rank != 0:
+        return
+    from math_b200 import scenes
+    from oracle import oracle
+
+    if not oracle.available():
+        print(json.dumps({"impl": "reference", "unavailable": "the reference painter (oracle/_ref) is not built"}))
+        return
+    # --steps timed passes of the bounded slab (warm-up passes untimed)
+
+    slab = [16, 16, 2] if args.small else REFERENCE_SLAB
+    desc = scenes.cornell_4d(size=tuple(slab), points=2000 if args.small else WORKLOAD["points"])
+    s = oracle.Scene(desc, "float", True)
+    cores = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        s.paint(WORKLOAD["spp"], WORKLOAD["max_depth"], passes=1, threads=cores)
+    samples = 0
+    seconds = 0.0
+    for _ in range(args.steps):
+        st, _ = s.paint(WORKLOAD["spp"], WORKLOAD["max_depth"], passes=1, threads=cores)
+        samples += st["sample_count"]
+        seconds += st["pass_duration"]
+    value = samples / seconds
+    sample = f"{args.steps} passes of a {slab[0]}x{slab[1]}x{slab[2]} slab of the workload"
+    print(json.dumps({
+        "metric": "bpt_paths_per_second", "value": value, "unit": "paths/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * seconds / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
+        "config": {"workload": "cornell4d 4-space Cornell box, hull of 20000 points on S^3, spectrum64, "
+                               "16 spp (27 rendered), depth 6", "screen": slab, "precision": "float"},
+        "cpu_baseline": {"value": value, "unit": "paths/s", "cores": cores, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def run_nbpt(args, rank: int, world: int, local: int):
+    import torch
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from math_b200 import painter as P
+
+    desc = scene_desc(args.small)
+    spectrum = True
+    t0 = time.perf_counter()
+    scene = P.Scene(desc, args.precision, spectrum)
+    build_s = time.perf_counter() - t0
+    # every rank renders its own pass sequence of the whole screen
+    # (independent samples: weak scaling, no data-path collective)
+    painter = scene.painter(WORKLOAD["spp"], WORKLOAD["max_depth"], seed=1 + rank)
+    stream = torch.cuda.ExternalStream(painter_stream(painter))
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    for _ in range(args.warmup):
+        painter.run(1)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    # device-timed steps: events on the painter's stream around each pass,
+    # L2 flushed between passes (outside the events)
+    step_ms = []
+    paths_s = 0.0
+    nodes = facets = shapes = rays = 0
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        painter.enqueue(1)
+        end.record(stream)
+        painter.wait()
+        step_ms.append(start.elapsed_time(end))
+        st = painter.statistics()
+        paths_s += st["paths_seconds"]
+        nodes += st["nodes"]
+        facets += st["facets"]
+        shapes += st["shapes"]
+        rays += st["ray_count"]
+    torch.cuda.synchronize()
+    clock_info = clocks.stop()
+
+    paths_per_step = scene.pixels * painter.spp
+    ms = float(np.sum(step_ms))
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * paths_per_step * args.steps / (ms / 1000)
+
+    # end to end through the C ABI: pass + image read back to host memory
+    rgb = np.zeros((scene.pixels, 3), np.float32)
+    rgba = np.zeros((scene.pixels, 4), np.float32)
+    torch.cuda.synchronize()
+    e0 = time.perf_counter()
+    for _ in range(args.steps):
+        painter.run(1)
+        P._check(P.lib().nbpt_painter_images(painter.h, P._p(rgb, P._F), P._p(rgba, P._F)))
+    e2e_s = time.perf_counter() - e0
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = world * paths_per_step * args.steps / e2e_s
+
+    # whole job: scene from host arrays (upload, BVH build, facet setup),
+    # one pass, image read back
+    j0 = time.perf_counter()
+    job_scene = P.Scene(desc, args.precision, spectrum)
+    job = job_scene.painter(WORKLOAD["spp"], WORKLOAD["max_depth"], seed=99)
+    job.run(1)
+    job.images()
+    job_s = time.perf_counter() - j0
+    del job, job_scene
+
+    sizes = record_bytes(desc["n"], args.precision)
+    algorithmic = nodes * sizes["node"] + facets * sizes["facet"] + shapes * sizes["shape"]
+    achieved = algorithmic / paths_s / 1e9 if paths_s > 0 else None
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except (OSError, ValueError):
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": None,
+                "kernel": "paths_kernel",
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                "algorithmic_bytes_per_path": algorithmic / (paths_per_step * args.steps),
+                "node_visits_per_path": nodes / (paths_per_step * args.steps),
+                "facet_tests_per_path": facets / (paths_per_step * args.steps),
+                "rays_per_path": rays / (paths_per_step * args.steps),
+                "paths_kernel_share": paths_s / (ms / 1000) if ms > 0 else None}
+
+    if rank == 0:
+        cpu = None if args.no_cpu_baseline else cpu_baseline(args.small)
+        line = {
+            "metric": "bpt_paths_per_second", "value": value, "unit": "paths/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.precision == "float" else "f64",
+            "data": "synthetic (seeded generators)",
+            "config": {"workload": "cornell4d 4-space Cornell box, hull of 20000 points on S^3 "
+                                   f"({scene.pixels} voxels), spectrum64, 16 spp ({painter.spp} rendered), "
+                                   "depth 6", "screen": desc["projector"]["size"],
+                       "paths_per_step": paths_per_step, "precision": args.precision,
+                       "l2": "flushed (256 MiB write) between timed steps",
+                       "scene_build_s": build_s},
+            "e2e": {"value": e2e, "unit": "paths/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": int(rgb.nbytes + rgba.nbytes),
+                    "note": "scene resident on the device; each step one pass through the C ABI plus the "
+                            "image read back to host memory"},
+            "e2e_job": {"seconds": job_s, "paths": paths_per_step,
+                        "note": "scene built from host arrays (upload, BVH, facet setup), one pass, image read back"},
+            "gpu_launches": 3 * args.steps,
+            "roofline": roofline,
+            "clocks": clock_info,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def painter_stream(painter) -> int:
+    from math_b200 import painter as P
+
+    return P.painter_stream(painter)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    run_nbpt(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,210 @@
+/*
+ * nbpt: C ABI of the B200 n-dimensional bidirectional path tracer.
+ *
+ * This is the drop-in boundary for the CPU painter of cppd/math: it replaces
+ * the render path behind the reference's painter API
+ *   create_painter(Integrator::BPT, notifier, samples_per_pixel,
+ *                  max_pass_count, scene, thread_count, flat_shading)
+ *   (src/painter/painter.h:149-157, src/painter/painter.cpp:139-151)
+ * and the scene factories it renders
+ *   scenes::create_storage_scene      (src/painter/scenes/storage.h:40-47)
+ *   shapes::HyperplaneParallelotope   (src/painter/shapes/hyperplane_parallelotope.h:66-77)
+ *   shapes::Parallelotope             (src/painter/shapes/parallelotope.h:65-71)
+ *   shapes::create_mesh               (src/painter/shapes/mesh.h:32-37)
+ *   lights::ParallelotopeLight        (src/painter/lights/parallelotope_light.h:73-83)
+ *   lights::BallLight                 (src/painter/lights/ball_light.h:76-90)
+ *   projectors::PerspectiveProjector  (src/painter/projectors/perspective_projector.h)
+ *   projectors::ParallelProjector     (src/painter/projectors/parallel_projector.h)
+ * The reference's Scene interface exposes no geometry (src/painter/objects.h:330-359),
+ * so a drop-in re-implements the factories: every scene object is described
+ * through the calls below and rendered on the GPU.
+ *
+ * Conventions: plain pointers and sizes; vectors are arrays of `dimension`
+ * doubles; arrays of vectors are row-major.  Functions return 0 (or a
+ * non-negative index) on success and a negative status on error, with the
+ * message in nbpt_last_error() (thread-local).  No exception crosses the ABI.
+ * Objects are not thread-safe; use one object from one thread at a time.
+ */
+#ifndef NBPT_H
+#define NBPT_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct nbpt_scene nbpt_scene;
+typedef struct nbpt_painter nbpt_painter;
+
+enum nbpt_status
+{
+        NBPT_OK = 0,
+        NBPT_ERROR = -1,        /* invalid argument or state, see nbpt_last_error() */
+        NBPT_CUDA_ERROR = -2,   /* CUDA runtime error, see nbpt_last_error() */
+        NBPT_NO_DEVICE = -3     /* no usable GPU */
+};
+
+enum nbpt_precision
+{
+        NBPT_FLOAT = 0, /* geometry, pdfs and MIS in float (the reference's float instantiation) */
+        NBPT_DOUBLE = 1 /* geometry, pdfs and MIS in double */
+};
+
+enum nbpt_color
+{
+        NBPT_RGB = 0,     /* color::Color = RGB<float> */
+        NBPT_SPECTRUM = 1 /* color::Spectrum = 64 samples over 380-720 nm */
+};
+
+/* Statistics of the painter, as painter::Statistics (src/painter/painter.h:120-132)
+ * plus counters of the last pass for the roofline. */
+typedef struct nbpt_statistics
+{
+        long long pass_number;
+        long long pixel_count;
+        long long ray_count;    /* scene queries of the last pass */
+        long long sample_count; /* paths of the last pass (actual samples) */
+        double previous_pass_duration; /* seconds, device time of the last pass */
+        double paths_seconds;          /* device time of the path kernel, last pass */
+        unsigned long long nodes;      /* BVH nodes visited, last pass */
+        unsigned long long facets;     /* facet records tested, last pass */
+        unsigned long long shapes;     /* other shapes tested, last pass */
+} nbpt_statistics;
+
+const char* nbpt_last_error(void);
+int nbpt_device_count(void);
+
+/* ---- scene (scenes::create_storage_scene and the shape/light/projector factories) ---- */
+
+nbpt_scene* nbpt_scene_create(int dimension, int precision, int color);
+void nbpt_scene_destroy(nbpt_scene* scene);
+
+/* shapes::HyperplaneParallelotope(metalness, roughness, color, alpha, org, vectors[N-1]);
+ * returns the shape index. */
+int nbpt_scene_add_hyperplane_parallelotope(
+        nbpt_scene* scene, double metalness, double roughness, const float* rgb, double alpha,
+        const double* org, const double* vectors);
+
+/* shapes::Parallelotope(metalness, roughness, color, alpha, org, vectors[N]) */
+int nbpt_scene_add_parallelotope(
+        nbpt_scene* scene, double metalness, double roughness, const float* rgb, double alpha,
+        const double* org, const double* vectors);
+
+/* One model::mesh::MeshObject<N> of a mesh shape: points [point_count][N],
+ * simplex facets [facet_count][N] (vertex indices), the (N+1)x(N+1)
+ * object matrix, optional per-point normals (NULL: computed as
+ * model::mesh::create_mesh_for_facets does), and the object's material.
+ * Objects accumulate until nbpt_scene_add_mesh(). */
+int nbpt_scene_add_mesh_object(
+        nbpt_scene* scene, const float* points, long long point_count, const int* facets, long long facet_count,
+        const double* matrix, const float* normals, float metalness, float roughness, const float* rgb, float alpha);
+
+/* shapes::create_mesh(mesh_objects, no clip plane, ...): one mesh shape from
+ * the accumulated objects; returns the shape index. */
+int nbpt_scene_add_mesh(nbpt_scene* scene);
+
+/* A mesh shape given as the painter's mesh data (src/painter/shapes/mesh/data.h:34-50):
+ * transformed vertices and normals [vertex_count][N] (normals may be NULL),
+ * facets [facet_count][N], facet_materials [facet_count],
+ * material_params [material_count][3] = (metalness, roughness, alpha),
+ * material_colors [material_count][channels]. */
+int nbpt_scene_add_mesh_data(
+        nbpt_scene* scene, long long vertex_count, const double* vertices, const double* normals,
+        long long facet_count, const int* facets, const int* facet_materials, int material_count,
+        const double* material_params, const float* material_colors);
+
+/* lights::ParallelotopeLight on the hyperplane parallelotope `shape`
+ * (hyperplane_parallelotope().set_light_source); returns the light index. */
+int nbpt_scene_add_parallelotope_light(nbpt_scene* scene, int shape, const double* direction, const float* rgb);
+
+/* lights::BallLight(center, direction, radius, radiance) */
+int nbpt_scene_add_ball_light(
+        nbpt_scene* scene, const double* center, const double* direction, double radius, const float* rgb);
+
+/* projectors::PerspectiveProjector(org, dir, screen_axes[N-1], width_view_angle_degrees, screen_size[N-1]) */
+int nbpt_scene_set_perspective_projector(
+        nbpt_scene* scene, const double* org, const double* dir, const double* axes, double fov_degrees,
+        const int* size);
+
+/* projectors::ParallelProjector(org, dir, screen_axes[N-1], units_per_pixel, screen_size[N-1]) */
+int nbpt_scene_set_parallel_projector(
+        nbpt_scene* scene, const double* org, const double* dir, const double* axes, double units_per_pixel,
+        const int* size);
+
+/* background colour (only black is supported) */
+int nbpt_scene_set_background(nbpt_scene* scene, const float* rgb);
+
+/* Builds the acceleration structures and uploads the scene to the GPU. */
+int nbpt_scene_finalize(nbpt_scene* scene);
+
+long long nbpt_scene_pixel_count(const nbpt_scene* scene);
+/* samples per pixel actually rendered: spp rounded up to a power of the screen dimension */
+int nbpt_scene_actual_spp(const nbpt_scene* scene, int samples_per_pixel);
+long long nbpt_scene_device_bytes(const nbpt_scene* scene);
+
+/* ---- painter (painter::create_painter with Integrator::BPT) ---- */
+
+/* A render of a finalized scene.  Every pass renders samples_per_pixel
+ * stratified samples per pixel with per-path random streams derived from
+ * (seed, pass, pixel, sample) and accumulates the filtered, trimmed pixel
+ * estimator.  max_depth is the reference's MAX_DEPTH (1..8). */
+nbpt_painter* nbpt_painter_create(nbpt_scene* scene, int samples_per_pixel, int max_depth, unsigned seed);
+void nbpt_painter_destroy(nbpt_painter* painter);
+/* enqueues `passes` passes on the painter's CUDA stream and returns */
+int nbpt_painter_enqueue(nbpt_painter* painter, int passes);
+/* waits for the enqueued passes and updates the statistics */
+int nbpt_painter_wait(nbpt_painter* painter);
+/* images as Pixels::images (src/painter/pixels/pixels.cpp:123-166):
+ * rgb [pixels][3] with background, rgba [pixels][4] premultiplied; either may be NULL */
+int nbpt_painter_images(nbpt_painter* painter, float* rgb, float* rgba);
+/* per-sample output of the last pass: points [pixels][spp][N-1], colors
+ * [pixels][spp][channels], valid [pixels][spp] (0: background sample); any may be NULL */
+int nbpt_painter_samples(nbpt_painter* painter, double* points, float* colors, unsigned char* valid);
+int nbpt_painter_statistics(nbpt_painter* painter, nbpt_statistics* statistics);
+/* the CUDA stream (cudaStream_t) the painter's passes run on, for callers
+ * that order their own work or events with it */
+void* nbpt_painter_stream(nbpt_painter* painter);
+
+/* ---- verification entry points (same arithmetic as the render path) ---- */
+
+/* closest hit (any = 0): kind (0 none, 1 flat, 2 solid, 3 facet), index,
+ * distance, point [count][N]; any hit (any = 1): kind = 0/1.
+ * rays [count][2N] = (origin, direction). */
+int nbpt_scene_trace(
+        nbpt_scene* scene, const double* rays, long long count, int any, int* kind, int* index, double* t,
+        double* point);
+
+/* facet records and BVH of mesh `mesh` (order of creation among meshes):
+ * counts = (facets, nodes, indices); planes [facets][N][N+1] (facet
+ * hyperplane then N-1 barycentric hyperplanes, each n[N], d);
+ * node_lo/node_hi [nodes][N]; node_info [nodes][3] (offset, count, axis);
+ * indices [indices]; normal_info [facets][2] (normal type, reverse mask).
+ * With planes == NULL only the counts are returned. */
+int nbpt_scene_mesh_export(
+        nbpt_scene* scene, int mesh, long long* counts, double* planes, double* node_lo, double* node_hi,
+        unsigned* node_info, unsigned* indices, int* normal_info);
+
+/* GGX brdf f and pdf of material `material` (src/shading/ggx/brdf.h:146-194) */
+int nbpt_scene_brdf(
+        nbpt_scene* scene, int material, const double* n, const double* v, const double* l, float* f, double* pdf);
+/* one brdf sample from the stream seed_seq(seed[0..seed_words)) */
+int nbpt_scene_brdf_sample(
+        nbpt_scene* scene, int material, const double* n, const double* v, const unsigned* seed, int seed_words,
+        double* l, double* pdf, float* f);
+/* one leave (kind 0) or arrive (kind 1) sample of light `light`;
+ * leave: out = [org N, dir N, normal N, pdf_pos, pdf_dir];
+ * arrive: out = [l N, pdf, distance] */
+int nbpt_scene_light_sample(
+        nbpt_scene* scene, int light, int kind, const unsigned* seed, int seed_words, const double* point,
+        double* out, float* radiance);
+
+/* raw PCG32 draws and uniform [0, 1) draws of a seed_seq stream, computed on the GPU */
+int nbpt_test_pcg(const unsigned* seed, int seed_words, int count, unsigned* out);
+int nbpt_test_canonical(const unsigned* seed, int seed_words, int count, int use_double, double* out);
+/* stratified jittered points of one pixel; returns the point count */
+int nbpt_test_sj_points(int dimension, int use_double, int spp, const unsigned* seed, int seed_words, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,751 @@
+// C ABI of the painter (include/nbpt.h): argument checks, error codes and
+// the thread-local error message around the C++ scene/painter classes.
+#include "../../include/nbpt.h"
+
+#include "core.cuh"
+#include "painter_api.h"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <exception>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+struct nbpt_scene
+{
+        std::unique_ptr<nbpt::Scene> impl;
+};
+
+struct nbpt_painter
+{
+        std::unique_ptr<nbpt::Painter> impl;
+};
+
+namespace
+{
+thread_local std::string g_error;
+
+class CudaError final : public std::runtime_error
+{
+public:
+        using std::runtime_error::runtime_error;
+};
+
+template <typename F>
+int guarded(const F& f)
+{
+        try
+        {
+                return f();
+        }
+        catch (const std::exception& e)
+        {
+                g_error = e.what();
+                const cudaError_t last = cudaGetLastError();
+                if (last != cudaSuccess || g_error.find("cuda") != std::string::npos)
+                {
+                        if (last != cudaSuccess)
+                        {
+                                g_error += std::string(" (") + cudaGetErrorString(last) + ")";
+                        }
+                        return NBPT_CUDA_ERROR;
+                }
+                return NBPT_ERROR;
+        }
+        catch (...)
+        {
+                g_error = "unknown error";
+                return NBPT_ERROR;
+        }
+}
+
+nbpt::Scene& scene_of(nbpt_scene* s)
+{
+        if (!s || !s->impl)
+        {
+                throw std::runtime_error("null scene");
+        }
+        return *s->impl;
+}
+
+nbpt::Painter& painter_of(nbpt_painter* p)
+{
+        if (!p || !p->impl)
+        {
+                throw std::runtime_error("null painter");
+        }
+        return *p->impl;
+}
+
+void require(const void* p, const char* what)
+{
+        if (!p)
+        {
+                throw std::runtime_error(std::string("null ") + what);
+        }
+}
+
+void require_device()
+{
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+        {
+                cudaGetLastError();
+                throw std::runtime_error("no CUDA device");
+        }
+}
+
+__global__ void pcg_kernel(const std::uint32_t* seed, const int words, const int count, std::uint32_t* out)
+{
+        nbpt::Pcg g = nbpt::seed_seq_pcg(seed, words);
+        for (int i = 0; i < count; ++i)
+        {
+                out[i] = g();
+        }
+}
+
+__global__ void canonical_kernel(const std::uint32_t* seed, const int words, const int count, const int use_double,
+                                 double* out)
+{
+        nbpt::Pcg g = nbpt::seed_seq_pcg(seed, words);
+        for (int i = 0; i < count; ++i)
+        {
+                out[i] = use_double ? nbpt::uniform<double>(g, 0.0, 1.0)
+                                    : static_cast<double>(nbpt::uniform<float>(g, 0.0f, 1.0f));
+        }
+}
+
+template <typename T>
+__global__ void sj_kernel(const std::uint32_t* seed, const int words, const int dimension, const int k,
+                          const T* offsets, double* out)
+{
+        nbpt::Pcg g = nbpt::seed_seq_pcg(seed, words);
+        int count = 1;
+        for (int d = 0; d < dimension; ++d)
+        {
+                count *= k;
+        }
+        for (int s = 0; s < count; ++s)
+        {
+                int rest = s;
+                for (int d = 0; d < dimension; ++d)
+                {
+                        const int idx = rest % k;
+                        rest /= k;
+                        const T a = offsets[idx];
+                        const T b = offsets[idx + 1];
+                        T v;
+                        do
+                        {
+                                v = nbpt::uniform<T>(g, a, b);
+                        } while (!(v < b));
+                        out[s * dimension + d] = static_cast<double>(v);
+                }
+        }
+}
+
+template <typename X>
+struct Buffer final
+{
+        X* p = nullptr;
+        explicit Buffer(const std::size_t n)
+        {
+                if (cudaMalloc(&p, n * sizeof(X)) != cudaSuccess)
+                {
+                        throw CudaError("cudaMalloc failed");
+                }
+        }
+        ~Buffer()
+        {
+                cudaFree(p);
+        }
+};
+
+template <typename T>
+int sj_points(const int dimension, const int spp, const std::uint32_t* seed, const int words, double* out)
+{
+        const double v = std::pow(spp, 1.0 / dimension);
+        int k = static_cast<int>(std::floor(v));
+        long long p = 1;
+        for (int i = 0; i < dimension; ++i)
+        {
+                p *= k;
+        }
+        if (p < spp)
+        {
+                k = static_cast<int>(std::ceil(v));
+        }
+        int count = 1;
+        for (int i = 0; i < dimension; ++i)
+        {
+                count *= k;
+        }
+        if (!out)
+        {
+                return count;
+        }
+        std::vector<T> offsets(k + 1);
+        const T size = (T(1) - T(0)) / static_cast<T>(k);
+        offsets[0] = 0;
+        for (int i = 1; i < k; ++i)
+        {
+                offsets[i] = T(0) + static_cast<T>(i) * size;
+        }
+        offsets[k] = 1;
+        Buffer<std::uint32_t> d_seed(words);
+        Buffer<T> d_offsets(k + 1);
+        Buffer<double> d_out(static_cast<std::size_t>(count) * dimension);
+        cudaMemcpy(d_seed.p, seed, words * sizeof(std::uint32_t), cudaMemcpyHostToDevice);
+        cudaMemcpy(d_offsets.p, offsets.data(), (k + 1) * sizeof(T), cudaMemcpyHostToDevice);
+        sj_kernel<T><<<1, 1>>>(d_seed.p, words, dimension, k, d_offsets.p, d_out.p);
+        if (cudaDeviceSynchronize() != cudaSuccess)
+        {
+                throw CudaError("sj kernel failed");
+        }
+        cudaMemcpy(out, d_out.p, static_cast<std::size_t>(count) * dimension * sizeof(double), cudaMemcpyDeviceToHost);
+        return count;
+}
+} // namespace
+
+extern "C"
+{
+const char* nbpt_last_error(void)
+{
+        return g_error.c_str();
+}
+
+int nbpt_device_count(void)
+{
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess)
+        {
+                cudaGetLastError();
+                return 0;
+        }
+        return count;
+}
+
+nbpt_scene* nbpt_scene_create(const int dimension, const int precision, const int color)
+{
+        nbpt_scene* out = nullptr;
+        guarded(
+                [&]
+                {
+                        if (precision != NBPT_FLOAT && precision != NBPT_DOUBLE)
+                        {
+                                throw std::runtime_error("precision must be NBPT_FLOAT or NBPT_DOUBLE");
+                        }
+                        if (color != NBPT_RGB && color != NBPT_SPECTRUM)
+                        {
+                                throw std::runtime_error("color must be NBPT_RGB or NBPT_SPECTRUM");
+                        }
+                        const bool d = precision == NBPT_DOUBLE;
+                        const bool s = color == NBPT_SPECTRUM;
+                        auto scene = std::make_unique<nbpt_scene>();
+                        switch (dimension)
+                        {
+                        case 3:
+                                scene->impl = nbpt::make_scene_3(d, s);
+                                break;
+                        case 4:
+                                scene->impl = nbpt::make_scene_4(d, s);
+                                break;
+                        case 5:
+                                scene->impl = nbpt::make_scene_5(d, s);
+                                break;
+                        default:
+                                throw std::runtime_error("dimension must be 3, 4 or 5");
+                        }
+                        out = scene.release();
+                        return 0;
+                });
+        return out;
+}
+
+void nbpt_scene_destroy(nbpt_scene* scene)
+{
+        delete scene;
+}
+
+int nbpt_scene_add_hyperplane_parallelotope(
+        nbpt_scene* scene,
+        const double metalness,
+        const double roughness,
+        const float* rgb,
+        const double alpha,
+        const double* org,
+        const double* vectors)
+{
+        return guarded(
+                [&]
+                {
+                        require(rgb, "color");
+                        require(org, "org");
+                        require(vectors, "vectors");
+                        return scene_of(scene).add_hyperplane_parallelotope(metalness, roughness, rgb, alpha, org, vectors);
+                });
+}
+
+int nbpt_scene_add_parallelotope(
+        nbpt_scene* scene,
+        const double metalness,
+        const double roughness,
+        const float* rgb,
+        const double alpha,
+        const double* org,
+        const double* vectors)
+{
+        return guarded(
+                [&]
+                {
+                        require(rgb, "color");
+                        require(org, "org");
+                        require(vectors, "vectors");
+                        return scene_of(scene).add_parallelotope(metalness, roughness, rgb, alpha, org, vectors);
+                });
+}
+
+int nbpt_scene_add_mesh_object(
+        nbpt_scene* scene,
+        const float* points,
+        const long long point_count,
+        const int* facets,
+        const long long facet_count,
+        const double* matrix,
+        const float* normals,
+        const float metalness,
+        const float roughness,
+        const float* rgb,
+        const float alpha)
+{
+        return guarded(
+                [&]
+                {
+                        require(points, "points");
+                        require(facets, "facets");
+                        require(matrix, "matrix");
+                        require(rgb, "color");
+                        return scene_of(scene).add_mesh_object(
+                                points, point_count, facets, facet_count, matrix, normals, metalness, roughness, rgb,
+                                alpha);
+                });
+}
+
+int nbpt_scene_add_mesh(nbpt_scene* scene)
+{
+        return guarded(
+                [&]
+                {
+                        return scene_of(scene).add_mesh();
+                });
+}
+
+int nbpt_scene_add_mesh_data(
+        nbpt_scene* scene,
+        const long long vertex_count,
+        const double* vertices,
+        const double* normals,
+        const long long facet_count,
+        const int* facets,
+        const int* facet_materials,
+        const int material_count,
+        const double* material_params,
+        const float* material_colors)
+{
+        return guarded(
+                [&]
+                {
+                        require(vertices, "vertices");
+                        require(facets, "facets");
+                        require(facet_materials, "facet materials");
+                        require(material_params, "material parameters");
+                        require(material_colors, "material colors");
+                        return scene_of(scene).add_mesh_data(
+                                vertex_count, vertices, normals, facet_count, facets, facet_materials, material_count,
+                                material_params, material_colors);
+                });
+}
+
+int nbpt_scene_add_parallelotope_light(nbpt_scene* scene, const int shape, const double* direction, const float* rgb)
+{
+        return guarded(
+                [&]
+                {
+                        require(direction, "direction");
+                        require(rgb, "radiance");
+                        return scene_of(scene).add_parallelotope_light(shape, direction, rgb);
+                });
+}
+
+int nbpt_scene_add_ball_light(
+        nbpt_scene* scene,
+        const double* center,
+        const double* direction,
+        const double radius,
+        const float* rgb)
+{
+        return guarded(
+                [&]
+                {
+                        require(center, "center");
+                        require(direction, "direction");
+                        require(rgb, "radiance");
+                        return scene_of(scene).add_ball_light(center, direction, radius, rgb);
+                });
+}
+
+int nbpt_scene_set_perspective_projector(
+        nbpt_scene* scene,
+        const double* org,
+        const double* dir,
+        const double* axes,
+        const double fov_degrees,
+        const int* size)
+{
+        return guarded(
+                [&]
+                {
+                        require(org, "org");
+                        require(dir, "dir");
+                        require(axes, "axes");
+                        require(size, "size");
+                        scene_of(scene).set_perspective_projector(org, dir, axes, fov_degrees, size);
+                        return 0;
+                });
+}
+
+int nbpt_scene_set_parallel_projector(
+        nbpt_scene* scene,
+        const double* org,
+        const double* dir,
+        const double* axes,
+        const double units_per_pixel,
+        const int* size)
+{
+        return guarded(
+                [&]
+                {
+                        require(org, "org");
+                        require(dir, "dir");
+                        require(axes, "axes");
+                        require(size, "size");
+                        scene_of(scene).set_parallel_projector(org, dir, axes, units_per_pixel, size);
+                        return 0;
+                });
+}
+
+int nbpt_scene_set_background(nbpt_scene* scene, const float* rgb)
+{
+        return guarded(
+                [&]
+                {
+                        require(rgb, "background");
+                        scene_of(scene).set_background(rgb);
+                        return 0;
+                });
+}
+
+int nbpt_scene_finalize(nbpt_scene* scene)
+{
+        return guarded(
+                [&]
+                {
+                        require_device();
+                        scene_of(scene).finalize();
+                        return 0;
+                });
+}
+
+long long nbpt_scene_pixel_count(const nbpt_scene* scene)
+{
+        long long r = NBPT_ERROR;
+        guarded(
+                [&]
+                {
+                        r = scene_of(const_cast<nbpt_scene*>(scene)).pixel_count();
+                        return 0;
+                });
+        return r;
+}
+
+int nbpt_scene_actual_spp(const nbpt_scene* scene, const int samples_per_pixel)
+{
+        return guarded(
+                [&]
+                {
+                        return scene_of(const_cast<nbpt_scene*>(scene)).actual_spp(samples_per_pixel);
+                });
+}
+
+long long nbpt_scene_device_bytes(const nbpt_scene* scene)
+{
+        long long r = NBPT_ERROR;
+        guarded(
+                [&]
+                {
+                        r = scene_of(const_cast<nbpt_scene*>(scene)).device_bytes();
+                        return 0;
+                });
+        return r;
+}
+
+nbpt_painter* nbpt_painter_create(nbpt_scene* scene, const int samples_per_pixel, const int max_depth, const unsigned seed)
+{
+        nbpt_painter* out = nullptr;
+        guarded(
+                [&]
+                {
+                        auto p = std::make_unique<nbpt_painter>();
+                        p->impl = scene_of(scene).create_painter(samples_per_pixel, max_depth, seed);
+                        out = p.release();
+                        return 0;
+                });
+        return out;
+}
+
+void nbpt_painter_destroy(nbpt_painter* painter)
+{
+        delete painter;
+}
+
+int nbpt_painter_enqueue(nbpt_painter* painter, const int passes)
+{
+        return guarded(
+                [&]
+                {
+                        if (passes < 1)
+                        {
+                                throw std::runtime_error("pass count must be greater than 0");
+                        }
+                        painter_of(painter).enqueue_passes(passes);
+                        return 0;
+                });
+}
+
+int nbpt_painter_wait(nbpt_painter* painter)
+{
+        return guarded(
+                [&]
+                {
+                        painter_of(painter).wait();
+                        return 0;
+                });
+}
+
+int nbpt_painter_images(nbpt_painter* painter, float* rgb, float* rgba)
+{
+        return guarded(
+                [&]
+                {
+                        painter_of(painter).images(rgb, rgba);
+                        return 0;
+                });
+}
+
+int nbpt_painter_samples(nbpt_painter* painter, double* points, float* colors, unsigned char* valid)
+{
+        return guarded(
+                [&]
+                {
+                        painter_of(painter).samples(points, colors, valid);
+                        return 0;
+                });
+}
+
+int nbpt_painter_statistics(nbpt_painter* painter, nbpt_statistics* statistics)
+{
+        return guarded(
+                [&]
+                {
+                        require(statistics, "statistics");
+                        const nbpt::Statistics s = painter_of(painter).statistics();
+                        statistics->pass_number = s.pass_number;
+                        statistics->pixel_count = s.pixel_count;
+                        statistics->ray_count = s.ray_count;
+                        statistics->sample_count = s.sample_count;
+                        statistics->previous_pass_duration = s.previous_pass_duration;
+                        statistics->paths_seconds = s.paths_seconds;
+                        statistics->nodes = s.nodes;
+                        statistics->facets = s.facets;
+                        statistics->shapes = s.shapes;
+                        return 0;
+                });
+}
+
+void* nbpt_painter_stream(nbpt_painter* painter)
+{
+        void* s = nullptr;
+        guarded(
+                [&]
+                {
+                        s = painter_of(painter).stream();
+                        return 0;
+                });
+        return s;
+}
+
+int nbpt_scene_trace(
+        nbpt_scene* scene,
+        const double* rays,
+        const long long count,
+        const int any,
+        int* kind,
+        int* index,
+        double* t,
+        double* point)
+{
+        return guarded(
+                [&]
+                {
+                        require(rays, "rays");
+                        require(kind, "kind");
+                        if (!any)
+                        {
+                                require(index, "index");
+                                require(t, "t");
+                                require(point, "point");
+                        }
+                        scene_of(scene).trace(rays, count, any, kind, index, t, point);
+                        return 0;
+                });
+}
+
+int nbpt_scene_mesh_export(
+        nbpt_scene* scene,
+        const int mesh,
+        long long* counts,
+        double* planes,
+        double* node_lo,
+        double* node_hi,
+        unsigned* node_info,
+        unsigned* indices,
+        int* normal_info)
+{
+        return guarded(
+                [&]
+                {
+                        require(counts, "counts");
+                        scene_of(scene).mesh_export(mesh, counts, planes, node_lo, node_hi, node_info, indices, normal_info);
+                        return 0;
+                });
+}
+
+int nbpt_scene_brdf(
+        nbpt_scene* scene,
+        const int material,
+        const double* n,
+        const double* v,
+        const double* l,
+        float* f,
+        double* pdf)
+{
+        return guarded(
+                [&]
+                {
+                        scene_of(scene).brdf(material, n, v, l, f, pdf);
+                        return 0;
+                });
+}
+
+int nbpt_scene_brdf_sample(
+        nbpt_scene* scene,
+        const int material,
+        const double* n,
+        const double* v,
+        const unsigned* seed,
+        const int seed_words,
+        double* l,
+        double* pdf,
+        float* f)
+{
+        return guarded(
+                [&]
+                {
+                        scene_of(scene).brdf_sample(material, n, v, seed, seed_words, l, pdf, f);
+                        return 0;
+                });
+}
+
+int nbpt_scene_light_sample(
+        nbpt_scene* scene,
+        const int light,
+        const int kind,
+        const unsigned* seed,
+        const int seed_words,
+        const double* point,
+        double* out,
+        float* radiance)
+{
+        return guarded(
+                [&]
+                {
+                        scene_of(scene).light_sample(light, kind, seed, seed_words, point, out, radiance);
+                        return 0;
+                });
+}
+
+int nbpt_test_pcg(const unsigned* seed, const int seed_words, const int count, unsigned* out)
+{
+        return guarded(
+                [&]
+                {
+                        require_device();
+                        Buffer<std::uint32_t> d_seed(seed_words);
+                        Buffer<std::uint32_t> d_out(count);
+                        cudaMemcpy(d_seed.p, seed, seed_words * sizeof(std::uint32_t), cudaMemcpyHostToDevice);
+                        pcg_kernel<<<1, 1>>>(d_seed.p, seed_words, count, d_out.p);
+                        if (cudaDeviceSynchronize() != cudaSuccess)
+                        {
+                                throw CudaError("pcg kernel failed");
+                        }
+                        cudaMemcpy(out, d_out.p, count * sizeof(std::uint32_t), cudaMemcpyDeviceToHost);
+                        return 0;
+                });
+}
+
+int nbpt_test_canonical(const unsigned* seed, const int seed_words, const int count, const int use_double, double* out)
+{
+        return guarded(
+                [&]
+                {
+                        require_device();
+                        Buffer<std::uint32_t> d_seed(seed_words);
+                        Buffer<double> d_out(count);
+                        cudaMemcpy(d_seed.p, seed, seed_words * sizeof(std::uint32_t), cudaMemcpyHostToDevice);
+                        canonical_kernel<<<1, 1>>>(d_seed.p, seed_words, count, use_double, d_out.p);
+                        if (cudaDeviceSynchronize() != cudaSuccess)
+                        {
+                                throw CudaError("canonical kernel failed");
+                        }
+                        cudaMemcpy(out, d_out.p, count * sizeof(double), cudaMemcpyDeviceToHost);
+                        return 0;
+                });
+}
+
+int nbpt_test_sj_points(
+        const int dimension,
+        const int use_double,
+        const int spp,
+        const unsigned* seed,
+        const int seed_words,
+        double* out)
+{
+        return guarded(
+                [&]
+                {
+                        if (dimension < 2 || dimension > 4 || spp < 1)
+                        {
+                                throw std::runtime_error("bad sampler arguments");
+                        }
+                        if (out)
+                        {
+                                require_device();
+                        }
+                        return use_double ? sj_points<double>(dimension, spp, seed, seed_words, out)
+                                          : sj_points<float>(dimension, spp, seed, seed_words, out);
+                });
+}
+}

@@ -1,0 +1,1139 @@
+// The painter's per-pixel estimator on the GPU: filtered, trimmed, with the
+// reference's exact merge semantics.
+//
+// Every sample of a source pixel is splatted into its 3^(n-1) neighbours with
+// the truncated Gaussian weight (src/painter/pixels/pixel_filter.h:32-70,
+// gaussian.h:38-78).  For one (receiving pixel, source pixel) pair the
+// weighted samples form a group; the group's two lowest and two highest
+// weighted luminances are held out and the rest summed
+// (samples/create.cpp:147-250); the group is merged into the receiving
+// pixel's state keeping the two lowest and two highest of the union
+// (samples/merge.cpp:78-223, com/merge.h:34-233).  Background samples (paths
+// that escape at the first hit) keep their own held-out weights.
+//
+// Which of several equal keys is held out, and the order of the float sums,
+// follow the reference step for step: groups are ordered with the same
+// insertion-sort and binary-heap selection the reference's sort and
+// partial_sort perform, sources are merged into a receiving pixel in
+// increasing pixel index, and all sums are in float as the reference keeps
+// them.  From the same samples the image is therefore the reference's, bit
+// for bit.  One thread gathers for one receiving pixel, so no atomics are
+// needed.
+#pragma once
+
+#include "core.cuh"
+
+#include <cstdint>
+
+namespace nbpt
+{
+inline constexpr int HELD_OUT = 4; // the reference's FILTER_SAMPLE_COUNT (pixels.h:42)
+
+// largest number of samples per pixel a pass can gather in one group
+inline constexpr int MAX_GROUP = 256;
+
+// ---------------------------------------------------------------------------
+// ordering of a group: the steps of an insertion sort (for up to eight
+// entries) and of a binary-heap partial selection (more entries), with the
+// "hole" moves of the classic sift-down / sift-up, on an index array ordered
+// by `less(a, b)`.
+
+template <typename Less>
+NBPT_HD void insertion_sort(int* a, const int n, const Less& less)
+{
+        for (int i = 1; i < n; ++i)
+        {
+                const int v = a[i];
+                if (less(v, a[0]))
+                {
+                        for (int k = i; k > 0; --k)
+                        {
+                                a[k] = a[k - 1];
+                        }
+                        a[0] = v;
+                }
+                else
+                {
+                        int k = i;
+                        while (less(v, a[k - 1]))
+                        {
+                                a[k] = a[k - 1];
+                                --k;
+                        }
+                        a[k] = v;
+                }
+        }
+}
+
+// Accessors that view either a plain range or its reverse.
+struct Forward final
+{
+        int* base;
+        NBPT_HD int& at(const int i) const
+        {
+                return base[i];
+        }
+};
+
+struct Reverse final
+{
+        int* last; // element 0 of the view is *last, element i is last[-i]
+        NBPT_HD int& at(const int i) const
+        {
+                return last[-i];
+        }
+};
+
+template <typename View, typename Less>
+NBPT_HD void heap_push(const View& v, int hole, const int top, const int value, const Less& less)
+{
+        int parent = (hole - 1) / 2;
+        while (hole > top && less(v.at(parent), value))
+        {
+                v.at(hole) = v.at(parent);
+                hole = parent;
+                parent = (hole - 1) / 2;
+        }
+        v.at(hole) = value;
+}
+
+template <typename View, typename Less>
+NBPT_HD void heap_adjust(const View& v, int hole, const int len, const int value, const Less& less)
+{
+        const int top = hole;
+        int second = hole;
+        while (second < (len - 1) / 2)
+        {
+                second = 2 * (second + 1);
+                if (less(v.at(second), v.at(second - 1)))
+                {
+                        --second;
+                }
+                v.at(hole) = v.at(second);
+                hole = second;
+        }
+        if ((len & 1) == 0 && second == (len - 2) / 2)
+        {
+                second = 2 * (second + 1);
+                v.at(hole) = v.at(second - 1);
+                hole = second - 1;
+        }
+        heap_push(v, hole, top, value, less);
+}
+
+template <typename View, typename Less>
+NBPT_HD void heap_make(const View& v, const int len, const Less& less)
+{
+        if (len < 2)
+        {
+                return;
+        }
+        int parent = (len - 2) / 2;
+        while (true)
+        {
+                const int value = v.at(parent);
+                heap_adjust(v, parent, len, value, less);
+                if (parent == 0)
+                {
+                        return;
+                }
+                --parent;
+        }
+}
+
+// pop the top of the heap [0, len) into position `result`
+template <typename View, typename Less>
+NBPT_HD void heap_pop(const View& v, const int len, const int result, const Less& less)
+{
+        const int value = v.at(result);
+        v.at(result) = v.at(0);
+        heap_adjust(v, 0, len, value, less);
+}
+
+// the `middle` smallest of [0, last) sorted into [0, middle)
+template <typename View, typename Less>
+NBPT_HD void partial_sort(const View& v, const int middle, const int last, const Less& less)
+{
+        heap_make(v, middle, less);
+        for (int i = middle; i < last; ++i)
+        {
+                if (less(v.at(i), v.at(0)))
+                {
+                        heap_pop(v, middle, i, less);
+                }
+        }
+        for (int len = middle; len > 1;)
+        {
+                --len;
+                heap_pop(v, len, len, less);
+        }
+}
+
+// src/painter/pixels/samples/com/sort.h:26-46
+template <typename Less, typename Greater>
+NBPT_HD void order_group(int* a, const int n, const Less& less, const Greater& greater)
+{
+        if (n <= 1)
+        {
+                return;
+        }
+        if (n <= HELD_OUT * 2)
+        {
+                insertion_sort(a, n, less);
+                return;
+        }
+        partial_sort(Forward{a}, HELD_OUT / 2, n, less);
+        // the highest of [HELD_OUT / 2, n), viewed from the end
+        partial_sort(Reverse{a + n - 1}, HELD_OUT / 2, n - HELD_OUT / 2, greater);
+}
+
+// ---------------------------------------------------------------------------
+// sample sets (samples/color.h, samples/background.h)
+
+template <int C>
+struct ColorSet final
+{
+        float color_sum[C];
+        float weight_sum;
+        float colors[HELD_OUT][C];
+        float weights[HELD_OUT];
+        float contributions[HELD_OUT];
+        int count; // held-out entries in use
+        int full;  // more than HELD_OUT samples seen: the sums are valid
+};
+
+struct BackgroundSet final
+{
+        float weight_sum;
+        float weights[HELD_OUT];
+        int count;
+        int full;
+};
+
+template <int C>
+struct PixelState final
+{
+        ColorSet<C> color;
+        BackgroundSet background;
+};
+
+// A group of one source pixel's samples for one receiving pixel: sample
+// indices in the source pixel and their float weights; colours are read
+// from global memory and weighted on use (sample.color = weight * colour).
+template <int C>
+struct ColorGroup final
+{
+        const float* colors; // the source pixel's sample colours [spp][C]
+        const float* weights;
+        const float* contributions;
+        const int* order;
+        int n;
+
+        NBPT_HD float color(const int k, const int c) const
+        {
+                const int i = order[k];
+                return weights[i] * colors[i * C + c];
+        }
+};
+
+// ---- merges (com/merge.h) ------------------------------------------------
+
+// Entry accessor over a set or a group, in the set's (sorted) order.
+template <int C>
+struct SetView final
+{
+        const ColorSet<C>* s;
+        const ColorGroup<C>* g; // when merging a fresh group
+        int g_full;
+        // group held-out positions: 0, 1 -> order[0], order[1]; 2, 3 -> order[n-2], order[n-1]
+
+        NBPT_HD int count() const
+        {
+                if (s)
+                {
+                        return s->full ? HELD_OUT : s->count;
+                }
+                return g_full ? HELD_OUT : g->n;
+        }
+
+        NBPT_HD int group_position(const int k) const
+        {
+                if (!g_full)
+                {
+                        return k;
+                }
+                return k < HELD_OUT / 2 ? k : g->n - HELD_OUT + k;
+        }
+
+        NBPT_HD float contribution(const int k) const
+        {
+                if (s)
+                {
+                        return s->contributions[k];
+                }
+                return g->contributions[g->order[group_position(k)]];
+        }
+
+        NBPT_HD float weight(const int k) const
+        {
+                if (s)
+                {
+                        return s->weights[k];
+                }
+                return g->weights[g->order[group_position(k)]];
+        }
+
+        NBPT_HD float color(const int k, const int c) const
+        {
+                if (s)
+                {
+                        return s->colors[k][c];
+                }
+                return g->color(group_position(k), c);
+        }
+};
+
+template <int C>
+NBPT_HD void copy_entry(ColorSet<C>& out, const int to, const SetView<C>& from, const int k)
+{
+#pragma unroll 8
+        for (int c = 0; c < C; ++c)
+        {
+                out.colors[to][c] = from.color(k, c);
+        }
+        out.weights[to] = from.weight(k);
+        out.contributions[to] = from.contribution(k);
+}
+
+template <int C>
+NBPT_HD void sum_entry(float* color_sum, float& weight_sum, const SetView<C>& from, const int k)
+{
+#pragma unroll 8
+        for (int c = 0; c < C; ++c)
+        {
+                color_sum[c] += from.color(k, c);
+        }
+        weight_sum += from.weight(k);
+}
+
+// merge_with_sum (com/merge.h:199-233, samples/merge.cpp:109-145)
+template <int C>
+NBPT_HD void merge_colors_with_sum(const SetView<C>& a, const SetView<C>& b, const float* a_sum, float a_wsum,
+                                   const float* b_sum, float b_wsum, const bool a_full, const bool b_full,
+                                   ColorSet<C>& out)
+{
+        // samples_color_sum / samples_weight_sum (samples/merge.cpp:37-76)
+        float sum[C];
+        float wsum;
+        if (a_full && b_full)
+        {
+#pragma unroll 8
+                for (int c = 0; c < C; ++c)
+                {
+                        sum[c] = a_sum[c] + b_sum[c];
+                }
+                wsum = a_wsum + b_wsum;
+        }
+        else if (a_full)
+        {
+#pragma unroll 8
+                for (int c = 0; c < C; ++c)
+                {
+                        sum[c] = a_sum[c];
+                }
+                wsum = a_wsum;
+        }
+        else if (b_full)
+        {
+#pragma unroll 8
+                for (int c = 0; c < C; ++c)
+                {
+                        sum[c] = b_sum[c];
+                }
+                wsum = b_wsum;
+        }
+        else
+        {
+#pragma unroll 8
+                for (int c = 0; c < C; ++c)
+                {
+                        sum[c] = 0;
+                }
+                wsum = 0;
+        }
+
+        const int a_size = a.count();
+        const int b_size = b.count();
+        ColorSet<C> r;
+        if (a_size == HELD_OUT && b_size == HELD_OUT)
+        {
+                int ai = 0;
+                int bi = 0;
+                for (int i = 0; i < HELD_OUT / 2; ++i)
+                {
+                        if (a.contribution(ai) < b.contribution(bi))
+                        {
+                                copy_entry(r, i, a, ai++);
+                        }
+                        else
+                        {
+                                copy_entry(r, i, b, bi++);
+                        }
+                }
+                while (ai < HELD_OUT / 2)
+                {
+                        sum_entry(sum, wsum, a, ai++);
+                }
+                while (bi < HELD_OUT / 2)
+                {
+                        sum_entry(sum, wsum, b, bi++);
+                }
+                ai = HELD_OUT - 1;
+                bi = HELD_OUT - 1;
+                for (int i = HELD_OUT - 1; i >= HELD_OUT / 2; --i)
+                {
+                        if (a.contribution(ai) > b.contribution(bi))
+                        {
+                                copy_entry(r, i, a, ai--);
+                        }
+                        else
+                        {
+                                copy_entry(r, i, b, bi--);
+                        }
+                }
+                while (ai >= HELD_OUT / 2)
+                {
+                        sum_entry(sum, wsum, a, ai--);
+                }
+                while (bi >= HELD_OUT / 2)
+                {
+                        sum_entry(sum, wsum, b, bi--);
+                }
+        }
+        else
+        {
+                int ai = 0;
+                int bi = 0;
+                int i = 0;
+                while (i < HELD_OUT / 2 && ai < a_size && bi < b_size)
+                {
+                        if (a.contribution(ai) < b.contribution(bi))
+                        {
+                                copy_entry(r, i++, a, ai++);
+                        }
+                        else
+                        {
+                                copy_entry(r, i++, b, bi++);
+                        }
+                }
+                while (i < HELD_OUT / 2 && ai < a_size)
+                {
+                        copy_entry(r, i++, a, ai++);
+                }
+                while (i < HELD_OUT / 2 && bi < b_size)
+                {
+                        copy_entry(r, i++, b, bi++);
+                }
+                const int a_low = ai;
+                const int b_low = bi;
+                int aj = a_size - 1;
+                int bj = b_size - 1;
+                int j = HELD_OUT - 1;
+                while (j >= HELD_OUT / 2 && aj >= a_low && bj >= b_low)
+                {
+                        if (a.contribution(aj) > b.contribution(bj))
+                        {
+                                copy_entry(r, j--, a, aj--);
+                        }
+                        else
+                        {
+                                copy_entry(r, j--, b, bj--);
+                        }
+                }
+                while (j >= HELD_OUT / 2 && aj >= a_low)
+                {
+                        copy_entry(r, j--, a, aj--);
+                }
+                while (j >= HELD_OUT / 2 && bj >= b_low)
+                {
+                        copy_entry(r, j--, b, bj--);
+                }
+                for (int k = a_low; k <= aj; ++k)
+                {
+                        sum_entry(sum, wsum, a, k);
+                }
+                for (int k = b_low; k <= bj; ++k)
+                {
+                        sum_entry(sum, wsum, b, k);
+                }
+        }
+#pragma unroll 8
+        for (int c = 0; c < C; ++c)
+        {
+                r.color_sum[c] = sum[c];
+        }
+        r.weight_sum = wsum;
+        r.count = HELD_OUT;
+        r.full = 1;
+        out = r;
+}
+
+// Merge a fresh group into a pixel's colour set (samples/merge.cpp:198-223).
+template <int C>
+NBPT_HD void merge_color_group(ColorSet<C>& s, const ColorGroup<C>& g, const float* g_sum, const float g_wsum,
+                               const bool g_full)
+{
+        const SetView<C> a{&s, nullptr, 0};
+        const SetView<C> b{nullptr, &g, g_full ? 1 : 0};
+        const int a_count = a.count();
+        const int b_count = b.count();
+        if (a_count + b_count > HELD_OUT)
+        {
+                merge_colors_with_sum(a, b, s.color_sum, s.weight_sum, g_sum, g_wsum, s.full != 0, g_full, s);
+                return;
+        }
+        if (b_count == 0)
+        {
+                return;
+        }
+        if (a_count == 0)
+        {
+                ColorSet<C> r;
+                for (int k = 0; k < b_count; ++k)
+                {
+                        copy_entry(r, k, b, k);
+                }
+                r.count = b_count;
+                r.full = 0;
+                s = r;
+                return;
+        }
+        // merge (com/merge.h:235-271): sorted merge of two small sets
+        ColorSet<C> r;
+        int i = 0;
+        int ai = 0;
+        int bi = 0;
+        while (ai < a_count && bi < b_count)
+        {
+                if (a.contribution(ai) < b.contribution(bi))
+                {
+                        copy_entry(r, i++, a, ai++);
+                }
+                else
+                {
+                        copy_entry(r, i++, b, bi++);
+                }
+        }
+        while (ai < a_count)
+        {
+                copy_entry(r, i++, a, ai++);
+        }
+        while (bi < b_count)
+        {
+                copy_entry(r, i++, b, bi++);
+        }
+        r.count = a_count + b_count;
+        r.full = 0;
+        s = r;
+}
+
+// Background sets: the same merges on weights only.
+NBPT_HD void merge_background_group(BackgroundSet& s, const float* gw, const int n)
+{
+        // gw: the group's weights, already ordered (order_group on values)
+        const bool g_full = n > HELD_OUT;
+        float held[HELD_OUT];
+        float g_sum = 0;
+        int g_count = n;
+        if (g_full)
+        {
+                held[0] = gw[0];
+                held[1] = gw[1];
+                for (int k = 2; k < n - 2; ++k)
+                {
+                        g_sum += gw[k];
+                }
+                held[2] = gw[n - 2];
+                held[3] = gw[n - 1];
+                g_count = HELD_OUT;
+        }
+        else
+        {
+                for (int k = 0; k < n; ++k)
+                {
+                        held[k] = gw[k];
+                }
+        }
+        const int a_count = s.full ? HELD_OUT : s.count;
+        if (a_count + g_count > HELD_OUT)
+        {
+                float wsum;
+                if (s.full && g_full)
+                {
+                        wsum = s.weight_sum + g_sum;
+                }
+                else if (s.full)
+                {
+                        wsum = s.weight_sum;
+                }
+                else if (g_full)
+                {
+                        wsum = g_sum;
+                }
+                else
+                {
+                        wsum = 0;
+                }
+                float out[HELD_OUT];
+                const float* a = s.weights;
+                const float* b = held;
+                const int a_size = a_count;
+                const int b_size = g_count;
+                if (a_size == HELD_OUT && b_size == HELD_OUT)
+                {
+                        int ai = 0;
+                        int bi = 0;
+                        for (int i = 0; i < HELD_OUT / 2; ++i)
+                        {
+                                out[i] = (a[ai] < b[bi]) ? a[ai++] : b[bi++];
+                        }
+                        while (ai < HELD_OUT / 2)
+                        {
+                                wsum += a[ai++];
+                        }
+                        while (bi < HELD_OUT / 2)
+                        {
+                                wsum += b[bi++];
+                        }
+                        ai = HELD_OUT - 1;
+                        bi = HELD_OUT - 1;
+                        for (int i = HELD_OUT - 1; i >= HELD_OUT / 2; --i)
+                        {
+                                out[i] = (a[ai] > b[bi]) ? a[ai--] : b[bi--];
+                        }
+                        while (ai >= HELD_OUT / 2)
+                        {
+                                wsum += a[ai--];
+                        }
+                        while (bi >= HELD_OUT / 2)
+                        {
+                                wsum += b[bi--];
+                        }
+                }
+                else
+                {
+                        int ai = 0;
+                        int bi = 0;
+                        int i = 0;
+                        while (i < HELD_OUT / 2 && ai < a_size && bi < b_size)
+                        {
+                                out[i++] = (a[ai] < b[bi]) ? a[ai++] : b[bi++];
+                        }
+                        while (i < HELD_OUT / 2 && ai < a_size)
+                        {
+                                out[i++] = a[ai++];
+                        }
+                        while (i < HELD_OUT / 2 && bi < b_size)
+                        {
+                                out[i++] = b[bi++];
+                        }
+                        const int a_low = ai;
+                        const int b_low = bi;
+                        int aj = a_size - 1;
+                        int bj = b_size - 1;
+                        int j = HELD_OUT - 1;
+                        while (j >= HELD_OUT / 2 && aj >= a_low && bj >= b_low)
+                        {
+                                out[j--] = (a[aj] > b[bj]) ? a[aj--] : b[bj--];
+                        }
+                        while (j >= HELD_OUT / 2 && aj >= a_low)
+                        {
+                                out[j--] = a[aj--];
+                        }
+                        while (j >= HELD_OUT / 2 && bj >= b_low)
+                        {
+                                out[j--] = b[bj--];
+                        }
+                        for (int k = a_low; k <= aj; ++k)
+                        {
+                                wsum += a[k];
+                        }
+                        for (int k = b_low; k <= bj; ++k)
+                        {
+                                wsum += b[k];
+                        }
+                }
+                for (int k = 0; k < HELD_OUT; ++k)
+                {
+                        s.weights[k] = out[k];
+                }
+                s.weight_sum = wsum;
+                s.count = HELD_OUT;
+                s.full = 1;
+                return;
+        }
+        if (g_count == 0)
+        {
+                return;
+        }
+        if (a_count == 0)
+        {
+                for (int k = 0; k < g_count; ++k)
+                {
+                        s.weights[k] = held[k];
+                }
+                s.count = g_count;
+                s.full = 0;
+                return;
+        }
+        float out[HELD_OUT];
+        int i = 0;
+        int ai = 0;
+        int bi = 0;
+        while (ai < a_count && bi < g_count)
+        {
+                out[i++] = (s.weights[ai] < held[bi]) ? s.weights[ai++] : held[bi++];
+        }
+        while (ai < a_count)
+        {
+                out[i++] = s.weights[ai++];
+        }
+        while (bi < g_count)
+        {
+                out[i++] = held[bi++];
+        }
+        for (int k = 0; k < i; ++k)
+        {
+                s.weights[k] = out[k];
+        }
+        s.count = i;
+        s.full = 0;
+}
+
+// ---------------------------------------------------------------------------
+// accumulation kernel: one thread per receiving pixel
+
+template <int N>
+struct Screen final
+{
+        int size[N - 1];
+};
+
+template <int N, typename T, int C>
+__global__ void __launch_bounds__(128) accumulate_kernel(
+        const Screen<N> screen,
+        const long long pixel_count,
+        const int spp,
+        const T* __restrict__ points,
+        const float* __restrict__ colors,
+        const float* __restrict__ lum,
+        const unsigned char* __restrict__ valid,
+        const T alpha,
+        const T exp_radius,
+        PixelState<C>* __restrict__ state)
+{
+        const long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+        if (t >= pixel_count)
+        {
+                return;
+        }
+        int tc[N - 1];
+        {
+                long long rest = t;
+#pragma unroll
+                for (int d = 0; d < N - 1; ++d)
+                {
+                        tc[d] = static_cast<int>(rest % screen.size[d]);
+                        rest /= screen.size[d];
+                }
+        }
+        PixelState<C> st = state[t];
+
+        float w[MAX_GROUP];
+        float contribution[MAX_GROUP];
+        int color_order[MAX_GROUP];
+        float background[MAX_GROUP];
+
+        int neighbours = 1;
+#pragma unroll
+        for (int d = 0; d < N - 1; ++d)
+        {
+                neighbours *= 3;
+        }
+        // sources in increasing pixel index: the last screen axis outermost
+        for (int nb = 0; nb < neighbours; ++nb)
+        {
+                int pc[N - 1];
+                bool inside = true;
+                {
+                        int rest = nb;
+#pragma unroll
+                        for (int d = 0; d < N - 1; ++d)
+                        {
+                                pc[d] = tc[d] + (rest % 3) - 1;
+                                rest /= 3;
+                                inside = inside && pc[d] >= 0 && pc[d] < screen.size[d];
+                        }
+                }
+                if (!inside)
+                {
+                        continue;
+                }
+                long long p = 0;
+#pragma unroll
+                for (int d = N - 2; d >= 0; --d)
+                {
+                        p = p * screen.size[d] + pc[d];
+                }
+
+                // weights (pixel_filter.h:57-69, gaussian.h:66-77) and the
+                // selection of colour and background samples (com/select.h:28-47)
+                int nc = 0;
+                int nbg = 0;
+                for (int j = 0; j < spp; ++j)
+                {
+                        const long long sidx = p * spp + j;
+                        const T x0 = (static_cast<T>(tc[0] - pc[0]) + T(0.5)) - points[sidx * (N - 1)];
+                        T weight = max_value(T(0), exp(alpha * x0 * x0) - exp_radius);
+#pragma unroll
+                        for (int d = 1; d < N - 1; ++d)
+                        {
+                                const T x = (static_cast<T>(tc[d] - pc[d]) + T(0.5)) - points[sidx * (N - 1) + d];
+                                weight *= max_value(T(0), exp(alpha * x * x) - exp_radius);
+                        }
+                        if (!(weight > 0))
+                        {
+                                continue;
+                        }
+                        const float wf = static_cast<float>(weight);
+                        if (valid[sidx])
+                        {
+                                w[j] = wf;
+                                contribution[j] = wf * lum[sidx];
+                                color_order[nc++] = j;
+                        }
+                        else
+                        {
+                                background[nbg++] = wf;
+                        }
+                }
+
+                if (nc > 0)
+                {
+                        const auto less = [&](const int a, const int b)
+                        {
+                                return contribution[a] < contribution[b];
+                        };
+                        const auto greater = [&](const int a, const int b)
+                        {
+                                return contribution[a] > contribution[b];
+                        };
+                        order_group(color_order, nc, less, greater);
+                        const ColorGroup<C> g{colors + p * spp * C, w, contribution, color_order, nc};
+                        float g_sum[C];
+                        float g_wsum = 0;
+#pragma unroll 8
+                        for (int c = 0; c < C; ++c)
+                        {
+                                g_sum[c] = 0;
+                        }
+                        const bool g_full = nc > HELD_OUT;
+                        if (g_full)
+                        {
+                                // create_with_sum (samples/com/create.h:28-55)
+                                for (int k = HELD_OUT / 2; k < nc - HELD_OUT / 2; ++k)
+                                {
+#pragma unroll 8
+                                        for (int c = 0; c < C; ++c)
+                                        {
+                                                g_sum[c] += g.color(k, c);
+                                        }
+                                        g_wsum += w[color_order[k]];
+                                }
+                        }
+                        merge_color_group(st.color, g, g_sum, g_wsum, g_full);
+                }
+                if (nbg > 0)
+                {
+                        // background samples are ordered by value
+                        int order[MAX_GROUP];
+                        for (int k = 0; k < nbg; ++k)
+                        {
+                                order[k] = k;
+                        }
+                        const auto less = [&](const int a, const int b)
+                        {
+                                return background[a] < background[b];
+                        };
+                        const auto greater = [&](const int a, const int b)
+                        {
+                                return background[a] > background[b];
+                        };
+                        order_group(order, nbg, less, greater);
+                        float sorted[MAX_GROUP];
+                        for (int k = 0; k < nbg; ++k)
+                        {
+                                sorted[k] = background[order[k]];
+                        }
+                        merge_background_group(st.background, sorted, nbg);
+                }
+        }
+        state[t] = st;
+}
+
+// ---------------------------------------------------------------------------
+// image resolve: merge_color / merge_color_alpha (samples/merge_color.cpp:45-177)
+// and the RGB of the colour (src/color/color.h rgb32).  The background is
+// black: its colour and contribution are 0.
+
+template <int C>
+struct Resolved final
+{
+        bool has;
+        float color[C];
+        float color_weight;
+        float background_weight;
+};
+
+template <int C>
+NBPT_HD Resolved<C> resolve_pixel(const PixelState<C>& st)
+{
+        Resolved<C> res;
+        res.has = false;
+        const ColorSet<C>& a = st.color;
+        const BackgroundSet& b = st.background;
+        const int a_size = a.full ? HELD_OUT : a.count;
+        const int b_size = b.full ? HELD_OUT : b.count;
+        if (a_size + b_size <= HELD_OUT)
+        {
+                if (a_size == 0 || b_size != 0 || !a.full)
+                {
+                        return res;
+                }
+                res.has = true;
+#pragma unroll 8
+                for (int c = 0; c < C; ++c)
+                {
+                        res.color[c] = a.color_sum[c];
+                }
+                res.color_weight = a.weight_sum;
+                res.background_weight = 0;
+                return res;
+        }
+        res.has = true;
+#pragma unroll 8
+        for (int c = 0; c < C; ++c)
+        {
+                res.color[c] = a.full ? a.color_sum[c] : 0.0f;
+        }
+        res.color_weight = a.full ? a.weight_sum : 0.0f;
+        res.background_weight = b.full ? b.weight_sum : 0.0f;
+
+        const auto a_key = [&](const int i)
+        {
+                return a.contributions[i];
+        };
+        const auto b_key = [&](const int i)
+        {
+                return b.weights[i] * 0.0f;
+        };
+        const auto sum_a = [&](const int i)
+        {
+#pragma unroll 8
+                for (int c = 0; c < C; ++c)
+                {
+                        res.color[c] += a.colors[i][c];
+                }
+                res.color_weight += a.weights[i];
+        };
+        const auto sum_b = [&](const int i)
+        {
+                res.background_weight += b.weights[i];
+        };
+        if (a_size == HELD_OUT && b_size == HELD_OUT)
+        {
+                int ai = 0;
+                int bi = 0;
+                for (int i = 0; i < HELD_OUT / 2; ++i)
+                {
+                        if (a_key(ai) < b_key(bi))
+                        {
+                                ++ai;
+                        }
+                        else
+                        {
+                                ++bi;
+                        }
+                }
+                while (ai < HELD_OUT / 2)
+                {
+                        sum_a(ai++);
+                }
+                while (bi < HELD_OUT / 2)
+                {
+                        sum_b(bi++);
+                }
+                ai = HELD_OUT - 1;
+                bi = HELD_OUT - 1;
+                for (int i = HELD_OUT - 1; i >= HELD_OUT / 2; --i)
+                {
+                        if (a_key(ai) > b_key(bi))
+                        {
+                                --ai;
+                        }
+                        else
+                        {
+                                --bi;
+                        }
+                }
+                while (ai >= HELD_OUT / 2)
+                {
+                        sum_a(ai--);
+                }
+                while (bi >= HELD_OUT / 2)
+                {
+                        sum_b(bi--);
+                }
+                return res;
+        }
+        int ai = 0;
+        int bi = 0;
+        int i = 0;
+        while (i < HELD_OUT / 2 && ai < a_size && bi < b_size)
+        {
+                if (a_key(ai) < b_key(bi))
+                {
+                        ++ai;
+                }
+                else
+                {
+                        ++bi;
+                }
+                ++i;
+        }
+        while (i < HELD_OUT / 2 && ai < a_size)
+        {
+                ++ai;
+                ++i;
+        }
+        while (i < HELD_OUT / 2 && bi < b_size)
+        {
+                ++bi;
+                ++i;
+        }
+        const int a_low = ai;
+        const int b_low = bi;
+        int aj = a_size - 1;
+        int bj = b_size - 1;
+        int j = HELD_OUT - 1;
+        while (j >= HELD_OUT / 2 && aj >= a_low && bj >= b_low)
+        {
+                if (a_key(aj) > b_key(bj))
+                {
+                        --aj;
+                }
+                else
+                {
+                        --bj;
+                }
+                --j;
+        }
+        while (j >= HELD_OUT / 2 && aj >= a_low)
+        {
+                --aj;
+                --j;
+        }
+        while (j >= HELD_OUT / 2 && bj >= b_low)
+        {
+                --bj;
+                --j;
+        }
+        for (int k = a_low; k <= aj; ++k)
+        {
+                sum_a(k);
+        }
+        for (int k = b_low; k <= bj; ++k)
+        {
+                sum_b(k);
+        }
+        return res;
+}
+
+template <int C>
+__global__ void resolve_kernel(
+        const long long pixel_count,
+        const PixelState<C>* __restrict__ state,
+        const float* __restrict__ xyz, // [3][64] colour matching functions (spectrum only)
+        float* __restrict__ rgb,
+        float* __restrict__ rgba)
+{
+        const long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+        if (t >= pixel_count)
+        {
+                return;
+        }
+        const Resolved<C> r = resolve_pixel(state[t]);
+        float out[3] = {0.0f, 0.0f, 0.0f};
+        float out_a[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        if (r.has)
+        {
+                const float sum = r.color_weight + r.background_weight;
+                float color[C];
+#pragma unroll 8
+                for (int c = 0; c < C; ++c)
+                {
+                        color[c] = r.color[c] / sum;
+                }
+                float c_rgb[3];
+                if constexpr (C == 3)
+                {
+                        c_rgb[0] = max_value(0.0f, color[0]);
+                        c_rgb[1] = max_value(0.0f, color[1]);
+                        c_rgb[2] = max_value(0.0f, color[2]);
+                }
+                else
+                {
+                        float v[3];
+                        for (int k = 0; k < 3; ++k)
+                        {
+                                const float* f = xyz + k * 64;
+                                float s = max_value(0.0f, color[0]) * f[0];
+                                for (int c = 1; c < C; ++c)
+                                {
+                                        s += max_value(0.0f, color[c]) * f[c];
+                                }
+                                v[k] = s;
+                        }
+                        c_rgb[0] = max_value(0.0f, 3.2406255f * v[0] + -1.5372080f * v[1] + -0.4986286f * v[2]);
+                        c_rgb[1] = max_value(0.0f, -0.9689307f * v[0] + 1.8757561f * v[1] + 0.0415175f * v[2]);
+                        c_rgb[2] = max_value(0.0f, 0.0557101f * v[0] + -0.2040211f * v[1] + 1.0569959f * v[2]);
+                }
+                const bool background_only =
+                        !(r.color_weight == sum || (r.color_weight / sum) == 1) &&
+                        (r.background_weight == sum || (r.background_weight / sum) == 1);
+                if (!background_only)
+                {
+                        out[0] = c_rgb[0];
+                        out[1] = c_rgb[1];
+                        out[2] = c_rgb[2];
+                }
+                if (r.color_weight != 0)
+                {
+                        out_a[0] = c_rgb[0];
+                        out_a[1] = c_rgb[1];
+                        out_a[2] = c_rgb[2];
+                        out_a[3] = r.color_weight / sum;
+                }
+        }
+        rgb[t * 3 + 0] = out[0];
+        rgb[t * 3 + 1] = out[1];
+        rgb[t * 3 + 2] = out[2];
+        if (rgba)
+        {
+                rgba[t * 4 + 0] = out_a[0];
+                rgba[t * 4 + 1] = out_a[1];
+                rgba[t * 4 + 2] = out_a[2];
+                rgba[t * 4 + 3] = out_a[3];
+        }
+}
+} // namespace nbpt

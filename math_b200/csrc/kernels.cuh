@@ -1,0 +1,295 @@
+// CUDA kernels of the painter: facet setup, stratified sub-pixel samples,
+// the path kernel, the filtered trimmed accumulation and image resolve, and
+// ray-query and per-function kernels used for verification.
+#pragma once
+
+#include "bpt.cuh"
+#include "core.cuh"
+#include "geometry.cuh"
+#include "scene.cuh"
+#include "shading.cuh"
+
+#include <cstdint>
+
+namespace nbpt
+{
+// ---------------------------------------------------------------------------
+// facet setup at scene load, in double precision (hyperplane_simplex.h:82-111,
+// mesh/facet.cpp:83-125), stored in the path precision T.
+
+template <int N, typename T>
+__global__ void facet_setup_kernel(
+        const double* __restrict__ vertices,
+        const double* __restrict__ normals, // nullptr: no vertex normals
+        const int* __restrict__ facet_vertices,
+        const int* __restrict__ facet_materials,
+        const long long count,
+        Facet<N, T>* __restrict__ out,
+        int* __restrict__ error)
+{
+        const long long f = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+        if (f >= count)
+        {
+                return;
+        }
+        Vec<N, double> v[N];
+        int idx[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+        {
+                idx[k] = facet_vertices[f * N + k];
+#pragma unroll
+                for (int d = 0; d < N; ++d)
+                {
+                        v[k][d] = vertices[static_cast<long long>(idx[k]) * N + d];
+                }
+        }
+        Simplex<N, double> s;
+        if (!s.set(v))
+        {
+                atomicMax(error, 1);
+                return;
+        }
+        int normal_type = static_cast<int>(NormalType::NONE);
+        unsigned reverse_mask = 0;
+        if (normals)
+        {
+                double dots[N];
+                bool unidirectional = true;
+                bool positive = true;
+                bool negative = true;
+#pragma unroll
+                for (int k = 0; k < N; ++k)
+                {
+                        Vec<N, double> n;
+#pragma unroll
+                        for (int d = 0; d < N; ++d)
+                        {
+                                n[d] = normals[static_cast<long long>(idx[k]) * N + d];
+                        }
+                        dots[k] = dot(n, s.plane.n);
+                        const double a = abs_value(dots[k]);
+                        if (!(dots[k] - dots[k] == 0 && a >= 0.7))
+                        {
+                                unidirectional = false;
+                        }
+                        positive = positive && dots[k] > 0;
+                        negative = negative && dots[k] < 0;
+                }
+                if (unidirectional)
+                {
+                        if (positive)
+                        {
+                                normal_type = static_cast<int>(NormalType::USE);
+                        }
+                        else if (negative)
+                        {
+                                normal_type = static_cast<int>(NormalType::USE);
+                                s.plane.n = -s.plane.n;
+                                s.plane.d = -s.plane.d;
+                        }
+                        else
+                        {
+                                normal_type = static_cast<int>(NormalType::REVERSE);
+#pragma unroll
+                                for (int k = 0; k < N; ++k)
+                                {
+                                        if (dots[k] < 0)
+                                        {
+                                                reverse_mask |= 1u << k;
+                                        }
+                                }
+                        }
+                }
+        }
+        Facet<N, T> r;
+#pragma unroll
+        for (int d = 0; d < N; ++d)
+        {
+                r.simplex.plane.n[d] = static_cast<T>(s.plane.n[d]);
+        }
+        r.simplex.plane.d = static_cast<T>(s.plane.d);
+#pragma unroll
+        for (int i = 0; i < N - 1; ++i)
+        {
+#pragma unroll
+                for (int d = 0; d < N; ++d)
+                {
+                        r.simplex.planes[i].n[d] = static_cast<T>(s.planes[i].n[d]);
+                }
+                r.simplex.planes[i].d = static_cast<T>(s.planes[i].d);
+        }
+        r.material = facet_materials[f];
+        r.normal_type = normal_type;
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+        {
+                r.normals[k] = idx[k];
+        }
+        r.reverse_mask = reverse_mask;
+        out[f] = r;
+}
+
+// ---------------------------------------------------------------------------
+// stratified jittered sub-pixel points (src/sampling/sj_sampler.h:51-205),
+// one thread per pixel, from the pixel's stream seed_seq{seed, pass, p, 0}.
+
+template <int M, typename T>
+__global__ void sj_points_kernel(
+        const long long begin,
+        const long long end,
+        const std::uint32_t seed,
+        const std::uint32_t pass,
+        const int k, // strata per dimension
+        const T* __restrict__ offsets,
+        T* __restrict__ points)
+{
+        const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+        if (i >= end - begin)
+        {
+                return;
+        }
+        const long long p = begin + i;
+        const std::uint32_t words[4] = {seed, pass, static_cast<std::uint32_t>(p), 0u};
+        Pcg g = seed_seq_pcg(words, 4);
+        int count = 1;
+#pragma unroll
+        for (int d = 0; d < M; ++d)
+        {
+                count *= k;
+        }
+        T* const out = points + i * count * M;
+        for (int s = 0; s < count; ++s)
+        {
+                int rest = s;
+#pragma unroll
+                for (int d = 0; d < M; ++d)
+                {
+                        const int idx = rest % k;
+                        rest /= k;
+                        const T a = offsets[idx];
+                        const T b = offsets[idx + 1];
+                        T v;
+                        do
+                        {
+                                v = uniform<T>(g, a, b);
+                        } while (!(v < b));
+                        out[s * M + d] = v;
+                }
+        }
+}
+
+// ---------------------------------------------------------------------------
+// paths: one thread per (pixel, sample), stream seed_seq{seed, pass, p, i+1}
+
+struct PathStats final
+{
+        unsigned long long queries;
+        unsigned long long nodes;
+        unsigned long long facets;
+        unsigned long long shapes;
+};
+
+template <int C>
+NBPT_HD float luminance(const Color<C>& c, const float* y)
+{
+        if constexpr (C == 3)
+        {
+                const float r = max_value(0.0f, c.c[0]);
+                const float g = max_value(0.0f, c.c[1]);
+                const float b = max_value(0.0f, c.c[2]);
+                return 0.2126f * r + 0.7152f * g + 0.0722f * b;
+        }
+        else
+        {
+                float s = max_value(0.0f, c.c[0]) * y[0];
+#pragma unroll 8
+                for (int i = 1; i < C; ++i)
+                {
+                        s += max_value(0.0f, c.c[i]) * y[i];
+                }
+                return s;
+        }
+}
+
+template <int N, typename T, int C>
+__global__ void __launch_bounds__(128) paths_kernel(
+        const DeviceScene<N, T, C> scene,
+        const long long begin,
+        const long long end,
+        const int spp,
+        const int max_depth,
+        const std::uint32_t seed,
+        const std::uint32_t pass,
+        const T* __restrict__ points,
+        float* __restrict__ colors,
+        float* __restrict__ lum,
+        unsigned char* __restrict__ valid,
+        const float* __restrict__ cie_y,
+        PathStats* __restrict__ stats)
+{
+        const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+        const long long paths = (end - begin) * spp;
+        QueryCounters counters{0, 0, 0, 0};
+        if (i < paths)
+        {
+                const long long local_pixel = i / spp;
+                const int sample = static_cast<int>(i - local_pixel * spp);
+                const long long p = begin + local_pixel;
+
+                Vec<N - 1, T> point;
+                {
+                        long long rest = p;
+#pragma unroll
+                        for (int d = 0; d < N - 1; ++d)
+                        {
+                                const int size = scene.projector.size[d];
+                                const long long q = rest / size;
+                                point[d] = static_cast<T>(static_cast<int>(rest - q * size)) + points[i * (N - 1) + d];
+                                rest = q;
+                        }
+                }
+                const Ray<N, T> ray = scene.projector.ray(point);
+
+                const std::uint32_t words[4] = {seed, pass, static_cast<std::uint32_t>(p),
+                                                static_cast<std::uint32_t>(sample + 1)};
+                Pcg g = seed_seq_pcg(words, 4);
+                const SceneQueries<N, T, C> q{scene, counters};
+                Bpt<N, T, C> bpt{q, scene, g, max_depth};
+                Color<C> color;
+                const bool has = bpt.run(ray, color);
+                valid[i] = has ? 1 : 0;
+                if (!has)
+                {
+                        color = Color<C>::filled(0);
+                }
+#pragma unroll 8
+                for (int c = 0; c < C; ++c)
+                {
+                        colors[i * C + c] = color.c[c];
+                }
+                lum[i] = has ? luminance(color, cie_y) : 0.0f;
+        }
+        // warp-aggregated statistics
+        unsigned long long a = counters.queries;
+        unsigned long long b = counters.nodes;
+        unsigned long long c = counters.facets;
+        unsigned long long d = counters.shapes;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+        {
+                a += __shfl_down_sync(0xffffffffu, a, o);
+                b += __shfl_down_sync(0xffffffffu, b, o);
+                c += __shfl_down_sync(0xffffffffu, c, o);
+                d += __shfl_down_sync(0xffffffffu, d, o);
+        }
+        if ((threadIdx.x & 31) == 0)
+        {
+                atomicAdd(&stats->queries, a);
+                atomicAdd(&stats->nodes, b);
+                atomicAdd(&stats->facets, c);
+                atomicAdd(&stats->shapes, d);
+        }
+}
+
+} // namespace nbpt

@@ -1,0 +1,92 @@
+// Type-erased interface between the C-ABI (capi.cpp) and the templated
+// scene/painter implementations compiled once per space dimension
+// (painter_n3.cu, painter_n4.cu, painter_n5.cu).
+#pragma once
+
+#include <cstdint>
+#include <memory>
+
+namespace nbpt
+{
+struct Statistics final
+{
+        long long pass_number;
+        long long pixel_count;
+        long long ray_count;
+        long long sample_count;
+        double previous_pass_duration; // seconds, device time of the last pass
+        double paths_seconds;          // device time of the path kernel, last pass
+        unsigned long long nodes;      // BVH nodes visited, last pass
+        unsigned long long facets;     // facet records tested, last pass
+        unsigned long long shapes;     // other shapes tested, last pass
+};
+
+class Painter
+{
+public:
+        virtual ~Painter() = default;
+        virtual void enqueue_passes(int passes) = 0;
+        virtual void wait() = 0;
+        virtual void images(float* rgb, float* rgba) = 0;
+        virtual void samples(double* points, float* colors, unsigned char* valid) = 0;
+        virtual Statistics statistics() = 0;
+        virtual void* stream() = 0;
+};
+
+class Scene
+{
+public:
+        virtual ~Scene() = default;
+
+        virtual int dimension() const = 0;
+        virtual int channels() const = 0;
+        virtual bool double_precision() const = 0;
+
+        virtual int add_hyperplane_parallelotope(double metalness, double roughness, const float* rgb, double alpha,
+                                                 const double* org, const double* vectors) = 0;
+        virtual int add_parallelotope(double metalness, double roughness, const float* rgb, double alpha,
+                                      const double* org, const double* vectors) = 0;
+        virtual int add_mesh_object(const float* points, long long point_count, const int* facets,
+                                    long long facet_count, const double* matrix, const float* normals,
+                                    float metalness, float roughness, const float* rgb, float alpha) = 0;
+        virtual int add_mesh() = 0;
+        virtual int add_mesh_data(long long vertex_count, const double* vertices, const double* normals,
+                                  long long facet_count, const int* facets, const int* facet_materials,
+                                  int material_count, const double* material_params, const float* material_colors) = 0;
+        virtual int add_parallelotope_light(int shape, const double* direction, const float* rgb) = 0;
+        virtual int add_ball_light(const double* center, const double* direction, double radius, const float* rgb) = 0;
+        virtual void set_perspective_projector(const double* org, const double* dir, const double* axes,
+                                               double fov_degrees, const int* size) = 0;
+        virtual void set_parallel_projector(const double* org, const double* dir, const double* axes,
+                                            double units_per_pixel, const int* size) = 0;
+        virtual void set_background(const float* rgb) = 0;
+        virtual void finalize() = 0;
+
+        virtual long long pixel_count() const = 0;
+        virtual int actual_spp(int samples_per_pixel) const = 0;
+        virtual long long device_bytes() const = 0;
+
+        virtual std::unique_ptr<Painter> create_painter(int samples_per_pixel, int max_depth, std::uint32_t seed) = 0;
+
+        // verification: closest hit (any == 0) or any hit of rays [n][2N]
+        virtual void trace(const double* rays, long long count, int any, int* kind, int* index, double* t,
+                           double* point) = 0;
+        virtual void mesh_export(int mesh, long long* counts, double* planes, double* node_lo, double* node_hi,
+                                 unsigned* node_info, unsigned* indices, int* normal_info) = 0;
+        virtual void brdf(int material, const double* n, const double* v, const double* l, float* f,
+                          double* pdf) = 0;
+        virtual void brdf_sample(int material, const double* n, const double* v, const std::uint32_t* seed,
+                                 int seed_words, double* l, double* pdf, float* f) = 0;
+        virtual void light_sample(int light, int kind, const std::uint32_t* seed, int seed_words,
+                                  const double* point, double* out, float* radiance) = 0;
+};
+
+std::unique_ptr<Scene> make_scene_3(bool double_precision, bool spectrum);
+std::unique_ptr<Scene> make_scene_4(bool double_precision, bool spectrum);
+std::unique_ptr<Scene> make_scene_5(bool double_precision, bool spectrum);
+
+// random-number kernels for verification (capi.cpp)
+void test_pcg(const std::uint32_t* seed, int seed_words, int count, std::uint32_t* out);
+void test_canonical(const std::uint32_t* seed, int seed_words, int count, int use_double, double* out);
+int test_sj_points(int dimension, int use_double, int spp, const std::uint32_t* seed, int seed_words, double* out);
+} // namespace nbpt

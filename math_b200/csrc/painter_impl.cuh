@@ -1,0 +1,1761 @@
+// Templated scene and painter implementation (one instantiation per space
+// dimension N, path precision T and colour channel count C).
+//
+// Scene preparation (host): shapes, meshes, lights and the projector are
+// turned into the device records of scene.cuh with the reference's
+// arithmetic (src/painter/shapes/*.cpp, lights/*.cpp, projectors/*.cpp,
+// shapes/mesh/data.cpp); the mesh BVH is built on the host (bvh_build.cpp)
+// and the facet records in double precision on the GPU (facet_setup_kernel).
+//
+// Painter: one pass renders every pixel's stratified samples through the path
+// kernel and folds them into the per-pixel estimator on the device.
+#pragma once
+
+#include "bvh_build.h"
+#include "estimator.cuh"
+#include "host_math.h"
+#include "kernels.cuh"
+#include "painter_api.h"
+#include "tables.inc"
+
+#include <cuda_runtime.h>
+
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+namespace nbpt
+{
+inline void cuda_check(const cudaError_t e, const char* what)
+{
+        if (e != cudaSuccess)
+        {
+                throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+        }
+}
+
+#define NBPT_CUDA(x) ::nbpt::cuda_check((x), #x)
+
+template <typename X>
+class DeviceArray final
+{
+        X* ptr_ = nullptr;
+        std::size_t size_ = 0;
+
+public:
+        DeviceArray() = default;
+        DeviceArray(const DeviceArray&) = delete;
+        DeviceArray& operator=(const DeviceArray&) = delete;
+
+        ~DeviceArray()
+        {
+                if (ptr_)
+                {
+                        cudaFree(ptr_);
+                }
+        }
+
+        void allocate(const std::size_t n)
+        {
+                if (ptr_)
+                {
+                        cudaFree(ptr_);
+                        ptr_ = nullptr;
+                }
+                size_ = n;
+                if (n > 0)
+                {
+                        NBPT_CUDA(cudaMalloc(&ptr_, n * sizeof(X)));
+                }
+        }
+
+        void upload(const std::vector<X>& v)
+        {
+                allocate(v.size());
+                if (!v.empty())
+                {
+                        NBPT_CUDA(cudaMemcpy(ptr_, v.data(), v.size() * sizeof(X), cudaMemcpyHostToDevice));
+                }
+        }
+
+        void upload(const X* data, const std::size_t n)
+        {
+                allocate(n);
+                if (n > 0)
+                {
+                        NBPT_CUDA(cudaMemcpy(ptr_, data, n * sizeof(X), cudaMemcpyHostToDevice));
+                }
+        }
+
+        void download(X* out, const std::size_t n) const
+        {
+                if (n > 0)
+                {
+                        NBPT_CUDA(cudaMemcpy(out, ptr_, n * sizeof(X), cudaMemcpyDeviceToHost));
+                }
+        }
+
+        [[nodiscard]] X* get() const
+        {
+                return ptr_;
+        }
+
+        [[nodiscard]] std::size_t size() const
+        {
+                return size_;
+        }
+
+        [[nodiscard]] std::size_t bytes() const
+        {
+                return size_ * sizeof(X);
+        }
+};
+
+inline unsigned blocks_for(const long long n, const int threads)
+{
+        return static_cast<unsigned>((n + threads - 1) / threads);
+}
+
+template <int N, typename T>
+NBPT_HD Vec<N, T> to_vec(const double* p)
+{
+        Vec<N, T> v;
+        for (int i = 0; i < N; ++i)
+        {
+                v[i] = static_cast<T>(p[i]);
+        }
+        return v;
+}
+
+// Gauss-Jordan inverse with partial pivoting of an M x M matrix in T.
+template <int M, typename T>
+std::array<T, M * M> inverse(std::array<T, M * M> a)
+{
+        std::array<T, M * M> b{};
+        for (int i = 0; i < M; ++i)
+        {
+                b[i * M + i] = 1;
+        }
+        for (int c = 0; c < M; ++c)
+        {
+                int pivot = c;
+                for (int r = c + 1; r < M; ++r)
+                {
+                        if (abs_value(a[r * M + c]) > abs_value(a[pivot * M + c]))
+                        {
+                                pivot = r;
+                        }
+                }
+                if (a[pivot * M + c] == 0)
+                {
+                        throw std::runtime_error("mesh matrix is singular");
+                }
+                if (pivot != c)
+                {
+                        for (int k = 0; k < M; ++k)
+                        {
+                                std::swap(a[c * M + k], a[pivot * M + k]);
+                                std::swap(b[c * M + k], b[pivot * M + k]);
+                        }
+                }
+                const T d = a[c * M + c];
+                for (int k = 0; k < M; ++k)
+                {
+                        a[c * M + k] /= d;
+                        b[c * M + k] /= d;
+                }
+                for (int r = 0; r < M; ++r)
+                {
+                        if (r == c)
+                        {
+                                continue;
+                        }
+                        const T f = a[r * M + c];
+                        if (f == 0)
+                        {
+                                continue;
+                        }
+                        for (int k = 0; k < M; ++k)
+                        {
+                                a[r * M + k] -= f * a[c * M + k];
+                                b[r * M + k] -= f * b[c * M + k];
+                        }
+                }
+        }
+        return b;
+}
+
+// Vertex normals of a simplex mesh: per vertex, the facet normals around it
+// weighted by the facet's solid angle at the vertex (n = 3, 4) or 1
+// (n >= 5), oriented consistently and averaged
+// (after src/model/mesh/normals.cpp:46-195).
+template <int N>
+std::vector<float> vertex_normals(const std::vector<float>& points, const std::vector<int>& facets)
+{
+        const std::size_t vcount = points.size() / N;
+        const std::size_t fcount = facets.size() / N;
+        std::vector<Vec<N, double>> fn(fcount);
+        for (std::size_t f = 0; f < fcount; ++f)
+        {
+                Vec<N, double> e[N - 1];
+                const int i0 = facets[f * N];
+                for (int k = 0; k < N - 1; ++k)
+                {
+                        for (int d = 0; d < N; ++d)
+                        {
+                                e[k][d] = static_cast<double>(points[facets[f * N + k + 1] * static_cast<std::size_t>(N) + d]) -
+                                          static_cast<double>(points[i0 * static_cast<std::size_t>(N) + d]);
+                        }
+                }
+                fn[f] = orthogonal_complement(e).normalized();
+        }
+        std::vector<Vec<N, double>> sum(vcount, Vec<N, double>::filled(0));
+        std::vector<Vec<N, double>> reference(vcount, Vec<N, double>::filled(0));
+        std::vector<char> has_reference(vcount, 0);
+        for (std::size_t f = 0; f < fcount; ++f)
+        {
+                for (int k = 0; k < N; ++k)
+                {
+                        const int v = facets[f * N + k];
+                        double w = 1;
+                        if constexpr (N == 3 || N == 4)
+                        {
+                                Vec<N, double> a[N - 1];
+                                for (int j = 0; j < N - 1; ++j)
+                                {
+                                        const int o = facets[f * N + (k + 1 + j) % N];
+                                        for (int d = 0; d < N; ++d)
+                                        {
+                                                a[j][d] = static_cast<double>(points[o * static_cast<std::size_t>(N) + d]) -
+                                                          static_cast<double>(points[v * static_cast<std::size_t>(N) + d]);
+                                        }
+                                        a[j] = a[j].normalized();
+                                }
+                                if constexpr (N == 3)
+                                {
+                                        w = std::acos(std::fmax(-1.0, std::fmin(1.0, dot(a[0], a[1]))));
+                                }
+                                else
+                                {
+                                        // solid angle of the spherical triangle (Van Oosterom-Strackee)
+                                        const Vec<3, double> p{{a[0][0], a[0][1], a[0][2]}};
+                                        (void)p;
+                                        Vec<N, double> c3[N - 1] = {a[0], a[1], a[2]};
+                                        Vec<N, double> n4 = orthogonal_complement(c3);
+                                        // |det| of the three unit vectors within their 3-space: the
+                                        // norm of their orthogonal complement
+                                        const double det = n4.norm();
+                                        const double d01 = dot(a[0], a[1]);
+                                        const double d02 = dot(a[0], a[2]);
+                                        const double d12 = dot(a[1], a[2]);
+                                        w = 2 * std::atan2(det, 1 + d01 + d02 + d12);
+                                }
+                        }
+                        if (!has_reference[v])
+                        {
+                                reference[v] = fn[f];
+                                has_reference[v] = 1;
+                        }
+                        const Vec<N, double> wn = fn[f] * w;
+                        if (dot(fn[f], reference[v]) >= 0)
+                        {
+                                sum[v] = sum[v] + wn;
+                        }
+                        else
+                        {
+                                sum[v] = sum[v] - wn;
+                        }
+                }
+        }
+        std::vector<float> out(vcount * N, 0.0f);
+        for (std::size_t v = 0; v < vcount; ++v)
+        {
+                if (!has_reference[v])
+                {
+                        continue;
+                }
+                const Vec<N, double> n = sum[v].normalized();
+                for (int d = 0; d < N; ++d)
+                {
+                        out[v * N + d] = static_cast<float>(n[d]);
+                }
+        }
+        return out;
+}
+
+// ---------------------------------------------------------------------------
+
+template <int N, typename T, int C>
+class PainterT;
+
+template <int N, typename T, int C>
+class SceneT final : public Scene
+{
+        friend class PainterT<N, T, C>;
+
+        enum class ShapeKind
+        {
+                FLAT,
+                SOLID,
+                MESH
+        };
+
+        struct ShapeRef final
+        {
+                ShapeKind kind;
+                int index;
+        };
+
+        struct FlatHost final
+        {
+                Vec<N, T> org;
+                Vec<N, T> vectors[N - 1];
+        };
+
+        struct MeshObjectHost final
+        {
+                std::vector<float> points;
+                std::vector<int> facets;
+                std::array<double, (N + 1) * (N + 1)> matrix;
+                std::vector<float> normals;
+                float metalness;
+                float roughness;
+                float alpha;
+                float rgb[3];
+        };
+
+        struct MeshHost final
+        {
+                std::vector<T> vertices; // [V][N]
+                std::vector<T> normals;  // [V][N] or empty
+                std::vector<int> facets;
+                std::vector<int> facet_materials;
+                host::BuiltBvh<N, T> bvh;
+                int facet_offset = 0;
+                int node_offset = 0;
+                int index_offset = 0;
+                int vertex_offset = 0;
+        };
+
+        std::vector<ShapeRef> shapes_;
+        std::vector<FlatShape<N, T>> flat_;
+        std::vector<FlatHost> flat_host_;
+        std::vector<SolidShape<N, T>> solid_;
+        std::vector<Material<T, C>> materials_;
+        std::vector<MeshObjectHost> pending_;
+        std::vector<MeshHost> meshes_;
+        std::vector<Light<N, T, C>> lights_;
+        Projector<N, T> projector_{};
+        bool has_projector_ = false;
+        bool finalized_ = false;
+
+        DeviceArray<FlatShape<N, T>> d_flat_;
+        DeviceArray<SolidShape<N, T>> d_solid_;
+        DeviceArray<MeshShape<N, T>> d_meshes_;
+        DeviceArray<BvhNode<N, T>> d_nodes_;
+        DeviceArray<std::uint32_t> d_indices_;
+        DeviceArray<Facet<N, T>> d_facets_;
+        DeviceArray<Vec<N, T>> d_normals_;
+        DeviceArray<Material<T, C>> d_materials_;
+        DeviceArray<Light<N, T, C>> d_lights_;
+        DeviceArray<T> d_f1_albedo_;
+        DeviceArray<T> d_f1_average_;
+        DeviceArray<float> d_cie_; // x, y, z colour matching functions
+        std::vector<MeshShape<N, T>> mesh_records_;
+        long long facet_total_ = 0;
+        long long node_total_ = 0;
+
+        DeviceScene<N, T, C> device_{};
+
+        void check_open() const
+        {
+                if (finalized_)
+                {
+                        throw std::runtime_error("the scene is finalized");
+                }
+        }
+
+        int add_material(const std::vector<float>& color, const float metalness, const T roughness)
+        {
+                std::vector<float> f0;
+                std::vector<float> rho;
+                host::metalness_colors(color, metalness, f0, rho);
+                Material<T, C> m;
+                m.roughness = roughness;
+                for (int c = 0; c < C; ++c)
+                {
+                        m.f0.c[c] = f0[c];
+                        m.rho_ss.c[c] = rho[c];
+                }
+                materials_.push_back(m);
+                return static_cast<int>(materials_.size()) - 1;
+        }
+
+        static T clamp_t(const T v)
+        {
+                return (v < T(0)) ? T(0) : ((T(1) < v) ? T(1) : v);
+        }
+
+        std::vector<float> clamped_surface_color(const float* rgb) const
+        {
+                std::vector<float> c = host::surface_color(C, rgb);
+                for (float& v : c)
+                {
+                        v = host::clamp01(v);
+                }
+                return c;
+        }
+
+        Vec<N, T> box_lo(const Vec<N, T>* pts, const int count) const
+        {
+                Vec<N, T> r = pts[0];
+                for (int k = 1; k < count; ++k)
+                {
+                        for (int d = 0; d < N; ++d)
+                        {
+                                r[d] = (pts[k][d] < r[d]) ? pts[k][d] : r[d];
+                        }
+                }
+                return r;
+        }
+
+        Vec<N, T> box_hi(const Vec<N, T>* pts, const int count) const
+        {
+                Vec<N, T> r = pts[0];
+                for (int k = 1; k < count; ++k)
+                {
+                        for (int d = 0; d < N; ++d)
+                        {
+                                r[d] = (r[d] < pts[k][d]) ? pts[k][d] : r[d];
+                        }
+                }
+                return r;
+        }
+
+public:
+        int dimension() const override
+        {
+                return N;
+        }
+
+        int channels() const override
+        {
+                return C;
+        }
+
+        bool double_precision() const override
+        {
+                return std::is_same_v<T, double>;
+        }
+
+        // shapes/hyperplane_parallelotope.cpp:175-188
+        int add_hyperplane_parallelotope(
+                const double metalness,
+                const double roughness,
+                const float* rgb,
+                const double alpha,
+                const double* org,
+                const double* vectors) override
+        {
+                check_open();
+                (void)alpha;
+                FlatHost h;
+                h.org = to_vec<N, T>(org);
+                for (int i = 0; i < N - 1; ++i)
+                {
+                        h.vectors[i] = to_vec<N, T>(vectors + i * N);
+                }
+                FlatShape<N, T> s;
+                if (!s.shape.set(h.org, h.vectors))
+                {
+                        throw std::runtime_error("hyperplane parallelotope normal is not finite");
+                }
+                // bounding box of the 2^(N-1) vertices
+                Vec<N, T> pts[1 << (N - 1)];
+                for (int m = 0; m < (1 << (N - 1)); ++m)
+                {
+                        Vec<N, T> p = h.org;
+                        for (int i = 0; i < N - 1; ++i)
+                        {
+                                if ((m >> i) & 1)
+                                {
+                                        p = p + h.vectors[i];
+                                }
+                        }
+                        pts[m] = p;
+                }
+                const Vec<N, T> lo = box_lo(pts, 1 << (N - 1));
+                const Vec<N, T> hi = box_hi(pts, 1 << (N - 1));
+                for (int d = 0; d < N; ++d)
+                {
+                        s.lo[d] = lo[d];
+                        s.hi[d] = hi[d];
+                }
+                const T m = clamp_t(static_cast<T>(metalness));
+                s.material = add_material(clamped_surface_color(rgb), static_cast<float>(m),
+                                          clamp_t(static_cast<T>(roughness)));
+                s.light = -1;
+                flat_.push_back(s);
+                flat_host_.push_back(h);
+                shapes_.push_back({ShapeKind::FLAT, static_cast<int>(flat_.size()) - 1});
+                return static_cast<int>(shapes_.size()) - 1;
+        }
+
+        // shapes/parallelotope.cpp:174-187
+        int add_parallelotope(
+                const double metalness,
+                const double roughness,
+                const float* rgb,
+                const double alpha,
+                const double* org,
+                const double* vectors) override
+        {
+                check_open();
+                (void)alpha;
+                const Vec<N, T> o = to_vec<N, T>(org);
+                Vec<N, T> v[N];
+                for (int i = 0; i < N; ++i)
+                {
+                        v[i] = to_vec<N, T>(vectors + i * N);
+                }
+                SolidShape<N, T> s;
+                s.shape.set(o, v);
+                Vec<N, T> pts[1 << N];
+                for (int m = 0; m < (1 << N); ++m)
+                {
+                        Vec<N, T> p = o;
+                        for (int i = 0; i < N; ++i)
+                        {
+                                if ((m >> i) & 1)
+                                {
+                                        p = p + v[i];
+                                }
+                        }
+                        pts[m] = p;
+                }
+                const Vec<N, T> lo = box_lo(pts, 1 << N);
+                const Vec<N, T> hi = box_hi(pts, 1 << N);
+                for (int d = 0; d < N; ++d)
+                {
+                        s.lo[d] = lo[d];
+                        s.hi[d] = hi[d];
+                }
+                const T m = clamp_t(static_cast<T>(metalness));
+                s.material = add_material(clamped_surface_color(rgb), static_cast<float>(m),
+                                          clamp_t(static_cast<T>(roughness)));
+                solid_.push_back(s);
+                shapes_.push_back({ShapeKind::SOLID, static_cast<int>(solid_.size()) - 1});
+                return static_cast<int>(shapes_.size()) - 1;
+        }
+
+        int add_mesh_object(
+                const float* points,
+                const long long point_count,
+                const int* facets,
+                const long long facet_count,
+                const double* matrix,
+                const float* normals,
+                const float metalness,
+                const float roughness,
+                const float* rgb,
+                const float alpha) override
+        {
+                check_open();
+                if (point_count <= 0 || facet_count <= 0)
+                {
+                        throw std::runtime_error("No facets for facet object");
+                }
+                MeshObjectHost o;
+                o.points.assign(points, points + point_count * N);
+                o.facets.assign(facets, facets + facet_count * N);
+                for (const int i : o.facets)
+                {
+                        if (i < 0 || i >= point_count)
+                        {
+                                throw std::runtime_error("facet vertex index out of range");
+                        }
+                }
+                std::copy(matrix, matrix + (N + 1) * (N + 1), o.matrix.begin());
+                if (normals)
+                {
+                        o.normals.assign(normals, normals + point_count * N);
+                }
+                o.metalness = metalness;
+                o.roughness = roughness;
+                o.alpha = alpha;
+                std::copy(rgb, rgb + 3, o.rgb);
+                pending_.push_back(std::move(o));
+                return static_cast<int>(pending_.size()) - 1;
+        }
+
+        // shapes/mesh/data.cpp:88-310: transform the objects' vertices and
+        // normals, one material per object
+        int add_mesh() override
+        {
+                check_open();
+                if (pending_.empty())
+                {
+                        throw std::runtime_error("No objects to paint");
+                }
+                MeshHost mesh;
+                for (MeshObjectHost& o : pending_)
+                {
+                        const T alpha = clamp_t(static_cast<T>(o.alpha));
+                        if (alpha == 0)
+                        {
+                                continue;
+                        }
+                        const int vertex_offset = static_cast<int>(mesh.vertices.size() / N);
+                        const std::size_t vcount = o.points.size() / N;
+                        if (o.normals.empty())
+                        {
+                                o.normals = vertex_normals<N>(o.points, o.facets);
+                        }
+                        // vertices: M * (v, 1)  (numerical/transform.h:83-119)
+                        for (std::size_t v = 0; v < vcount; ++v)
+                        {
+                                for (int r = 0; r < N; ++r)
+                                {
+                                        T x = static_cast<T>(o.matrix[r * (N + 1) + 0]) * static_cast<T>(o.points[v * N + 0]);
+                                        for (int c = 1; c < N; ++c)
+                                        {
+                                                x += static_cast<T>(o.matrix[r * (N + 1) + c]) * static_cast<T>(o.points[v * N + c]);
+                                        }
+                                        x += static_cast<T>(o.matrix[r * (N + 1) + N]);
+                                        mesh.vertices.push_back(x);
+                                }
+                        }
+                        // normals: inverse transpose of the linear part
+                        std::array<T, N * N> lin;
+                        for (int r = 0; r < N; ++r)
+                        {
+                                for (int c = 0; c < N; ++c)
+                                {
+                                        lin[r * N + c] = static_cast<T>(o.matrix[r * (N + 1) + c]);
+                                }
+                        }
+                        const std::array<T, N * N> inv = inverse<N, T>(lin);
+                        for (std::size_t v = 0; v < vcount; ++v)
+                        {
+                                for (int r = 0; r < N; ++r)
+                                {
+                                        // row r of the transpose = column r of the inverse
+                                        T x = inv[0 * N + r] * static_cast<T>(o.normals[v * N + 0]);
+                                        for (int c = 1; c < N; ++c)
+                                        {
+                                                x += inv[c * N + r] * static_cast<T>(o.normals[v * N + c]);
+                                        }
+                                        mesh.normals.push_back(x);
+                                }
+                        }
+                        const int material = add_material(
+                                [&]
+                                {
+                                        std::vector<float> c = host::surface_color(C, o.rgb);
+                                        for (float& x : c)
+                                        {
+                                                x = host::clamp01(x);
+                                        }
+                                        return c;
+                                }(),
+                                static_cast<float>(clamp_t(static_cast<T>(o.metalness))),
+                                clamp_t(static_cast<T>(o.roughness)));
+                        for (const int i : o.facets)
+                        {
+                                mesh.facets.push_back(i + vertex_offset);
+                        }
+                        mesh.facet_materials.insert(mesh.facet_materials.end(), o.facets.size() / N, material);
+                }
+                pending_.clear();
+                if (mesh.facets.empty())
+                {
+                        throw std::runtime_error("No facets found in meshes");
+                }
+                meshes_.push_back(std::move(mesh));
+                shapes_.push_back({ShapeKind::MESH, static_cast<int>(meshes_.size()) - 1});
+                return static_cast<int>(shapes_.size()) - 1;
+        }
+
+        // A mesh given as the painter's mesh data (shapes/mesh/data.h:34-50):
+        // transformed vertices and normals, facet vertex indices, per-facet
+        // material index; material_params [metalness, roughness, alpha] and
+        // material_colors [C] per material.
+        int add_mesh_data(
+                const long long vertex_count,
+                const double* vertices,
+                const double* normals,
+                const long long facet_count,
+                const int* facets,
+                const int* facet_materials,
+                const int material_count,
+                const double* material_params,
+                const float* material_colors) override
+        {
+                check_open();
+                if (facet_count <= 0)
+                {
+                        throw std::runtime_error("No facets found in meshes");
+                }
+                MeshHost mesh;
+                mesh.vertices.resize(vertex_count * N);
+                for (long long i = 0; i < vertex_count * N; ++i)
+                {
+                        mesh.vertices[i] = static_cast<T>(vertices[i]);
+                }
+                if (normals)
+                {
+                        mesh.normals.resize(vertex_count * N);
+                        for (long long i = 0; i < vertex_count * N; ++i)
+                        {
+                                mesh.normals[i] = static_cast<T>(normals[i]);
+                        }
+                }
+                const int base = static_cast<int>(materials_.size());
+                for (int m = 0; m < material_count; ++m)
+                {
+                        std::vector<float> color(material_colors + m * C, material_colors + (m + 1) * C);
+                        add_material(color, static_cast<float>(static_cast<T>(material_params[m * 3 + 0])),
+                                     static_cast<T>(material_params[m * 3 + 1]));
+                }
+                mesh.facets.assign(facets, facets + facet_count * N);
+                for (const int i : mesh.facets)
+                {
+                        if (i < 0 || i >= vertex_count)
+                        {
+                                throw std::runtime_error("facet vertex index out of range");
+                        }
+                }
+                mesh.facet_materials.resize(facet_count);
+                for (long long f = 0; f < facet_count; ++f)
+                {
+                        if (facet_materials[f] < 0 || facet_materials[f] >= material_count)
+                        {
+                                throw std::runtime_error("facet material index out of range");
+                        }
+                        mesh.facet_materials[f] = base + facet_materials[f];
+                }
+                meshes_.push_back(std::move(mesh));
+                shapes_.push_back({ShapeKind::MESH, static_cast<int>(meshes_.size()) - 1});
+                return static_cast<int>(shapes_.size()) - 1;
+        }
+
+        // lights/parallelotope_light.cpp:183-193 (normal turned towards
+        // `direction`, pdf 1 / area)
+        int add_parallelotope_light(const int shape, const double* direction, const float* rgb) override
+        {
+                check_open();
+                if (shape < 0 || shape >= static_cast<int>(shapes_.size()) || shapes_[shape].kind != ShapeKind::FLAT)
+                {
+                        throw std::runtime_error("light carrier is not a hyperplane parallelotope");
+                }
+                const int fi = shapes_[shape].index;
+                const FlatHost& h = flat_host_[fi];
+                Light<N, T, C> l{};
+                l.type = static_cast<int>(LightType::PARALLELOTOPE);
+                l.org = h.org;
+                for (int i = 0; i < N - 1; ++i)
+                {
+                        l.vectors[i] = h.vectors[i];
+                }
+                l.normal = flat_[fi].shape.plane.n;
+                const Vec<N, T> dir = to_vec<N, T>(direction);
+                if (dot(l.normal, dir) < 0)
+                {
+                        l.normal = -l.normal;
+                }
+                Vec<N, T> vv[N - 1];
+                for (int i = 0; i < N - 1; ++i)
+                {
+                        vv[i] = h.vectors[i];
+                }
+                l.pdf = 1 / orthogonal_complement(vv).norm();
+                const std::vector<float> rad = host::illuminant_color(C, rgb);
+                for (int c = 0; c < C; ++c)
+                {
+                        l.radiance.c[c] = rad[c];
+                }
+                lights_.push_back(l);
+                flat_[fi].light = static_cast<int>(lights_.size()) - 1;
+                return static_cast<int>(lights_.size()) - 1;
+        }
+
+        // lights/ball_light.cpp:181-202
+        int add_ball_light(const double* center, const double* direction, const double radius, const float* rgb) override
+        {
+                check_open();
+                const T r = static_cast<T>(radius);
+                if (!(r > 0))
+                {
+                        throw std::runtime_error("Ball light radius must be positive");
+                }
+                Light<N, T, C> l{};
+                l.type = static_cast<int>(LightType::BALL);
+                l.org = to_vec<N, T>(center);
+                l.normal = to_vec<N, T>(direction).normalized();
+                orthogonal_complement_of_unit_vector(l.normal, l.vectors);
+                for (int i = 0; i < N - 1; ++i)
+                {
+                        for (int d = 0; d < N; ++d)
+                        {
+                                l.vectors[i][d] *= r;
+                        }
+                }
+                const T pdf_unit = static_cast<T>(1 / host::ball_volume(N - 1));
+                l.pdf = pdf_unit / power<N - 1>(r);
+                const std::vector<float> rad = host::illuminant_color(C, rgb);
+                for (int c = 0; c < C; ++c)
+                {
+                        l.radiance.c[c] = rad[c];
+                }
+                lights_.push_back(l);
+                return static_cast<int>(lights_.size()) - 1;
+        }
+
+        // projectors/perspective_projector.cpp:37-90
+        void set_perspective_projector(
+                const double* org,
+                const double* dir,
+                const double* axes,
+                const double fov_degrees,
+                const int* size) override
+        {
+                check_open();
+                const T fov = static_cast<T>(fov_degrees);
+                if (!(fov > 0 && fov < 180))
+                {
+                        throw std::runtime_error("Perspective projection: error view angle");
+                }
+                Projector<N, T> p{};
+                p.type = static_cast<int>(ProjectorType::PERSPECTIVE);
+                p.org = to_vec<N, T>(org);
+                for (int i = 0; i < N - 1; ++i)
+                {
+                        if (size[i] < 1)
+                        {
+                                throw std::runtime_error("Screen size is not positive");
+                        }
+                        p.size[i] = size[i];
+                        p.axes[i] = to_vec<N, T>(axes + i * N).normalized();
+                        p.screen_org[i] = static_cast<T>(-size[i]) * (static_cast<T>(1) / 2);
+                }
+                const T pi = static_cast<T>(host::PI_L);
+                const T half_angle = (fov * T(0.5)) * (pi / 180);
+                const T dir_length = static_cast<T>(size[0]) * T(0.5) * std::tan(pi / 2 - half_angle);
+                p.dir = to_vec<N, T>(dir).normalized() * dir_length;
+                projector_ = p;
+                has_projector_ = true;
+        }
+
+        // projectors/parallel_projector.cpp:35-88
+        void set_parallel_projector(
+                const double* org,
+                const double* dir,
+                const double* axes,
+                const double units_per_pixel,
+                const int* size) override
+        {
+                check_open();
+                const T u = static_cast<T>(units_per_pixel);
+                if (!(u > 0))
+                {
+                        throw std::runtime_error("Error units per pixel for parallel projection");
+                }
+                Projector<N, T> p{};
+                p.type = static_cast<int>(ProjectorType::PARALLEL);
+                p.org = to_vec<N, T>(org);
+                p.dir = to_vec<N, T>(dir).normalized();
+                for (int i = 0; i < N - 1; ++i)
+                {
+                        if (size[i] < 1)
+                        {
+                                throw std::runtime_error("Screen size is not positive");
+                        }
+                        p.size[i] = size[i];
+                        p.axes[i] = to_vec<N, T>(axes + i * N).normalized();
+                        for (int d = 0; d < N; ++d)
+                        {
+                                p.axes[i][d] *= u;
+                        }
+                        p.screen_org[i] = static_cast<T>(-size[i]) * (static_cast<T>(1) / 2);
+                }
+                projector_ = p;
+                has_projector_ = true;
+        }
+
+        void set_background(const float* rgb) override
+        {
+                check_open();
+                if (rgb[0] != 0 || rgb[1] != 0 || rgb[2] != 0)
+                {
+                        throw std::runtime_error(
+                                "non-black backgrounds (an infinite area light) are not supported by this painter");
+                }
+        }
+
+        void finalize() override
+        {
+                check_open();
+                if (!has_projector_)
+                {
+                        throw std::runtime_error("no projector");
+                }
+                if (lights_.empty())
+                {
+                        throw std::runtime_error("No light sources");
+                }
+                if (shapes_.empty())
+                {
+                        throw std::runtime_error("No objects to paint");
+                }
+                // light distribution: equal power (light_distribution.cpp:36-111)
+                {
+                        const int count = static_cast<int>(lights_.size());
+                        double cumulative = 0;
+                        for (int i = 0; i < count; ++i)
+                        {
+                                const double p = 1.0 / static_cast<double>(count);
+                                lights_[i].distribution_pdf = static_cast<T>(p);
+                                cumulative += p;
+                                lights_[i].cumulative = (i == count - 1) ? 1.0 : cumulative;
+                        }
+                }
+
+                // meshes: BVH on the host, facet records on the GPU
+                std::vector<BvhNode<N, T>> nodes;
+                std::vector<std::uint32_t> indices;
+                std::vector<double> all_vertices;
+                std::vector<T> all_normals;
+                std::vector<int> all_facets;
+                std::vector<int> all_materials;
+                bool any_normals = false;
+                for (const MeshHost& m : meshes_)
+                {
+                        any_normals = any_normals || !m.normals.empty();
+                }
+                for (MeshHost& m : meshes_)
+                {
+                        m.bvh = host::build_facet_bvh<N, T>(m.vertices, m.facets);
+                        m.facet_offset = static_cast<int>(all_facets.size() / N);
+                        m.node_offset = static_cast<int>(nodes.size());
+                        m.index_offset = static_cast<int>(indices.size());
+                        m.vertex_offset = static_cast<int>(all_vertices.size() / N);
+                        const std::size_t node_count = m.bvh.count.size();
+                        for (std::size_t i = 0; i < node_count; ++i)
+                        {
+                                BvhNode<N, T> b;
+                                for (int d = 0; d < N; ++d)
+                                {
+                                        b.lo[d] = m.bvh.lo[i * N + d];
+                                        b.hi[d] = m.bvh.hi[i * N + d];
+                                }
+                                b.offset = m.bvh.offset[i];
+                                b.count = static_cast<std::uint16_t>(m.bvh.count[i]);
+                                b.axis = static_cast<std::uint16_t>(m.bvh.axis[i]);
+                                if (m.bvh.count[i] > 0xffff)
+                                {
+                                        throw std::runtime_error("BVH leaf too large");
+                                }
+                                nodes.push_back(b);
+                        }
+                        indices.insert(indices.end(), m.bvh.indices.begin(), m.bvh.indices.end());
+                        for (const T v : m.vertices)
+                        {
+                                all_vertices.push_back(static_cast<double>(v));
+                        }
+                        const std::size_t vcount = m.vertices.size() / N;
+                        if (any_normals)
+                        {
+                                if (m.normals.empty())
+                                {
+                                        all_normals.insert(all_normals.end(), vcount * N, T(0));
+                                }
+                                else
+                                {
+                                        all_normals.insert(all_normals.end(), m.normals.begin(), m.normals.end());
+                                }
+                        }
+                        const int vo = m.vertex_offset;
+                        for (const int f : m.facets)
+                        {
+                                all_facets.push_back(f + vo);
+                        }
+                        all_materials.insert(all_materials.end(), m.facet_materials.begin(), m.facet_materials.end());
+                        MeshShape<N, T> rec;
+                        for (int d = 0; d < N; ++d)
+                        {
+                                rec.lo[d] = m.bvh.lo[d];
+                                rec.hi[d] = m.bvh.hi[d];
+                        }
+                        rec.node_offset = m.node_offset;
+                        rec.index_offset = m.index_offset;
+                        rec.facet_offset = m.facet_offset;
+                        mesh_records_.push_back(rec);
+                }
+                facet_total_ = static_cast<long long>(all_facets.size() / N);
+                node_total_ = static_cast<long long>(nodes.size());
+
+                d_flat_.upload(flat_);
+                d_solid_.upload(solid_);
+                d_meshes_.upload(mesh_records_);
+                d_nodes_.upload(nodes);
+                d_indices_.upload(indices);
+                d_materials_.upload(materials_);
+                d_lights_.upload(lights_);
+
+                if (facet_total_ > 0)
+                {
+                        DeviceArray<double> dv;
+                        dv.upload(all_vertices);
+                        DeviceArray<double> dn;
+                        std::vector<double> normals_double(all_normals.begin(), all_normals.end());
+                        if (any_normals)
+                        {
+                                dn.upload(normals_double);
+                        }
+                        DeviceArray<int> df;
+                        df.upload(all_facets);
+                        DeviceArray<int> dm;
+                        dm.upload(all_materials);
+                        DeviceArray<int> derr;
+                        std::vector<int> zero(1, 0);
+                        derr.upload(zero);
+                        d_facets_.allocate(facet_total_);
+                        facet_setup_kernel<N, T><<<blocks_for(facet_total_, 128), 128>>>(
+                                dv.get(), any_normals ? dn.get() : nullptr, df.get(), dm.get(), facet_total_,
+                                d_facets_.get(), derr.get());
+                        NBPT_CUDA(cudaGetLastError());
+                        NBPT_CUDA(cudaDeviceSynchronize());
+                        int err = 0;
+                        derr.download(&err, 1);
+                        if (err)
+                        {
+                                throw std::runtime_error("Hyperplane simplex normal is not finite");
+                        }
+                        if (any_normals)
+                        {
+                                std::vector<Vec<N, T>> nv(all_normals.size() / N);
+                                for (std::size_t i = 0; i < nv.size(); ++i)
+                                {
+                                        for (int d = 0; d < N; ++d)
+                                        {
+                                                nv[i][d] = all_normals[i * N + d];
+                                        }
+                                }
+                                d_normals_.upload(nv);
+                        }
+                }
+
+                // shading constants and tables
+                std::vector<T> f1(1024);
+                std::vector<T> f1a(32);
+                for (int i = 0; i < 1024; ++i)
+                {
+                        if constexpr (std::is_same_v<T, double>)
+                        {
+                                f1[i] = N == 3 ? tables::F1_ALBEDO_3_D[i] : (N == 4 ? tables::F1_ALBEDO_4_D[i] : tables::F1_ALBEDO_5_D[i]);
+                        }
+                        else
+                        {
+                                f1[i] = N == 3 ? tables::F1_ALBEDO_3_F[i] : (N == 4 ? tables::F1_ALBEDO_4_F[i] : tables::F1_ALBEDO_5_F[i]);
+                        }
+                }
+                for (int i = 0; i < 32; ++i)
+                {
+                        if constexpr (std::is_same_v<T, double>)
+                        {
+                                f1a[i] = N == 3 ? tables::F1_AVERAGE_3_D[i] : (N == 4 ? tables::F1_AVERAGE_4_D[i] : tables::F1_AVERAGE_5_D[i]);
+                        }
+                        else
+                        {
+                                f1a[i] = N == 3 ? tables::F1_AVERAGE_3_F[i] : (N == 4 ? tables::F1_AVERAGE_4_F[i] : tables::F1_AVERAGE_5_F[i]);
+                        }
+                }
+                d_f1_albedo_.upload(f1);
+                d_f1_average_.upload(f1a);
+                std::vector<float> cie;
+                for (int r = 0; r < 3; ++r)
+                {
+                        const std::vector<float>& row = host::spectrum_row(r);
+                        cie.insert(cie.end(), row.begin(), row.end());
+                }
+                d_cie_.upload(cie);
+
+                device_.flat = d_flat_.get();
+                device_.flat_count = static_cast<int>(flat_.size());
+                device_.solid = d_solid_.get();
+                device_.solid_count = static_cast<int>(solid_.size());
+                device_.meshes = d_meshes_.get();
+                device_.mesh_count = static_cast<int>(mesh_records_.size());
+                device_.nodes = d_nodes_.get();
+                device_.indices = d_indices_.get();
+                device_.facets = d_facets_.get();
+                device_.normals = d_normals_.get();
+                device_.materials = d_materials_.get();
+                device_.lights = d_lights_.get();
+                device_.light_count = static_cast<int>(lights_.size());
+                device_.projector = projector_;
+                const long double k = host::hemisphere_cosine_integral(N);
+                device_.shading.k = static_cast<T>(k);
+                device_.shading.k_inv = static_cast<T>(1 / k);
+                device_.shading.ball_pdf = static_cast<T>(1 / host::ball_volume(N - 1));
+                const std::array<float, 2> fa = host::fresnel_average(N);
+                device_.shading.fresnel_a = fa[0];
+                device_.shading.fresnel_b = fa[1];
+                device_.shading.f1_albedo = d_f1_albedo_.get();
+                device_.shading.f1_average = d_f1_average_.get();
+                finalized_ = true;
+        }
+
+        long long pixel_count() const override
+        {
+                if (!has_projector_)
+                {
+                        throw std::runtime_error("no projector");
+                }
+                long long r = 1;
+                for (int i = 0; i < N - 1; ++i)
+                {
+                        r *= projector_.size[i];
+                }
+                return r;
+        }
+
+        // strata per screen dimension (sj_sampler.h:51-73)
+        static int strata(const int spp)
+        {
+                if (spp < 1)
+                {
+                        throw std::runtime_error("Painter samples per pixel must be greater than 0");
+                }
+                const double v = std::pow(spp, 1.0 / (N - 1));
+                const unsigned f = static_cast<unsigned>(std::floor(v));
+                unsigned p = 1;
+                for (int i = 0; i < N - 1; ++i)
+                {
+                        p *= f;
+                }
+                if (p >= static_cast<unsigned>(spp))
+                {
+                        return static_cast<int>(f);
+                }
+                const unsigned c = static_cast<unsigned>(std::ceil(v));
+                return static_cast<int>(c);
+        }
+
+        int actual_spp(const int spp) const override
+        {
+                const int k = strata(spp);
+                int r = 1;
+                for (int i = 0; i < N - 1; ++i)
+                {
+                        r *= k;
+                }
+                return r;
+        }
+
+        long long device_bytes() const override
+        {
+                return static_cast<long long>(d_flat_.bytes() + d_solid_.bytes() + d_meshes_.bytes() + d_nodes_.bytes() +
+                                              d_indices_.bytes() + d_facets_.bytes() + d_normals_.bytes() +
+                                              d_materials_.bytes() + d_lights_.bytes());
+        }
+
+        const DeviceScene<N, T, C>& device() const
+        {
+                if (!finalized_)
+                {
+                        throw std::runtime_error("the scene is not finalized");
+                }
+                return device_;
+        }
+
+        const float* cie() const
+        {
+                return d_cie_.get();
+        }
+
+        std::unique_ptr<Painter> create_painter(int spp, int max_depth, std::uint32_t seed) override;
+
+        void trace(const double* rays, long long count, int any, int* kind, int* index, double* t, double* point) override;
+        void mesh_export(int mesh, long long* counts, double* planes, double* node_lo, double* node_hi,
+                         unsigned* node_info, unsigned* indices, int* normal_info) override;
+        void brdf(int material, const double* n, const double* v, const double* l, float* f, double* pdf) override;
+        void brdf_sample(int material, const double* n, const double* v, const std::uint32_t* seed, int seed_words,
+                         double* l, double* pdf, float* f) override;
+        void light_sample(int light, int kind, const std::uint32_t* seed, int seed_words, const double* point,
+                          double* out, float* radiance) override;
+};
+
+// ---------------------------------------------------------------------------
+// verification kernels
+
+template <int N, typename T, int C>
+__global__ void trace_kernel(
+        const DeviceScene<N, T, C> scene,
+        const double* __restrict__ rays,
+        const long long count,
+        const int any,
+        int* __restrict__ kind,
+        int* __restrict__ index,
+        double* __restrict__ t,
+        double* __restrict__ point)
+{
+        const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+        if (i >= count)
+        {
+                return;
+        }
+        Vec<N, T> o;
+        Vec<N, T> d;
+        for (int k = 0; k < N; ++k)
+        {
+                o[k] = static_cast<T>(rays[i * 2 * N + k]);
+                d[k] = static_cast<T>(rays[i * 2 * N + N + k]);
+        }
+        const Ray<N, T> ray = Ray<N, T>::make(o, d);
+        QueryCounters counters{0, 0, 0, 0};
+        const SceneQueries<N, T, C> q{scene, counters};
+        if (any)
+        {
+                kind[i] = q.intersect_any(nullptr, ray, infinity<T>()) ? 1 : 0;
+                return;
+        }
+        const Hit<N, T> h = q.intersect(nullptr, ray, infinity<T>());
+        kind[i] = h.kind;
+        index[i] = h.index;
+        t[i] = h ? static_cast<double>(h.distance) : 0.0;
+        for (int k = 0; k < N; ++k)
+        {
+                point[i * N + k] = h ? static_cast<double>(h.point[k]) : 0.0;
+        }
+}
+
+template <int N, typename T, int C>
+__global__ void brdf_kernel(
+        const DeviceScene<N, T, C> scene,
+        const int material,
+        const double* in, // n, v, l
+        float* f,
+        double* pdf)
+{
+        const Vec<N, T> n = to_vec<N, T>(in);
+        const Vec<N, T> v = to_vec<N, T>(in + N);
+        const Vec<N, T> l = to_vec<N, T>(in + 2 * N);
+        const Material<T, C>& m = scene.materials[material];
+        const Color<C> c = brdf_f(scene.shading, m.roughness, m.f0, m.rho_ss, n, v, l);
+        for (int k = 0; k < C; ++k)
+        {
+                f[k] = c.c[k];
+        }
+        *pdf = static_cast<double>(brdf_pdf(scene.shading, m.roughness, n, v, l));
+}
+
+template <int N, typename T, int C>
+__global__ void brdf_sample_kernel(
+        const DeviceScene<N, T, C> scene,
+        const int material,
+        const double* in, // n, v
+        const std::uint32_t* seed,
+        const int seed_words,
+        double* l,
+        double* pdf,
+        float* f)
+{
+        const Vec<N, T> n = to_vec<N, T>(in);
+        const Vec<N, T> v = to_vec<N, T>(in + N);
+        const Material<T, C>& m = scene.materials[material];
+        Pcg g = seed_seq_pcg(seed, seed_words);
+        const BrdfSample<N, C, T> s = brdf_sample<N>(g, scene.shading, m.roughness, m.f0, m.rho_ss, n, v);
+        *pdf = static_cast<double>(s.pdf);
+        if (s.pdf > 0)
+        {
+                for (int k = 0; k < N; ++k)
+                {
+                        l[k] = static_cast<double>(s.l[k]);
+                }
+                for (int k = 0; k < C; ++k)
+                {
+                        f[k] = s.brdf.c[k];
+                }
+        }
+}
+
+// leave (kind 0): out = [org N, dir N, n N, pdf_pos, pdf_dir];
+// arrive (kind 1): out = [l N, pdf, distance or -1]
+template <int N, typename T, int C>
+__global__ void light_sample_kernel(
+        const DeviceScene<N, T, C> scene,
+        const int light,
+        const int kind,
+        const std::uint32_t* seed,
+        const int seed_words,
+        const double* point,
+        double* out,
+        float* radiance)
+{
+        Pcg g = seed_seq_pcg(seed, seed_words);
+        QueryCounters counters{0, 0, 0, 0};
+        const SceneQueries<N, T, C> q{scene, counters};
+        const Bpt<N, T, C> b{q, scene, g, 1};
+        const Light<N, T, C>& l = scene.lights[light];
+        if (kind == 0)
+        {
+                const LeaveSample<N, T, C> s = b.leave_sample(l);
+                for (int k = 0; k < N; ++k)
+                {
+                        out[k] = static_cast<double>(s.ray.org[k]);
+                        out[N + k] = static_cast<double>(s.ray.dir[k]);
+                        out[2 * N + k] = static_cast<double>(s.n[k]);
+                }
+                out[3 * N] = static_cast<double>(s.pdf_pos);
+                out[3 * N + 1] = static_cast<double>(s.pdf_dir);
+                for (int c = 0; c < C; ++c)
+                {
+                        radiance[c] = s.radiance.c[c];
+                }
+                return;
+        }
+        const ArriveSample<N, T, C> s = b.arrive_sample(l, to_vec<N, T>(point));
+        for (int k = 0; k < N; ++k)
+        {
+                out[k] = s.pdf > 0 ? static_cast<double>(s.l[k]) : 0.0;
+        }
+        out[N] = static_cast<double>(s.pdf);
+        out[N + 1] = s.pdf > 0 ? static_cast<double>(s.distance) : -1.0;
+        for (int c = 0; c < C; ++c)
+        {
+                radiance[c] = s.pdf > 0 ? s.radiance.c[c] : 0.0f;
+        }
+}
+
+// ---------------------------------------------------------------------------
+// painter: one render of one scene
+
+template <int N, typename T, int C>
+class PainterT final : public Painter
+{
+        const SceneT<N, T, C>* scene_;
+        int spp_request_;
+        int spp_;
+        int strata_;
+        int max_depth_;
+        std::uint32_t seed_;
+        long long pixels_;
+        long long pass_ = 0;
+        long long passes_done_ = 0;
+        cudaStream_t stream_ = nullptr;
+        cudaEvent_t ev_start_ = nullptr;
+        cudaEvent_t ev_paths_ = nullptr;
+        cudaEvent_t ev_paths_end_ = nullptr;
+        cudaEvent_t ev_end_ = nullptr;
+
+        DeviceArray<T> offsets_;
+        DeviceArray<T> points_;
+        DeviceArray<float> colors_;
+        DeviceArray<float> lum_;
+        DeviceArray<unsigned char> valid_;
+        DeviceArray<PixelState<C>> state_;
+        DeviceArray<PathStats> stats_;
+        DeviceArray<float> rgb_;
+        DeviceArray<float> rgba_;
+        Statistics statistics_{};
+
+public:
+        PainterT(const SceneT<N, T, C>* scene, const int spp, const int max_depth, const std::uint32_t seed)
+                : scene_(scene),
+                  spp_request_(spp),
+                  max_depth_(max_depth),
+                  seed_(seed)
+        {
+                if (spp < 1)
+                {
+                        throw std::runtime_error("Painter samples per pixel must be greater than 0");
+                }
+                if (max_depth < 1 || max_depth > MAX_PATH_VERTICES - 1)
+                {
+                        throw std::runtime_error("Painter maximum depth must be in [1, 8]");
+                }
+                scene_->device(); // throws if not finalized
+                strata_ = SceneT<N, T, C>::strata(spp);
+                spp_ = scene_->actual_spp(spp);
+                if (spp_ > MAX_GROUP)
+                {
+                        throw std::runtime_error(
+                                "Painter samples per pixel " + std::to_string(spp_) + " exceed the maximum "
+                                + std::to_string(MAX_GROUP) + " of one pass");
+                }
+                pixels_ = scene_->pixel_count();
+
+                // offsets of the strata (sj_sampler.h:75-114)
+                std::vector<T> offsets(strata_ + 1);
+                const T offset_size = (T(1) - T(0)) / static_cast<T>(strata_);
+                offsets[0] = 0;
+                for (int i = 1; i < strata_; ++i)
+                {
+                        offsets[i] = T(0) + static_cast<T>(i) * offset_size;
+                }
+                offsets[strata_] = 1;
+                offsets_.upload(offsets);
+
+                const long long samples = pixels_ * spp_;
+                points_.allocate(samples * (N - 1));
+                colors_.allocate(samples * C);
+                lum_.allocate(samples);
+                valid_.allocate(samples);
+                state_.allocate(pixels_);
+                stats_.allocate(1);
+                rgb_.allocate(pixels_ * 3);
+                rgba_.allocate(pixels_ * 4);
+
+                NBPT_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+                NBPT_CUDA(cudaEventCreate(&ev_start_));
+                NBPT_CUDA(cudaEventCreate(&ev_paths_));
+                NBPT_CUDA(cudaEventCreate(&ev_paths_end_));
+                NBPT_CUDA(cudaEventCreate(&ev_end_));
+                NBPT_CUDA(cudaMemsetAsync(state_.get(), 0, state_.bytes(), stream_));
+                statistics_.pixel_count = pixels_;
+        }
+
+        ~PainterT() override
+        {
+                if (stream_)
+                {
+                        cudaStreamSynchronize(stream_);
+                        cudaStreamDestroy(stream_);
+                }
+                for (cudaEvent_t e : {ev_start_, ev_paths_, ev_paths_end_, ev_end_})
+                {
+                        if (e)
+                        {
+                                cudaEventDestroy(e);
+                        }
+                }
+        }
+
+        void* stream() override
+        {
+                return stream_;
+        }
+
+        void enqueue_passes(const int passes) override
+        {
+                const DeviceScene<N, T, C>& scene = scene_->device();
+                for (int k = 0; k < passes; ++k)
+                {
+                        const std::uint32_t pass = static_cast<std::uint32_t>(pass_++);
+                        NBPT_CUDA(cudaMemsetAsync(stats_.get(), 0, sizeof(PathStats), stream_));
+                        NBPT_CUDA(cudaEventRecord(ev_start_, stream_));
+                        sj_points_kernel<N - 1, T><<<blocks_for(pixels_, 128), 128, 0, stream_>>>(
+                                0, pixels_, seed_, pass, strata_, offsets_.get(), points_.get());
+                        NBPT_CUDA(cudaGetLastError());
+                        NBPT_CUDA(cudaEventRecord(ev_paths_, stream_));
+                        const long long paths = pixels_ * spp_;
+                        paths_kernel<N, T, C><<<blocks_for(paths, 128), 128, 0, stream_>>>(
+                                scene, 0, pixels_, spp_, max_depth_, seed_, pass, points_.get(), colors_.get(),
+                                lum_.get(), valid_.get(), scene_->cie() + 64, stats_.get());
+                        NBPT_CUDA(cudaGetLastError());
+                        NBPT_CUDA(cudaEventRecord(ev_paths_end_, stream_));
+                        Screen<N> screen;
+                        for (int i = 0; i < N - 1; ++i)
+                        {
+                                screen.size[i] = scene.projector.size[i];
+                        }
+                        const T radius = T(1.5);
+                        const T width = radius / T(2.5);
+                        const T alpha = -1 / (2 * width * width);
+                        const T exp_radius = std::exp(alpha * radius * radius);
+                        accumulate_kernel<N, T, C><<<blocks_for(pixels_, 128), 128, 0, stream_>>>(
+                                screen, pixels_, spp_, points_.get(), colors_.get(), lum_.get(), valid_.get(), alpha,
+                                exp_radius, state_.get());
+                        NBPT_CUDA(cudaGetLastError());
+                        NBPT_CUDA(cudaEventRecord(ev_end_, stream_));
+                }
+                passes_done_ += passes;
+        }
+
+        void wait() override
+        {
+                NBPT_CUDA(cudaStreamSynchronize(stream_));
+                PathStats s{};
+                stats_.download(&s, 1);
+                float ms = 0;
+                float paths_ms = 0;
+                NBPT_CUDA(cudaEventElapsedTime(&ms, ev_start_, ev_end_));
+                NBPT_CUDA(cudaEventElapsedTime(&paths_ms, ev_paths_, ev_paths_end_));
+                statistics_.pass_number = passes_done_;
+                statistics_.ray_count = static_cast<long long>(s.queries);
+                statistics_.sample_count = pixels_ * spp_;
+                statistics_.previous_pass_duration = ms * 1e-3;
+                statistics_.paths_seconds = paths_ms * 1e-3;
+                statistics_.nodes = s.nodes;
+                statistics_.facets = s.facets;
+                statistics_.shapes = s.shapes;
+        }
+
+        void images(float* rgb, float* rgba) override
+        {
+                resolve_kernel<C><<<blocks_for(pixels_, 128), 128, 0, stream_>>>(
+                        pixels_, state_.get(), scene_->cie(), rgb_.get(), rgba_.get());
+                NBPT_CUDA(cudaGetLastError());
+                NBPT_CUDA(cudaStreamSynchronize(stream_));
+                if (rgb)
+                {
+                        rgb_.download(rgb, pixels_ * 3);
+                }
+                if (rgba)
+                {
+                        rgba_.download(rgba, pixels_ * 4);
+                }
+        }
+
+        void samples(double* points, float* colors, unsigned char* valid) override
+        {
+                NBPT_CUDA(cudaStreamSynchronize(stream_));
+                const long long samples = pixels_ * spp_;
+                if (points)
+                {
+                        std::vector<T> p(samples * (N - 1));
+                        points_.download(p.data(), p.size());
+                        for (std::size_t i = 0; i < p.size(); ++i)
+                        {
+                                points[i] = static_cast<double>(p[i]);
+                        }
+                }
+                if (colors)
+                {
+                        colors_.download(colors, samples * C);
+                }
+                if (valid)
+                {
+                        valid_.download(valid, samples);
+                }
+        }
+
+        Statistics statistics() override
+        {
+                return statistics_;
+        }
+};
+
+template <int N, typename T, int C>
+std::unique_ptr<Painter> SceneT<N, T, C>::create_painter(const int spp, const int max_depth, const std::uint32_t seed)
+{
+        return std::make_unique<PainterT<N, T, C>>(this, spp, max_depth, seed);
+}
+
+template <int N, typename T, int C>
+void SceneT<N, T, C>::trace(
+        const double* rays,
+        const long long count,
+        const int any,
+        int* kind,
+        int* index,
+        double* t,
+        double* point)
+{
+        const DeviceScene<N, T, C>& s = device();
+        DeviceArray<double> d_rays;
+        d_rays.upload(rays, count * 2 * N);
+        DeviceArray<int> d_kind;
+        d_kind.allocate(count);
+        DeviceArray<int> d_index;
+        d_index.allocate(count);
+        DeviceArray<double> d_t;
+        d_t.allocate(count);
+        DeviceArray<double> d_point;
+        d_point.allocate(count * N);
+        trace_kernel<N, T, C><<<blocks_for(count, 128), 128>>>(s, d_rays.get(), count, any, d_kind.get(), d_index.get(),
+                                                               d_t.get(), d_point.get());
+        NBPT_CUDA(cudaGetLastError());
+        NBPT_CUDA(cudaDeviceSynchronize());
+        d_kind.download(kind, count);
+        if (!any)
+        {
+                d_index.download(index, count);
+                d_t.download(t, count);
+                d_point.download(point, count * N);
+        }
+}
+
+// counts: facets, nodes, indices; planes [F][N][N+1]; node_lo/hi [nodes][N];
+// node_info [nodes][3] (offset, count, axis); normal_info [F][2] (type, reverse mask)
+template <int N, typename T, int C>
+void SceneT<N, T, C>::mesh_export(
+        const int mesh,
+        long long* counts,
+        double* planes,
+        double* node_lo,
+        double* node_hi,
+        unsigned* node_info,
+        unsigned* indices,
+        int* normal_info)
+{
+        device();
+        if (mesh < 0 || mesh >= static_cast<int>(meshes_.size()))
+        {
+                throw std::runtime_error("no such mesh");
+        }
+        const MeshHost& m = meshes_[mesh];
+        const long long facets = static_cast<long long>(m.facets.size() / N);
+        const long long nodes = static_cast<long long>(m.bvh.count.size());
+        counts[0] = facets;
+        counts[1] = nodes;
+        counts[2] = static_cast<long long>(m.bvh.indices.size());
+        if (!planes)
+        {
+                return;
+        }
+        std::vector<Facet<N, T>> f(facets);
+        NBPT_CUDA(cudaMemcpy(f.data(), d_facets_.get() + m.facet_offset, facets * sizeof(Facet<N, T>),
+                             cudaMemcpyDeviceToHost));
+        for (long long i = 0; i < facets; ++i)
+        {
+                double* out = planes + i * N * (N + 1);
+                for (int d = 0; d < N; ++d)
+                {
+                        out[d] = static_cast<double>(f[i].simplex.plane.n[d]);
+                }
+                out[N] = static_cast<double>(f[i].simplex.plane.d);
+                for (int j = 0; j < N - 1; ++j)
+                {
+                        for (int d = 0; d < N; ++d)
+                        {
+                                out[(j + 1) * (N + 1) + d] = static_cast<double>(f[i].simplex.planes[j].n[d]);
+                        }
+                        out[(j + 1) * (N + 1) + N] = static_cast<double>(f[i].simplex.planes[j].d);
+                }
+                normal_info[i * 2] = f[i].normal_type;
+                normal_info[i * 2 + 1] = static_cast<int>(f[i].reverse_mask);
+        }
+        for (long long i = 0; i < nodes; ++i)
+        {
+                for (int d = 0; d < N; ++d)
+                {
+                        node_lo[i * N + d] = static_cast<double>(m.bvh.lo[i * N + d]);
+                        node_hi[i * N + d] = static_cast<double>(m.bvh.hi[i * N + d]);
+                }
+                node_info[i * 3] = m.bvh.offset[i];
+                node_info[i * 3 + 1] = m.bvh.count[i];
+                node_info[i * 3 + 2] = m.bvh.axis[i];
+        }
+        std::copy(m.bvh.indices.begin(), m.bvh.indices.end(), indices);
+}
+
+template <int N, typename T, int C>
+void SceneT<N, T, C>::brdf(const int material, const double* n, const double* v, const double* l, float* f, double* pdf)
+{
+        const DeviceScene<N, T, C>& s = device();
+        if (material < 0 || material >= static_cast<int>(materials_.size()))
+        {
+                throw std::runtime_error("no such material");
+        }
+        std::vector<double> in(3 * N);
+        std::copy(n, n + N, in.begin());
+        std::copy(v, v + N, in.begin() + N);
+        std::copy(l, l + N, in.begin() + 2 * N);
+        DeviceArray<double> d_in;
+        d_in.upload(in);
+        DeviceArray<float> d_f;
+        d_f.allocate(C);
+        DeviceArray<double> d_pdf;
+        d_pdf.allocate(1);
+        brdf_kernel<N, T, C><<<1, 1>>>(s, material, d_in.get(), d_f.get(), d_pdf.get());
+        NBPT_CUDA(cudaGetLastError());
+        NBPT_CUDA(cudaDeviceSynchronize());
+        d_f.download(f, C);
+        d_pdf.download(pdf, 1);
+}
+
+template <int N, typename T, int C>
+void SceneT<N, T, C>::brdf_sample(
+        const int material,
+        const double* n,
+        const double* v,
+        const std::uint32_t* seed,
+        const int seed_words,
+        double* l,
+        double* pdf,
+        float* f)
+{
+        const DeviceScene<N, T, C>& s = device();
+        if (material < 0 || material >= static_cast<int>(materials_.size()))
+        {
+                throw std::runtime_error("no such material");
+        }
+        std::vector<double> in(2 * N);
+        std::copy(n, n + N, in.begin());
+        std::copy(v, v + N, in.begin() + N);
+        DeviceArray<double> d_in;
+        d_in.upload(in);
+        DeviceArray<std::uint32_t> d_seed;
+        d_seed.upload(seed, seed_words);
+        DeviceArray<double> d_l;
+        d_l.allocate(N);
+        DeviceArray<double> d_pdf;
+        d_pdf.allocate(1);
+        DeviceArray<float> d_f;
+        d_f.allocate(C);
+        brdf_sample_kernel<N, T, C><<<1, 1>>>(s, material, d_in.get(), d_seed.get(), seed_words, d_l.get(), d_pdf.get(),
+                                              d_f.get());
+        NBPT_CUDA(cudaGetLastError());
+        NBPT_CUDA(cudaDeviceSynchronize());
+        d_pdf.download(pdf, 1);
+        d_l.download(l, N);
+        d_f.download(f, C);
+}
+
+template <int N, typename T, int C>
+void SceneT<N, T, C>::light_sample(
+        const int light,
+        const int kind,
+        const std::uint32_t* seed,
+        const int seed_words,
+        const double* point,
+        double* out,
+        float* radiance)
+{
+        const DeviceScene<N, T, C>& s = device();
+        if (light < 0 || light >= static_cast<int>(lights_.size()))
+        {
+                throw std::runtime_error("no such light");
+        }
+        DeviceArray<std::uint32_t> d_seed;
+        d_seed.upload(seed, seed_words);
+        std::vector<double> p(point, point + N);
+        DeviceArray<double> d_point;
+        d_point.upload(p);
+        DeviceArray<double> d_out;
+        d_out.allocate(3 * N + 2);
+        DeviceArray<float> d_rad;
+        d_rad.allocate(C);
+        light_sample_kernel<N, T, C><<<1, 1>>>(s, light, kind, d_seed.get(), seed_words, d_point.get(), d_out.get(),
+                                               d_rad.get());
+        NBPT_CUDA(cudaGetLastError());
+        NBPT_CUDA(cudaDeviceSynchronize());
+        d_out.download(out, 3 * N + 2);
+        d_rad.download(radiance, C);
+}
+
+template <int N>
+std::unique_ptr<Scene> make_scene_n(const bool double_precision, const bool spectrum)
+{
+        if (double_precision)
+        {
+                if (spectrum)
+                {
+                        return std::make_unique<SceneT<N, double, 64>>();
+                }
+                return std::make_unique<SceneT<N, double, 3>>();
+        }
+        if (spectrum)
+        {
+                return std::make_unique<SceneT<N, float, 64>>();
+        }
+        return std::make_unique<SceneT<N, float, 3>>();
+}
+} // namespace nbpt

@@ -1,0 +1,10 @@
+// Scene and painter instantiations for 4-space.
+#include "painter_impl.cuh"
+
+namespace nbpt
+{
+std::unique_ptr<Scene> make_scene_4(const bool double_precision, const bool spectrum)
+{
+        return make_scene_n<4>(double_precision, spectrum);
+}
+} // namespace nbpt

@@ -1,0 +1,60 @@
+"""The compiled reference (the oracle) against the committed golden
+fixtures and the CPU restatement: the fixtures were made by this oracle, so
+these pin that it is built and seeded the same way wherever it runs."""
+
+import numpy as np
+import pytest
+
+from math_b200 import scenes
+from oracle import port
+
+
+def test_oracle_rng_matches_golden(oracle_lib, golden):
+    g = golden("rng")
+    for i in range(4):
+        words = [int(x) for x in g[f"seed_{i}"]]
+        assert np.array_equal(oracle_lib.pcg(words, 64), g[f"pcg_{i}"])
+        assert np.array_equal(oracle_lib.canonical(words, 64, True), g[f"canonical_double_{i}"])
+        assert np.array_equal(oracle_lib.canonical(words, 64, False), g[f"canonical_float_{i}"])
+        assert np.array_equal(oracle_lib.sj_points(4, 81, words, True), g[f"sj_4_1_{i}"])
+
+
+def test_oracle_rng_matches_restatement(oracle_lib):
+    rng = np.random.default_rng(5)
+    for _ in range(20):
+        words = [int(x) for x in rng.integers(0, 2**32, size=rng.integers(1, 6))]
+        g = port.Pcg(words)
+        assert np.array_equal(oracle_lib.pcg(words, 16), [g() for _ in range(16)])
+
+
+def test_oracle_cornell3d_matches_golden(oracle_lib, golden):
+    g = golden("cornell3d")
+    desc = scenes.cornell_3d(size=(16, 16), subdivisions=3)
+    s = oracle_lib.Scene(desc, "double", False)
+    points, colors, valid = s.render_samples(int(g["spp"]), int(g["depth"]), seed=1)
+    assert np.array_equal(points, g["points"])
+    assert np.array_equal(valid, g["valid"])
+    assert np.array_equal(colors, g["colors"])
+    m = s.mesh_dump()
+    assert np.array_equal(m["planes"], g["mesh_planes"])
+    assert np.array_equal(m["node_info"], g["mesh_node_info"])
+    facet, t = s.mesh_trace(g["rays"])
+    assert np.array_equal(facet, g["ray_facet"])
+
+
+def test_oracle_constants(oracle_lib):
+    # pdf of cosine-weighted hemisphere directions is cos / K with K the
+    # integral of the cosine over the hemisphere: pi (3-space), 4 pi / 3 (4-space)
+    c3 = oracle_lib.constants(3, True)
+    assert c3[0] == pytest.approx(np.pi)
+    c4 = oracle_lib.constants(4, True)
+    assert c4[0] == pytest.approx(4 * np.pi / 3)
+
+
+def test_oracle_painter_runs(oracle_lib):
+    desc = scenes.cornell_3d(size=(8, 8), subdivisions=2)
+    s = oracle_lib.Scene(desc, "double", False)
+    stats, rgb = s.paint(4, 5, passes=1, threads=2)
+    assert stats["sample_count"] == 64 * 4
+    assert stats["pass_number"] == 1
+    assert np.isfinite(rgb).all() and rgb.mean() > 0
