@@ -35,7 +35,6 @@ sys.path.insert(0, str(ROOT))
 
 WORKLOAD = {"scene": "cornell4d", "screen": [64, 64, 64], "spp": 16, "max_depth": 6,
             "points": 20000, "color": "spectrum64"}
-REFERENCE_SLAB = [64, 64, 4]  # bounded sample of the same scene for the CPU painter
 
 
 def parse():
@@ -47,6 +46,8 @@ def parse():
     p.add_argument("--precision", default="float", choices=["float", "double"])
     p.add_argument("--small", action="store_true", help="a small configuration for smoke runs")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--screen", type=int, default=None,
+                   help="edge of the voxel screen (default: the workload's 64), for smaller profiling runs")
     return p.parse_args()
 
 
@@ -57,12 +58,13 @@ def dist_env():
     return rank, world, local
 
 
-def scene_desc(small: bool):
+def scene_desc(small: bool, screen: int | None = None):
     from math_b200 import scenes
 
     if small:
         return scenes.cornell_4d(size=(16, 16, 16), points=2000)
-    return scenes.cornell_4d(size=tuple(WORKLOAD["screen"]), points=WORKLOAD["points"])
+    size = tuple(WORKLOAD["screen"]) if screen is None else (screen, screen, screen)
+    return scenes.cornell_4d(size=size, points=WORKLOAD["points"])
 
 
 class ClockSampler:
@@ -130,18 +132,24 @@ def cpu_baseline(small: bool, seconds_hint: float = 20.0) -> dict:
     if not oracle.available():
         return {"value": None, "unit": "paths/s", "cores": 0, "kind": "reference",
                 "sample": "oracle library not built"}
-    slab = [16, 16, 2] if small else REFERENCE_SLAB
-    desc = scenes.cornell_4d(size=tuple(slab), points=2000 if small else WORKLOAD["points"])
-    # the same camera as the full screen: the slab is the centre of the
-    # full screen's first two axes at full resolution, a few voxels thick
+    # the whole workload: one pass over the full screen
+    desc = scene_desc(small)
+    slab = desc["projector"]["size"]
     s = oracle.Scene(desc, "float", True)
     cores = os.cpu_count() or 1
     stats, _ = s.paint(WORKLOAD["spp"], WORKLOAD["max_depth"], passes=1, threads=cores)
     value = stats["sample_count"] / stats["pass_duration"]
     return {"value": value, "unit": "paths/s", "cores": cores, "kind": "reference",
-            "sample": (f"one pass of the reference painter over a {slab[0]}x{slab[1]}x{slab[2]} slab "
+            "sample": (f"one pass of the reference painter over the whole {'x'.join(map(str, slab))} screen "
                        f"({stats['sample_count']} paths, {stats['pass_duration']:.2f} s, "
                        f"ray_count {stats['ray_count']})")}
+
+
+# DRAM bytes (read + write) per path of one paths_kernel launch on this
+# workload in float, from the ncu capture summarised in
+# profiles/paths_kernel_cornell4d_32.md (a 32^3 screen of the same scene;
+# traffic scales with the number of paths)
+TRAFFIC_PER_PATH = {"float": 18496.0}
 
 
 def record_bytes(n: int, precision: str) -> dict:
@@ -160,8 +168,8 @@ def run_reference(args, rank: int):
         return
     # --steps timed passes of the bounded slab (warm-up passes untimed)
 
-    slab = [16, 16, 2] if args.small else REFERENCE_SLAB
-    desc = scenes.cornell_4d(size=tuple(slab), points=2000 if args.small else WORKLOAD["points"])
+    desc = scene_desc(args.small, args.screen)
+    slab = desc["projector"]["size"]
     s = oracle.Scene(desc, "float", True)
     cores = os.cpu_count() or 1
     for _ in range(args.warmup):
@@ -173,7 +181,7 @@ def run_reference(args, rank: int):
         samples += st["sample_count"]
         seconds += st["pass_duration"]
     value = samples / seconds
-    sample = f"{args.steps} passes of a {slab[0]}x{slab[1]}x{slab[2]} slab of the workload"
+    sample = f"{args.steps} passes over the whole {'x'.join(map(str, slab))} screen"
     print(json.dumps({
         "metric": "bpt_paths_per_second", "value": value, "unit": "paths/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -197,7 +205,7 @@ def run_nbpt(args, rank: int, world: int, local: int):
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     from math_b200 import painter as P
 
-    desc = scene_desc(args.small)
+    desc = scene_desc(args.small, args.screen)
     spectrum = True
     t0 = time.perf_counter()
     scene = P.Scene(desc, args.precision, spectrum)
@@ -248,30 +256,38 @@ def run_nbpt(args, rank: int, world: int, local: int):
         ms = float(t.item())
     value = world * paths_per_step * args.steps / (ms / 1000)
 
-    # end to end through the C ABI: pass + image read back to host memory
+    # end to end through the C ABI, every step a whole job: the scene built
+    # from host arrays (host->device copies, BVH build, facet setup on the
+    # device), one pass, and the image read back to host memory
     rgb = np.zeros((scene.pixels, 3), np.float32)
     rgba = np.zeros((scene.pixels, 4), np.float32)
     torch.cuda.synchronize()
-    e0 = time.perf_counter()
+    e2e_times = []
+    h2d = 0
     for _ in range(args.steps):
-        painter.run(1)
-        P._check(P.lib().nbpt_painter_images(painter.h, P._p(rgb, P._F), P._p(rgba, P._F)))
-    e2e_s = time.perf_counter() - e0
+        e0 = time.perf_counter()
+        job_scene = P.Scene(desc, args.precision, spectrum)
+        job = job_scene.painter(WORKLOAD["spp"], WORKLOAD["max_depth"], seed=1 + rank)
+        job.run(1)
+        P._check(P.lib().nbpt_painter_images(job.h, P._p(rgb, P._F), P._p(rgba, P._F)))
+        e2e_times.append(time.perf_counter() - e0)
+        h2d = job_scene.upload_bytes()
+        job.close()
+        job_scene.close()
+    e2e_s = float(np.sum(e2e_times))
     if world > 1:
         t = torch.tensor([e2e_s], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_s = float(t.item())
     e2e = world * paths_per_step * args.steps / e2e_s
 
-    # whole job: scene from host arrays (upload, BVH build, facet setup),
-    # one pass, image read back
-    j0 = time.perf_counter()
-    job_scene = P.Scene(desc, args.precision, spectrum)
-    job = job_scene.painter(WORKLOAD["spp"], WORKLOAD["max_depth"], seed=99)
-    job.run(1)
-    job.images()
-    job_s = time.perf_counter() - j0
-    del job, job_scene
+    # scene resident: one pass through the C ABI plus the image read back
+    torch.cuda.synchronize()
+    r0 = time.perf_counter()
+    for _ in range(args.steps):
+        painter.run(1)
+        P._check(P.lib().nbpt_painter_images(painter.h, P._p(rgb, P._F), P._p(rgba, P._F)))
+    resident_s = time.perf_counter() - r0
 
     sizes = record_bytes(desc["n"], args.precision)
     algorithmic = nodes * sizes["node"] + facets * sizes["facet"] + shapes * sizes["shape"]
@@ -283,7 +299,10 @@ def run_nbpt(args, rank: int, world: int, local: int):
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": (achieved / peak) if achieved else None, "traffic": None,
+                "frac": (achieved / peak) if achieved else None,
+                "traffic": (TRAFFIC_PER_PATH[args.precision] * paths_per_step
+                            if args.precision in TRAFFIC_PER_PATH and not args.small else None),
+                "traffic_source": "profiles/paths_kernel_cornell4d_32.md (per path, scaled to one launch)",
                 "kernel": "paths_kernel",
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 "algorithmic_bytes_per_path": algorithmic / (paths_per_step * args.steps),
@@ -293,7 +312,7 @@ def run_nbpt(args, rank: int, world: int, local: int):
                 "paths_kernel_share": paths_s / (ms / 1000) if ms > 0 else None}
 
     if rank == 0:
-        cpu = None if args.no_cpu_baseline else cpu_baseline(args.small)
+        cpu = None if (args.no_cpu_baseline or world > 1) else cpu_baseline(args.small)
         line = {
             "metric": "bpt_paths_per_second", "value": value, "unit": "paths/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -306,12 +325,13 @@ def run_nbpt(args, rank: int, world: int, local: int):
                        "paths_per_step": paths_per_step, "precision": args.precision,
                        "l2": "flushed (256 MiB write) between timed steps",
                        "scene_build_s": build_s},
-            "e2e": {"value": e2e, "unit": "paths/s", "h2d_bytes_per_step": 0,
+            "e2e": {"value": e2e, "unit": "paths/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(rgb.nbytes + rgba.nbytes),
-                    "note": "scene resident on the device; each step one pass through the C ABI plus the "
-                            "image read back to host memory"},
-            "e2e_job": {"seconds": job_s, "paths": paths_per_step,
-                        "note": "scene built from host arrays (upload, BVH, facet setup), one pass, image read back"},
+                    "seconds_per_step": e2e_s / args.steps,
+                    "note": "every step a whole job through the C ABI: scene from host arrays (copies, BVH "
+                            "build, facet setup), one pass, RGB and RGBA images read back to host memory"},
+            "resident": {"value": paths_per_step * args.steps / resident_s, "unit": "paths/s",
+                         "note": "scene resident; one pass through the C ABI plus the image read back"},
             "gpu_launches": 3 * args.steps,
             "roofline": roofline,
             "clocks": clock_info,

@@ -139,7 +139,10 @@ int nbpt_scene_finalize(nbpt_scene* scene);
 long long nbpt_scene_pixel_count(const nbpt_scene* scene);
 /* samples per pixel actually rendered: spp rounded up to a power of the screen dimension */
 int nbpt_scene_actual_spp(const nbpt_scene* scene, int samples_per_pixel);
+/* bytes of scene data the scene keeps on the GPU */
 long long nbpt_scene_device_bytes(const nbpt_scene* scene);
+/* bytes finalize copied from host to device (shapes, BVH, vertices, facets) */
+long long nbpt_scene_upload_bytes(const nbpt_scene* scene);
 
 /* ---- painter (painter::create_painter with Integrator::BPT) ---- */
 

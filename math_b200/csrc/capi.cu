@@ -492,6 +492,18 @@ long long nbpt_scene_device_bytes(const nbpt_scene* scene)
         return r;
 }
 
+long long nbpt_scene_upload_bytes(const nbpt_scene* scene)
+{
+        long long r = NBPT_ERROR;
+        guarded(
+                [&]
+                {
+                        r = scene_of(const_cast<nbpt_scene*>(scene)).upload_bytes();
+                        return 0;
+                });
+        return r;
+}
+
 nbpt_painter* nbpt_painter_create(nbpt_scene* scene, const int samples_per_pixel, const int max_depth, const unsigned seed)
 {
         nbpt_painter* out = nullptr;

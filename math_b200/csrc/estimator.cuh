@@ -498,13 +498,20 @@ NBPT_HD void merge_color_group(ColorSet<C>& s, const ColorGroup<C>& g, const flo
         }
         if (a_count == 0)
         {
+                // the group as created, held-out entries and sums
                 ColorSet<C> r;
                 for (int k = 0; k < b_count; ++k)
                 {
                         copy_entry(r, k, b, k);
                 }
+#pragma unroll 8
+                for (int c = 0; c < C; ++c)
+                {
+                        r.color_sum[c] = g_full ? g_sum[c] : 0.0f;
+                }
+                r.weight_sum = g_full ? g_wsum : 0.0f;
                 r.count = b_count;
-                r.full = 0;
+                r.full = g_full ? 1 : 0;
                 s = r;
                 return;
         }
@@ -682,8 +689,9 @@ NBPT_HD void merge_background_group(BackgroundSet& s, const float* gw, const int
                 {
                         s.weights[k] = held[k];
                 }
+                s.weight_sum = g_full ? g_sum : 0.0f;
                 s.count = g_count;
-                s.full = 0;
+                s.full = g_full ? 1 : 0;
                 return;
         }
         float out[HELD_OUT];
@@ -719,10 +727,11 @@ struct Screen final
         int size[N - 1];
 };
 
+// Merge one pass's samples of the 3^(n-1) neighbours into receiving pixel t.
 template <int N, typename T, int C>
-__global__ void __launch_bounds__(128) accumulate_kernel(
-        const Screen<N> screen,
-        const long long pixel_count,
+NBPT_HD void accumulate_pixel(
+        const Screen<N>& screen,
+        const long long t,
         const int spp,
         const T* __restrict__ points,
         const float* __restrict__ colors,
@@ -730,13 +739,8 @@ __global__ void __launch_bounds__(128) accumulate_kernel(
         const unsigned char* __restrict__ valid,
         const T alpha,
         const T exp_radius,
-        PixelState<C>* __restrict__ state)
+        PixelState<C>& st)
 {
-        const long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-        if (t >= pixel_count)
-        {
-                return;
-        }
         int tc[N - 1];
         {
                 long long rest = t;
@@ -747,7 +751,6 @@ __global__ void __launch_bounds__(128) accumulate_kernel(
                         rest /= screen.size[d];
                 }
         }
-        PixelState<C> st = state[t];
 
         float w[MAX_GROUP];
         float contribution[MAX_GROUP];
@@ -878,6 +881,29 @@ __global__ void __launch_bounds__(128) accumulate_kernel(
                         merge_background_group(st.background, sorted, nbg);
                 }
         }
+}
+
+// accumulation kernel: one thread per receiving pixel, no atomics
+template <int N, typename T, int C>
+__global__ void __launch_bounds__(128) accumulate_kernel(
+        const Screen<N> screen,
+        const long long pixel_count,
+        const int spp,
+        const T* __restrict__ points,
+        const float* __restrict__ colors,
+        const float* __restrict__ lum,
+        const unsigned char* __restrict__ valid,
+        const T alpha,
+        const T exp_radius,
+        PixelState<C>* __restrict__ state)
+{
+        const long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+        if (t >= pixel_count)
+        {
+                return;
+        }
+        PixelState<C> st = state[t];
+        accumulate_pixel<N, T, C>(screen, t, spp, points, colors, lum, valid, alpha, exp_radius, st);
         state[t] = st;
 }
 
@@ -1059,20 +1085,11 @@ NBPT_HD Resolved<C> resolve_pixel(const PixelState<C>& st)
         return res;
 }
 
+// The pixel's RGB and premultiplied RGBA (pixel.h:51-88, color.h rgb32).
 template <int C>
-__global__ void resolve_kernel(
-        const long long pixel_count,
-        const PixelState<C>* __restrict__ state,
-        const float* __restrict__ xyz, // [3][64] colour matching functions (spectrum only)
-        float* __restrict__ rgb,
-        float* __restrict__ rgba)
+NBPT_HD void resolve_rgb(const PixelState<C>& state, const float* xyz, float* rgb, float* rgba)
 {
-        const long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-        if (t >= pixel_count)
-        {
-                return;
-        }
-        const Resolved<C> r = resolve_pixel(state[t]);
+        const Resolved<C> r = resolve_pixel(state);
         float out[3] = {0.0f, 0.0f, 0.0f};
         float out_a[4] = {0.0f, 0.0f, 0.0f, 0.0f};
         if (r.has)
@@ -1125,15 +1142,31 @@ __global__ void resolve_kernel(
                         out_a[3] = r.color_weight / sum;
                 }
         }
-        rgb[t * 3 + 0] = out[0];
-        rgb[t * 3 + 1] = out[1];
-        rgb[t * 3 + 2] = out[2];
+        rgb[0] = out[0];
+        rgb[1] = out[1];
+        rgb[2] = out[2];
         if (rgba)
         {
-                rgba[t * 4 + 0] = out_a[0];
-                rgba[t * 4 + 1] = out_a[1];
-                rgba[t * 4 + 2] = out_a[2];
-                rgba[t * 4 + 3] = out_a[3];
+                rgba[0] = out_a[0];
+                rgba[1] = out_a[1];
+                rgba[2] = out_a[2];
+                rgba[3] = out_a[3];
         }
+}
+
+template <int C>
+__global__ void resolve_kernel(
+        const long long pixel_count,
+        const PixelState<C>* __restrict__ state,
+        const float* __restrict__ xyz, // [3][64] colour matching functions (spectrum only)
+        float* __restrict__ rgb,
+        float* __restrict__ rgba)
+{
+        const long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+        if (t >= pixel_count)
+        {
+                return;
+        }
+        resolve_rgb<C>(state[t], xyz, rgb + t * 3, rgba ? rgba + t * 4 : nullptr);
 }
 } // namespace nbpt

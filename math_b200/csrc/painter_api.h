@@ -65,6 +65,7 @@ public:
         virtual long long pixel_count() const = 0;
         virtual int actual_spp(int samples_per_pixel) const = 0;
         virtual long long device_bytes() const = 0;
+        virtual long long upload_bytes() const = 0;
 
         virtual std::unique_ptr<Painter> create_painter(int samples_per_pixel, int max_depth, std::uint32_t seed) = 0;
 

@@ -368,6 +368,7 @@ class SceneT final : public Scene
         DeviceArray<float> d_cie_; // x, y, z colour matching functions
         std::vector<MeshShape<N, T>> mesh_records_;
         long long facet_total_ = 0;
+        long long upload_bytes_ = 0;
         long long node_total_ = 0;
 
         DeviceScene<N, T, C> device_{};
@@ -1006,6 +1007,9 @@ public:
                 d_indices_.upload(indices);
                 d_materials_.upload(materials_);
                 d_lights_.upload(lights_);
+                upload_bytes_ = static_cast<long long>(d_flat_.bytes() + d_solid_.bytes() + d_meshes_.bytes() +
+                                                       d_nodes_.bytes() + d_indices_.bytes() + d_materials_.bytes() +
+                                                       d_lights_.bytes());
 
                 if (facet_total_ > 0)
                 {
@@ -1024,6 +1028,8 @@ public:
                         DeviceArray<int> derr;
                         std::vector<int> zero(1, 0);
                         derr.upload(zero);
+                        upload_bytes_ += static_cast<long long>(dv.bytes() + dn.bytes() + df.bytes() + dm.bytes() +
+                                                                derr.bytes());
                         d_facets_.allocate(facet_total_);
                         facet_setup_kernel<N, T><<<blocks_for(facet_total_, 128), 128>>>(
                                 dv.get(), any_normals ? dn.get() : nullptr, df.get(), dm.get(), facet_total_,
@@ -1047,6 +1053,7 @@ public:
                                         }
                                 }
                                 d_normals_.upload(nv);
+                                upload_bytes_ += static_cast<long long>(d_normals_.bytes());
                         }
                 }
 
@@ -1156,6 +1163,11 @@ public:
                         r *= k;
                 }
                 return r;
+        }
+
+        long long upload_bytes() const override
+        {
+                return upload_bytes_;
         }
 
         long long device_bytes() const override

@@ -68,6 +68,7 @@ SIGNATURES = [
     ("nbpt_scene_pixel_count", ctypes.c_longlong, [_P]),
     ("nbpt_scene_actual_spp", ctypes.c_int, [_P, ctypes.c_int]),
     ("nbpt_scene_device_bytes", ctypes.c_longlong, [_P]),
+    ("nbpt_scene_upload_bytes", ctypes.c_longlong, [_P]),
     ("nbpt_painter_create", _P, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_uint]),
     ("nbpt_painter_destroy", None, [_P]),
     ("nbpt_painter_enqueue", ctypes.c_int, [_P, ctypes.c_int]),
@@ -235,6 +236,9 @@ class Scene:
 
     def device_bytes(self) -> int:
         return _check(lib().nbpt_scene_device_bytes(self.h))
+
+    def upload_bytes(self) -> int:
+        return _check(lib().nbpt_scene_upload_bytes(self.h))
 
     def painter(self, samples_per_pixel: int, max_depth: int, seed: int = 1) -> "Painter":
         return Painter(self, samples_per_pixel, max_depth, seed)
