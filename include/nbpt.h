@@ -176,6 +176,29 @@ int nbpt_scene_trace(
         nbpt_scene* scene, const double* rays, long long count, int any, int* kind, int* index, double* t,
         double* point);
 
+/* Ray queries that allocate nothing.  No counterpart in the reference: an
+ * addition for callers that must not allocate device memory while they run,
+ * such as a caller whose own allocator or memory pool already holds the
+ * free device memory (an allocation here could fail), or a caller on a
+ * latency-critical thread (cudaFree synchronizes the whole device, stalling
+ * work on every stream).  Same arguments, results and arithmetic as
+ * nbpt_scene_trace, which allocates device buffers for every call.
+ *
+ * The rays and results pass through one fixed scratch array in device
+ * memory (2,228,224 bytes per device, part of the library image), so a call
+ * takes at most NBPT_TRACE_NOALLOC_MAX_RAYS rays; more are rejected with
+ * NBPT_ERROR and a message, before any device work.  Nothing in the scratch
+ * needs to start at zero.  The first call on each device looks up the
+ * scratch's device address (cudaGetSymbolAddress), which can initialise the
+ * CUDA context; make that first call before any stream capture begins.
+ * Calls share the scratch: two calls that overlap on one device, from two
+ * host threads, race on it and corrupt each other's results, so serialise
+ * them.  The call returns when the results are in the host arrays. */
+#define NBPT_TRACE_NOALLOC_MAX_RAYS 16384
+int nbpt_scene_trace_noalloc(
+        nbpt_scene* scene, const double* rays, long long count, int any, int* kind, int* index, double* t,
+        double* point);
+
 /* facet records and BVH of mesh `mesh` (order of creation among meshes):
  * counts = (facets, nodes, indices); planes [facets][N][N+1] (facet
  * hyperplane then N-1 barycentric hyperplanes, each n[N], d);

@@ -10,6 +10,7 @@
 #include <cmath>
 #include <exception>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -621,6 +622,141 @@ int nbpt_scene_trace(
                                 require(point, "point");
                         }
                         scene_of(scene).trace(rays, count, any, kind, index, t, point);
+                        return 0;
+                });
+}
+
+// ---------------------------------------------------------------------------
+// Ray queries without allocation (nbpt_scene_trace_noalloc)
+//
+// The rays and results of one call pass through a fixed scratch array in
+// device memory, defined here at file scope, instead of buffers allocated per
+// call.  Its layout holds NBPT_TRACE_NOALLOC_MAX_RAYS rays of the largest
+// dimension (5): origins and directions, then kind, index, distance and
+// point, each part starting on a 256-byte boundary.  Nothing in it needs to
+// start at zero: for every one of the `count` rays of a call the query
+// kernel writes each result slot that is read back.
+
+namespace
+{
+constexpr long long NOALLOC_MAX_N = 5;
+constexpr long long NOALLOC_RAYS = NBPT_TRACE_NOALLOC_MAX_RAYS;
+
+constexpr long long align256(const long long bytes)
+{
+        return (bytes + 255) / 256 * 256;
+}
+
+constexpr long long NOALLOC_RAYS_OFFSET = 0;
+constexpr long long NOALLOC_KIND_OFFSET = NOALLOC_RAYS_OFFSET + align256(NOALLOC_RAYS * 2 * NOALLOC_MAX_N * 8);
+constexpr long long NOALLOC_INDEX_OFFSET = NOALLOC_KIND_OFFSET + align256(NOALLOC_RAYS * 4);
+constexpr long long NOALLOC_T_OFFSET = NOALLOC_INDEX_OFFSET + align256(NOALLOC_RAYS * 4);
+constexpr long long NOALLOC_POINT_OFFSET = NOALLOC_T_OFFSET + align256(NOALLOC_RAYS * 8);
+constexpr long long NOALLOC_BYTES = NOALLOC_POINT_OFFSET + align256(NOALLOC_RAYS * NOALLOC_MAX_N * 8);
+static_assert(NOALLOC_BYTES == 2228224, "the scratch size stated in nbpt.h");
+
+// one copy per device (each device's context loads the module's own copy)
+static __device__ __align__(256) unsigned char g_trace_scratch[NOALLOC_BYTES];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_trace_scratch_mutex;
+unsigned char* g_trace_scratch_address[NOALLOC_MAX_DEVICES] = {};
+
+// The scratch's device address on the current device, looked up once per
+// device (cudaGetSymbolAddress) and cached.
+unsigned char* trace_scratch()
+{
+        int device = 0;
+        const cudaError_t e = cudaGetDevice(&device);
+        if (e != cudaSuccess)
+        {
+                throw CudaError(std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+        }
+        if (device < 0 || device >= NOALLOC_MAX_DEVICES)
+        {
+                throw std::runtime_error("nbpt_scene_trace_noalloc: device ordinal " + std::to_string(device) +
+                                         " beyond the " + std::to_string(NOALLOC_MAX_DEVICES) + " devices it serves");
+        }
+        const std::lock_guard lock(g_trace_scratch_mutex);
+        if (!g_trace_scratch_address[device])
+        {
+                void* address = nullptr;
+                const cudaError_t r = cudaGetSymbolAddress(&address, g_trace_scratch);
+                if (r != cudaSuccess || !address)
+                {
+                        throw CudaError(std::string("cudaGetSymbolAddress of the trace scratch: ") +
+                                        cudaGetErrorString(r));
+                }
+                g_trace_scratch_address[device] = static_cast<unsigned char*>(address);
+        }
+        return g_trace_scratch_address[device];
+}
+
+void copy_checked(void* to, const void* from, const long long bytes, const cudaMemcpyKind kind)
+{
+        const cudaError_t e = cudaMemcpy(to, from, static_cast<std::size_t>(bytes), kind);
+        if (e != cudaSuccess)
+        {
+                throw CudaError(std::string("cudaMemcpy: ") + cudaGetErrorString(e));
+        }
+}
+} // namespace
+
+int nbpt_scene_trace_noalloc(
+        nbpt_scene* scene,
+        const double* rays,
+        const long long count,
+        const int any,
+        int* kind,
+        int* index,
+        double* t,
+        double* point)
+{
+        return guarded(
+                [&]
+                {
+                        const nbpt::Scene& sc = scene_of(scene);
+                        require(rays, "rays");
+                        require(kind, "kind");
+                        if (!any)
+                        {
+                                require(index, "index");
+                                require(t, "t");
+                                require(point, "point");
+                        }
+                        if (count < 0)
+                        {
+                                throw std::runtime_error("nbpt_scene_trace_noalloc: negative ray count");
+                        }
+                        if (count > NOALLOC_RAYS)
+                        {
+                                throw std::runtime_error(
+                                        "nbpt_scene_trace_noalloc: " + std::to_string(count) +
+                                        " rays exceed its fixed scratch of " + std::to_string(NOALLOC_RAYS) +
+                                        " rays per call; split the batch or use nbpt_scene_trace");
+                        }
+                        if (count == 0)
+                        {
+                                return 0;
+                        }
+                        const long long n = sc.dimension();
+                        unsigned char* const base = trace_scratch();
+                        double* const d_rays = reinterpret_cast<double*>(base + NOALLOC_RAYS_OFFSET);
+                        int* const d_kind = reinterpret_cast<int*>(base + NOALLOC_KIND_OFFSET);
+                        int* const d_index = reinterpret_cast<int*>(base + NOALLOC_INDEX_OFFSET);
+                        double* const d_t = reinterpret_cast<double*>(base + NOALLOC_T_OFFSET);
+                        double* const d_point = reinterpret_cast<double*>(base + NOALLOC_POINT_OFFSET);
+
+                        copy_checked(d_rays, rays, count * 2 * n * 8, cudaMemcpyHostToDevice);
+                        sc.trace_device(d_rays, count, any, d_kind, d_index, d_t, d_point);
+                        // copies on the legacy default stream wait for the query kernel
+                        copy_checked(kind, d_kind, count * 4, cudaMemcpyDeviceToHost);
+                        if (!any)
+                        {
+                                copy_checked(index, d_index, count * 4, cudaMemcpyDeviceToHost);
+                                copy_checked(t, d_t, count * 8, cudaMemcpyDeviceToHost);
+                                copy_checked(point, d_point, count * n * 8, cudaMemcpyDeviceToHost);
+                        }
                         return 0;
                 });
 }

@@ -72,6 +72,11 @@ public:
         // verification: closest hit (any == 0) or any hit of rays [n][2N]
         virtual void trace(const double* rays, long long count, int any, int* kind, int* index, double* t,
                            double* point) = 0;
+        // the same query on device buffers the caller provides: launches the
+        // query kernel on the legacy default stream and returns without
+        // waiting; allocates nothing
+        virtual void trace_device(const double* rays, long long count, int any, int* kind, int* index, double* t,
+                                  double* point) const = 0;
         virtual void mesh_export(int mesh, long long* counts, double* planes, double* node_lo, double* node_hi,
                                  unsigned* node_info, unsigned* indices, int* normal_info) = 0;
         virtual void brdf(int material, const double* n, const double* v, const double* l, float* f,

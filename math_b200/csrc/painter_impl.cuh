@@ -1194,6 +1194,8 @@ public:
         std::unique_ptr<Painter> create_painter(int spp, int max_depth, std::uint32_t seed) override;
 
         void trace(const double* rays, long long count, int any, int* kind, int* index, double* t, double* point) override;
+        void trace_device(const double* rays, long long count, int any, int* kind, int* index, double* t,
+                          double* point) const override;
         void mesh_export(int mesh, long long* counts, double* planes, double* node_lo, double* node_hi,
                          unsigned* node_info, unsigned* indices, int* normal_info) override;
         void brdf(int material, const double* n, const double* v, const double* l, float* f, double* pdf) override;
@@ -1592,6 +1594,21 @@ void SceneT<N, T, C>::trace(
                 d_t.download(t, count);
                 d_point.download(point, count * N);
         }
+}
+
+template <int N, typename T, int C>
+void SceneT<N, T, C>::trace_device(
+        const double* rays,
+        const long long count,
+        const int any,
+        int* kind,
+        int* index,
+        double* t,
+        double* point) const
+{
+        const DeviceScene<N, T, C>& s = device();
+        trace_kernel<N, T, C><<<blocks_for(count, 128), 128>>>(s, rays, count, any, kind, index, t, point);
+        NBPT_CUDA(cudaGetLastError());
 }
 
 // counts: facets, nodes, indices; planes [F][N][N+1]; node_lo/hi [nodes][N];

@@ -78,6 +78,7 @@ SIGNATURES = [
     ("nbpt_painter_statistics", ctypes.c_int, [_P, ctypes.POINTER(Statistics)]),
     ("nbpt_painter_stream", _P, [_P]),
     ("nbpt_scene_trace", ctypes.c_int, [_P, _D, ctypes.c_longlong, ctypes.c_int, _I, _I, _D, _D]),
+    ("nbpt_scene_trace_noalloc", ctypes.c_int, [_P, _D, ctypes.c_longlong, ctypes.c_int, _I, _I, _D, _D]),
     ("nbpt_scene_mesh_export", ctypes.c_int, [_P, ctypes.c_int, _L, _D, _D, _D, _U, _U, _I]),
     ("nbpt_scene_brdf", ctypes.c_int, [_P, ctypes.c_int, _D, _D, _D, _F, _D]),
     ("nbpt_scene_brdf_sample", ctypes.c_int, [_P, ctypes.c_int, _D, _D, _U, ctypes.c_int, _D, _D, _F]),
