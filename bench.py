@@ -228,7 +228,7 @@ def run_nbpt(args, rank: int, world: int, local: int):
     # L2 flushed between passes (outside the events)
     step_ms = []
     paths_s = 0.0
-    nodes = facets = shapes = rays = 0
+    nodes = facets = shapes = rays = launches = 0
     for _ in range(args.steps):
         with torch.cuda.stream(stream):
             flush.fill_(1)
@@ -245,6 +245,7 @@ def run_nbpt(args, rank: int, world: int, local: int):
         facets += st["facets"]
         shapes += st["shapes"]
         rays += st["ray_count"]
+        launches += st["kernel_launches"]
     torch.cuda.synchronize()
     clock_info = clocks.stop()
 
@@ -332,7 +333,7 @@ def run_nbpt(args, rank: int, world: int, local: int):
                             "build, facet setup), one pass, RGB and RGBA images read back to host memory"},
             "resident": {"value": paths_per_step * args.steps / resident_s, "unit": "paths/s",
                          "note": "scene resident; one pass through the C ABI plus the image read back"},
-            "gpu_launches": 3 * args.steps,
+            "gpu_launches": launches,
             "roofline": roofline,
             "clocks": clock_info,
             "cpu_baseline": cpu,

@@ -68,6 +68,7 @@ typedef struct nbpt_statistics
         unsigned long long nodes;      /* BVH nodes visited, last pass */
         unsigned long long facets;     /* facet records tested, last pass */
         unsigned long long shapes;     /* other shapes tested, last pass */
+        long long kernel_launches;     /* kernels launched by the last pass */
 } nbpt_statistics;
 
 const char* nbpt_last_error(void);

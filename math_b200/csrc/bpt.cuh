@@ -12,6 +12,7 @@
 #include "geometry.cuh"
 #include "scene.cuh"
 #include "shading.cuh"
+#include "tape.cuh"
 
 namespace nbpt
 {
@@ -66,13 +67,17 @@ struct ArriveSample final
         }
 };
 
-template <int N, typename T, int C>
+// RECORD: trace with channel 0 only (C == 1) and write the path's colour
+// factors to `tape` (tape.cuh); the colours are then formed for all
+// channels by replaying the tape.
+template <int N, typename T, int C, bool RECORD = false>
 struct Bpt final
 {
         const SceneQueries<N, T, C>& q;
         const DeviceScene<N, T, C>& s;
         Pcg& g;
         int max_depth;
+        mutable TapeWriter tape{};
 
         PathVertex<N, T, C> camera[MAX_PATH_VERTICES];
         PathVertex<N, T, C> light[MAX_PATH_VERTICES];
@@ -174,10 +179,11 @@ struct Bpt final
                 return brdf_pdf(s.shading, s.materials[v.material].roughness, v.nrm.shading, dv, dl);
         }
 
-        __device__ Color<C> vertex_brdf(const PathVertex<N, T, C>& v, const Vec<N, T>& dv, const Vec<N, T>& dl) const
+        __device__ Color<C> vertex_brdf(const PathVertex<N, T, C>& v, const Vec<N, T>& dv, const Vec<N, T>& dl,
+                                        BrdfTerms* const terms = nullptr) const
         {
                 const Material<T, C>& m = s.materials[v.material];
-                return brdf_f(s.shading, m.roughness, m.f0, m.rho_ss, v.nrm.shading, dv, dl);
+                return brdf_f(s.shading, m.roughness, m.f0, m.rho_ss, v.nrm.shading, dv, dl, terms);
         }
 
         // prev.area_pdf(angle_pdf, next_pos, next_normal) for the vertex kinds
@@ -408,9 +414,12 @@ struct Bpt final
                         }
 
                         // surface_sample_with_pdf (surface_sample.cpp:39-82)
-                        const Material<T, C>& m = s.materials[q.material(surface)];
+                        const int material = q.material(surface);
+                        const Material<T, C>& m = s.materials[material];
                         const Vec<N, T>& n = normals.shading;
-                        const BrdfSample<N, C, T> bs = brdf_sample<N>(g, s.shading, m.roughness, m.f0, m.rho_ss, n, v);
+                        BrdfTerms terms;
+                        const BrdfSample<N, C, T> bs =
+                                brdf_sample<N>(g, s.shading, m.roughness, m.f0, m.rho_ss, n, v, RECORD ? &terms : nullptr);
                         bool ok = bs.pdf > 0 && !bs.brdf.is_black();
                         T n_l = 0;
                         if (ok)
@@ -434,7 +443,8 @@ struct Bpt final
                                 }
                                 return;
                         }
-                        const Color<C> sample_beta = bs.brdf * static_cast<float>(n_l / bs.pdf);
+                        const float sample_k = static_cast<float>(n_l / bs.pdf);
+                        const Color<C> sample_beta = bs.brdf * sample_k;
                         const T pdf_reversed = brdf_pdf(s.shading, m.roughness, n, bs.l, v);
 
                         // add_sample (bpt.cpp:119-134)
@@ -457,9 +467,23 @@ struct Bpt final
 
                         pdf_forward = bs.pdf;
                         beta *= sample_beta;
+                        float normals_k = 1;
                         if (!camera_path)
                         {
-                                beta *= static_cast<float>(correct_normals(normals, bs.l, v));
+                                normals_k = static_cast<float>(correct_normals(normals, bs.l, v));
+                                beta *= normals_k;
+                        }
+                        if constexpr (RECORD)
+                        {
+                                tape.put(static_cast<int>(camera_path ? TapeRecord::CAMERA_BOUNCE
+                                                                      : TapeRecord::LIGHT_BOUNCE));
+                                tape.put(material);
+                                tape.put(terms);
+                                tape.put(sample_k);
+                                if (!camera_path)
+                                {
+                                        tape.put(normals_k);
+                                }
                         }
                         if (beta.is_black())
                         {
@@ -507,7 +531,14 @@ struct Bpt final
 
                 const T pdf = dpdf * ls.pdf_pos * ls.pdf_dir;
                 const T k = max_value(T(0), dot(ls.n, ls.ray.dir));
-                const Color<C> beta = ls.radiance * static_cast<float>(k / pdf);
+                const float start_k = static_cast<float>(k / pdf);
+                const Color<C> beta = ls.radiance * start_k;
+                if constexpr (RECORD)
+                {
+                        tape.put(static_cast<int>(TapeRecord::LIGHT_START));
+                        tape.put(li);
+                        tape.put(start_k);
+                }
                 walk(false, beta, ls.pdf_dir, ls.ray, light, light_size);
         }
 
@@ -625,7 +656,15 @@ struct Bpt final
                         {
                                 return false;
                         }
-                        out = c * static_cast<float>(mis_weight(light, 0, t_count));
+                        const float mis = static_cast<float>(mis_weight(light, 0, t_count));
+                        out = c * mis;
+                        if constexpr (RECORD)
+                        {
+                                tape.put(static_cast<int>(TapeRecord::STRATEGY_EMITTED));
+                                tape.put(t_count);
+                                tape.put(cv.light);
+                                tape.put(mis);
+                        }
                         return true;
                 }
                 if (cv.type == static_cast<int>(VertexType::INFINITE))
@@ -657,8 +696,10 @@ struct Bpt final
                         {
                                 return false;
                         }
-                        const Color<C> c = cv.beta * vertex_brdf(cv, cv.dir, ray_to_light.dir) * as.radiance *
-                                           static_cast<float>(n_l / (as.pdf * l.distribution_pdf));
+                        BrdfTerms terms;
+                        const float light_k = static_cast<float>(n_l / (as.pdf * l.distribution_pdf));
+                        const Color<C> c = cv.beta * vertex_brdf(cv, cv.dir, ray_to_light.dir, RECORD ? &terms : nullptr) *
+                                           as.radiance * light_k;
                         if (c.is_black())
                         {
                                 return false;
@@ -667,7 +708,18 @@ struct Bpt final
                         {
                                 return false;
                         }
-                        out = c * static_cast<float>(mis_weight(&lv, 1, t_count));
+                        const float mis = static_cast<float>(mis_weight(&lv, 1, t_count));
+                        out = c * mis;
+                        if constexpr (RECORD)
+                        {
+                                tape.put(static_cast<int>(TapeRecord::STRATEGY_LIGHT));
+                                tape.put(t_count);
+                                tape.put(cv.material);
+                                tape.put(terms);
+                                tape.put(li);
+                                tape.put(light_k);
+                                tape.put(mis);
+                        }
                         return true;
                 }
 
@@ -687,10 +739,13 @@ struct Bpt final
                 {
                         return false;
                 }
-                const Color<C> c0 = cv.beta * vertex_brdf(cv, cv.dir, from_camera_to_light) *
-                                    vertex_brdf(lv, lv.dir, light_l) * lv.beta;
+                BrdfTerms camera_terms;
+                BrdfTerms light_terms;
+                const Color<C> c0 = cv.beta * vertex_brdf(cv, cv.dir, from_camera_to_light, RECORD ? &camera_terms : nullptr) *
+                                    vertex_brdf(lv, lv.dir, light_l, RECORD ? &light_terms : nullptr) * lv.beta;
                 const T geometry = camera_n_l * light_n_l / power<N - 1>(distance);
-                const Color<C> c = c0 * static_cast<float>(geometry);
+                const float geometry_k = static_cast<float>(geometry);
+                const Color<C> c = c0 * geometry_k;
                 if (c.is_black())
                 {
                         return false;
@@ -699,7 +754,20 @@ struct Bpt final
                 {
                         return false;
                 }
-                out = c * static_cast<float>(mis_weight(light, s_count, t_count));
+                const float mis = static_cast<float>(mis_weight(light, s_count, t_count));
+                out = c * mis;
+                if constexpr (RECORD)
+                {
+                        tape.put(static_cast<int>(TapeRecord::STRATEGY_CONNECT));
+                        tape.put(s_count);
+                        tape.put(t_count);
+                        tape.put(cv.material);
+                        tape.put(camera_terms);
+                        tape.put(lv.material);
+                        tape.put(light_terms);
+                        tape.put(geometry_k);
+                        tape.put(mis);
+                }
                 return true;
         }
 

@@ -584,6 +584,7 @@ int nbpt_painter_statistics(nbpt_painter* painter, nbpt_statistics* statistics)
                         statistics->nodes = s.nodes;
                         statistics->facets = s.facets;
                         statistics->shapes = s.shapes;
+                        statistics->kernel_launches = s.kernel_launches;
                         return 0;
                 });
 }

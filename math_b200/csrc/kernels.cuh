@@ -8,6 +8,7 @@
 #include "geometry.cuh"
 #include "scene.cuh"
 #include "shading.cuh"
+#include "tape.cuh"
 
 #include <cstdint>
 
@@ -289,6 +290,256 @@ __global__ void __launch_bounds__(128) paths_kernel(
                 atomicAdd(&stats->nodes, b);
                 atomicAdd(&stats->facets, c);
                 atomicAdd(&stats->shapes, d);
+        }
+}
+
+// ---------------------------------------------------------------------------
+// spectral paths in two kernels (tape.cuh): trace with channel 0 and record,
+// then colour all channels from the tapes
+
+// One thread per path, as paths_kernel, on the scene's channel-0 view.
+// Writes the path's tape (words_per_path 32-bit words at tape + i *
+// words_per_path: words used, valid, records) and its validity.
+template <int N, typename T>
+__global__ void __launch_bounds__(128) paths_record_kernel(
+        const DeviceScene<N, T, 1> scene,
+        const long long begin,
+        const long long end,
+        const int spp,
+        const int max_depth,
+        const std::uint32_t seed,
+        const std::uint32_t pass,
+        const T* __restrict__ points,
+        std::uint32_t* __restrict__ tape,
+        const int words_per_path,
+        unsigned char* __restrict__ valid,
+        PathStats* __restrict__ stats)
+{
+        const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+        const long long paths = (end - begin) * spp;
+        QueryCounters counters{0, 0, 0, 0};
+        if (i < paths)
+        {
+                const long long local_pixel = i / spp;
+                const int sample = static_cast<int>(i - local_pixel * spp);
+                const long long p = begin + local_pixel;
+
+                Vec<N - 1, T> point;
+                {
+                        long long rest = p;
+#pragma unroll
+                        for (int d = 0; d < N - 1; ++d)
+                        {
+                                const int size = scene.projector.size[d];
+                                const long long q = rest / size;
+                                point[d] = static_cast<T>(static_cast<int>(rest - q * size)) + points[i * (N - 1) + d];
+                                rest = q;
+                        }
+                }
+                const Ray<N, T> ray = scene.projector.ray(point);
+
+                const std::uint32_t words[4] = {seed, pass, static_cast<std::uint32_t>(p),
+                                                static_cast<std::uint32_t>(sample + 1)};
+                Pcg g = seed_seq_pcg(words, 4);
+                const SceneQueries<N, T, 1> q{scene, counters};
+                Bpt<N, T, 1, true> bpt{q, scene, g, max_depth};
+                std::uint32_t* const w = tape + i * static_cast<long long>(words_per_path);
+                bpt.tape.w = w;
+                Color<1> color;
+                const bool has = bpt.run(ray, color);
+                w[0] = static_cast<std::uint32_t>(bpt.tape.n);
+                w[1] = has ? 1u : 0u;
+                valid[i] = has ? 1 : 0;
+        }
+        unsigned long long a = counters.queries;
+        unsigned long long b = counters.nodes;
+        unsigned long long c = counters.facets;
+        unsigned long long d = counters.shapes;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+        {
+                a += __shfl_down_sync(0xffffffffu, a, o);
+                b += __shfl_down_sync(0xffffffffu, b, o);
+                c += __shfl_down_sync(0xffffffffu, c, o);
+                d += __shfl_down_sync(0xffffffffu, d, o);
+        }
+        if ((threadIdx.x & 31) == 0)
+        {
+                atomicAdd(&stats->queries, a);
+                atomicAdd(&stats->nodes, b);
+                atomicAdd(&stats->facets, c);
+                atomicAdd(&stats->shapes, d);
+        }
+}
+
+// One warp per path; lane l colours channels l, l + 32, ... (C / 32 of
+// them).  Every channel goes through the float operations of Bpt::walk,
+// light_path and connect_strategy in the recorded order.  Then lane 0 forms
+// the luminance by the reference's left-to-right dot product.
+template <int N, typename T, int C>
+__global__ void __launch_bounds__(128) paths_replay_kernel(
+        const Material<T, C>* __restrict__ materials,
+        const Light<N, T, C>* __restrict__ lights,
+        const float fresnel_a,
+        const float fresnel_b,
+        const long long paths,
+        const std::uint32_t* __restrict__ tape,
+        const int words_per_path,
+        float* __restrict__ colors,
+        float* __restrict__ lum,
+        const float* __restrict__ cie_y)
+{
+        static_assert(C % 32 == 0);
+        constexpr int K = C / 32;
+        const long long i = (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) / 32;
+        const int lane = threadIdx.x & 31;
+        if (i >= paths)
+        {
+                return;
+        }
+        TapeReader r{tape + i * static_cast<long long>(words_per_path)};
+        const int used = static_cast<int>(r.w[0]);
+        const bool has = r.w[1] != 0;
+
+        float camera_beta[MAX_PATH_VERTICES + 1][K];
+        float light_beta[MAX_PATH_VERTICES + 1][K];
+        float color[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+        {
+                camera_beta[1][k] = 1.0f;
+                color[k] = 0.0f;
+        }
+        int camera_vertex = 1;
+        int light_vertex = 1;
+        while (r.n < used)
+        {
+                const TapeRecord kind = static_cast<TapeRecord>(r.get_int());
+                switch (kind)
+                {
+                case TapeRecord::CAMERA_BOUNCE:
+                {
+                        const Material<T, C>& m = materials[r.get_int()];
+                        const BrdfTerms t = r.get_terms();
+                        const float sk = r.get_float();
+#pragma unroll
+                        for (int k = 0; k < K; ++k)
+                        {
+                                const int ch = lane + 32 * k;
+                                const float b = brdf_channel(t, m.f0.c[ch], m.rho_ss.c[ch], fresnel_a, fresnel_b);
+                                camera_beta[camera_vertex + 1][k] = camera_beta[camera_vertex][k] * (b * sk);
+                        }
+                        ++camera_vertex;
+                        break;
+                }
+                case TapeRecord::LIGHT_START:
+                {
+                        const Light<N, T, C>& l = lights[r.get_int()];
+                        const float sk = r.get_float();
+#pragma unroll
+                        for (int k = 0; k < K; ++k)
+                        {
+                                light_beta[1][k] = l.radiance.c[lane + 32 * k] * sk;
+                        }
+                        light_vertex = 1;
+                        break;
+                }
+                case TapeRecord::LIGHT_BOUNCE:
+                {
+                        const Material<T, C>& m = materials[r.get_int()];
+                        const BrdfTerms t = r.get_terms();
+                        const float sk = r.get_float();
+                        const float nk = r.get_float();
+#pragma unroll
+                        for (int k = 0; k < K; ++k)
+                        {
+                                const int ch = lane + 32 * k;
+                                const float b = brdf_channel(t, m.f0.c[ch], m.rho_ss.c[ch], fresnel_a, fresnel_b);
+                                const float beta = light_beta[light_vertex][k] * (b * sk);
+                                light_beta[light_vertex + 1][k] = beta * nk;
+                        }
+                        ++light_vertex;
+                        break;
+                }
+                case TapeRecord::STRATEGY_EMITTED:
+                {
+                        const int t_count = r.get_int();
+                        const Light<N, T, C>& l = lights[r.get_int()];
+                        const float mis = r.get_float();
+#pragma unroll
+                        for (int k = 0; k < K; ++k)
+                        {
+                                const float c = l.radiance.c[lane + 32 * k] * camera_beta[t_count - 1][k];
+                                color[k] += c * mis;
+                        }
+                        break;
+                }
+                case TapeRecord::STRATEGY_LIGHT:
+                {
+                        const int t_count = r.get_int();
+                        const Material<T, C>& m = materials[r.get_int()];
+                        const BrdfTerms t = r.get_terms();
+                        const Light<N, T, C>& l = lights[r.get_int()];
+                        const float lk = r.get_float();
+                        const float mis = r.get_float();
+#pragma unroll
+                        for (int k = 0; k < K; ++k)
+                        {
+                                const int ch = lane + 32 * k;
+                                const float b = brdf_channel(t, m.f0.c[ch], m.rho_ss.c[ch], fresnel_a, fresnel_b);
+                                const float c = ((camera_beta[t_count - 1][k] * b) * l.radiance.c[ch]) * lk;
+                                color[k] += c * mis;
+                        }
+                        break;
+                }
+                case TapeRecord::STRATEGY_CONNECT:
+                {
+                        const int s_count = r.get_int();
+                        const int t_count = r.get_int();
+                        const Material<T, C>& mc = materials[r.get_int()];
+                        const BrdfTerms tc = r.get_terms();
+                        const Material<T, C>& ml = materials[r.get_int()];
+                        const BrdfTerms tl = r.get_terms();
+                        const float gk = r.get_float();
+                        const float mis = r.get_float();
+#pragma unroll
+                        for (int k = 0; k < K; ++k)
+                        {
+                                const int ch = lane + 32 * k;
+                                const float bc = brdf_channel(tc, mc.f0.c[ch], mc.rho_ss.c[ch], fresnel_a, fresnel_b);
+                                const float bl = brdf_channel(tl, ml.f0.c[ch], ml.rho_ss.c[ch], fresnel_a, fresnel_b);
+                                const float c0 = ((camera_beta[t_count - 1][k] * bc) * bl) * light_beta[s_count - 1][k];
+                                const float c = c0 * gk;
+                                color[k] += c * mis;
+                        }
+                        break;
+                }
+                default:
+                        r.n = used; // unknown record: stop (tapes are written by paths_record_kernel only)
+                        break;
+                }
+        }
+        float* const out = colors + i * C;
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+        {
+                out[lane + 32 * k] = has ? color[k] : 0.0f;
+        }
+        // luminance: max(0, c_j) * y_j summed for j = 0, 1, ..., C - 1 in order
+        float sum = 0.0f;
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+        {
+                const float mine = max_value(0.0f, color[k]) * cie_y[lane + 32 * k];
+                for (int j = 0; j < 32; ++j)
+                {
+                        const float v = __shfl_sync(0xffffffffu, mine, j);
+                        sum = (k == 0 && j == 0) ? v : sum + v;
+                }
+        }
+        if (lane == 0)
+        {
+                lum[i] = has ? sum : 0.0f;
         }
 }
 

@@ -19,6 +19,7 @@ struct Statistics final
         unsigned long long nodes;      // BVH nodes visited, last pass
         unsigned long long facets;     // facet records tested, last pass
         unsigned long long shapes;     // other shapes tested, last pass
+        long long kernel_launches;     // kernels launched by the last pass
 };
 
 class Painter

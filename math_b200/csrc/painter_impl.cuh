@@ -372,6 +372,11 @@ class SceneT final : public Scene
         long long node_total_ = 0;
 
         DeviceScene<N, T, C> device_{};
+        // channel-0 view of the materials and lights, for tracing spectral
+        // paths with one channel (tape.cuh)
+        DeviceArray<Material<T, 1>> d_materials_1_;
+        DeviceArray<Light<N, T, 1>> d_lights_1_;
+        DeviceScene<N, T, 1> device_1_{};
 
         void check_open() const
         {
@@ -1115,7 +1120,69 @@ public:
                 device_.shading.fresnel_b = fa[1];
                 device_.shading.f1_albedo = d_f1_albedo_.get();
                 device_.shading.f1_average = d_f1_average_.get();
+
+                if constexpr (C > 3)
+                {
+                        std::vector<Material<T, 1>> m1(materials_.size());
+                        for (std::size_t i = 0; i < materials_.size(); ++i)
+                        {
+                                m1[i].roughness = materials_[i].roughness;
+                                m1[i].f0.c[0] = materials_[i].f0.c[0];
+                                m1[i].rho_ss.c[0] = materials_[i].rho_ss.c[0];
+                        }
+                        std::vector<Light<N, T, 1>> l1(lights_.size());
+                        for (std::size_t i = 0; i < lights_.size(); ++i)
+                        {
+                                const Light<N, T, C>& l = lights_[i];
+                                Light<N, T, 1>& o = l1[i];
+                                o.type = l.type;
+                                o.org = l.org;
+                                for (int k = 0; k < N - 1; ++k)
+                                {
+                                        o.vectors[k] = l.vectors[k];
+                                }
+                                o.normal = l.normal;
+                                o.pdf = l.pdf;
+                                o.radiance.c[0] = l.radiance.c[0];
+                                o.distribution_pdf = l.distribution_pdf;
+                                o.cumulative = l.cumulative;
+                        }
+                        d_materials_1_.upload(m1);
+                        d_lights_1_.upload(l1);
+                        upload_bytes_ += static_cast<long long>(d_materials_1_.bytes() + d_lights_1_.bytes());
+                        device_1_.flat = device_.flat;
+                        device_1_.flat_count = device_.flat_count;
+                        device_1_.solid = device_.solid;
+                        device_1_.solid_count = device_.solid_count;
+                        device_1_.meshes = device_.meshes;
+                        device_1_.mesh_count = device_.mesh_count;
+                        device_1_.nodes = device_.nodes;
+                        device_1_.indices = device_.indices;
+                        device_1_.facets = device_.facets;
+                        device_1_.normals = device_.normals;
+                        device_1_.materials = d_materials_1_.get();
+                        device_1_.lights = d_lights_1_.get();
+                        device_1_.light_count = device_.light_count;
+                        device_1_.projector = device_.projector;
+                        device_1_.shading = device_.shading;
+                }
                 finalized_ = true;
+        }
+
+        const DeviceScene<N, T, 1>& device_channel_0() const
+        {
+                device(); // throws if not finalized
+                return device_1_;
+        }
+
+        const Material<T, C>* device_materials() const
+        {
+                return d_materials_.get();
+        }
+
+        const Light<N, T, C>* device_lights() const
+        {
+                return d_lights_.get();
         }
 
         long long pixel_count() const override
@@ -1377,7 +1444,15 @@ class PainterT final : public Painter
         DeviceArray<PathStats> stats_;
         DeviceArray<float> rgb_;
         DeviceArray<float> rgba_;
+        // spectral colour: path tapes of one chunk of pixels (tape.cuh)
+        int tape_words_ = 0;
+        long long chunk_pixels_ = 0;
+        DeviceArray<std::uint32_t> tape_;
+        long long launches_ = 0;
         Statistics statistics_{};
+
+        // device memory for the tapes of one chunk
+        static constexpr long long TAPE_BUDGET = 4LL << 30;
 
 public:
         PainterT(const SceneT<N, T, C>* scene, const int spp, const int max_depth, const std::uint32_t seed)
@@ -1425,6 +1500,13 @@ public:
                 stats_.allocate(1);
                 rgb_.allocate(pixels_ * 3);
                 rgba_.allocate(pixels_ * 4);
+                if constexpr (C > 3)
+                {
+                        tape_words_ = tape_words(max_depth_);
+                        const long long per_pixel = static_cast<long long>(spp_) * tape_words_ * 4;
+                        chunk_pixels_ = std::max(1LL, std::min(pixels_, TAPE_BUDGET / per_pixel));
+                        tape_.allocate(chunk_pixels_ * spp_ * tape_words_);
+                }
 
                 NBPT_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
                 NBPT_CUDA(cudaEventCreate(&ev_start_));
@@ -1468,11 +1550,38 @@ public:
                                 0, pixels_, seed_, pass, strata_, offsets_.get(), points_.get());
                         NBPT_CUDA(cudaGetLastError());
                         NBPT_CUDA(cudaEventRecord(ev_paths_, stream_));
-                        const long long paths = pixels_ * spp_;
-                        paths_kernel<N, T, C><<<blocks_for(paths, 128), 128, 0, stream_>>>(
-                                scene, 0, pixels_, spp_, max_depth_, seed_, pass, points_.get(), colors_.get(),
-                                lum_.get(), valid_.get(), scene_->cie() + 64, stats_.get());
-                        NBPT_CUDA(cudaGetLastError());
+                        long long launches = 2;
+                        if constexpr (C > 3)
+                        {
+                                // trace with channel 0 and record, then colour every
+                                // channel from the tapes, one chunk of pixels at a time
+                                const DeviceScene<N, T, 1>& scene_1 = scene_->device_channel_0();
+                                for (long long b = 0; b < pixels_; b += chunk_pixels_)
+                                {
+                                        const long long e = std::min(pixels_, b + chunk_pixels_);
+                                        const long long n = (e - b) * spp_;
+                                        paths_record_kernel<N, T><<<blocks_for(n, 128), 128, 0, stream_>>>(
+                                                scene_1, b, e, spp_, max_depth_, seed_, pass, points_.get() + b * spp_ * (N - 1),
+                                                tape_.get(), tape_words_, valid_.get() + b * spp_, stats_.get());
+                                        NBPT_CUDA(cudaGetLastError());
+                                        paths_replay_kernel<N, T, C><<<blocks_for(n * 32, 128), 128, 0, stream_>>>(
+                                                scene_->device_materials(), scene_->device_lights(),
+                                                scene.shading.fresnel_a, scene.shading.fresnel_b, n, tape_.get(),
+                                                tape_words_, colors_.get() + b * spp_ * C, lum_.get() + b * spp_,
+                                                scene_->cie() + 64);
+                                        NBPT_CUDA(cudaGetLastError());
+                                        launches += 2;
+                                }
+                        }
+                        else
+                        {
+                                const long long paths = pixels_ * spp_;
+                                paths_kernel<N, T, C><<<blocks_for(paths, 128), 128, 0, stream_>>>(
+                                        scene, 0, pixels_, spp_, max_depth_, seed_, pass, points_.get(), colors_.get(),
+                                        lum_.get(), valid_.get(), scene_->cie() + 64, stats_.get());
+                                NBPT_CUDA(cudaGetLastError());
+                                launches += 1;
+                        }
                         NBPT_CUDA(cudaEventRecord(ev_paths_end_, stream_));
                         Screen<N> screen;
                         for (int i = 0; i < N - 1; ++i)
@@ -1488,6 +1597,7 @@ public:
                                 exp_radius, state_.get());
                         NBPT_CUDA(cudaGetLastError());
                         NBPT_CUDA(cudaEventRecord(ev_end_, stream_));
+                        launches_ = launches;
                 }
                 passes_done_ += passes;
         }
@@ -1509,6 +1619,7 @@ public:
                 statistics_.nodes = s.nodes;
                 statistics_.facets = s.facets;
                 statistics_.shapes = s.shapes;
+                statistics_.kernel_launches = launches_;
         }
 
         void images(float* rgb, float* rgba) override

@@ -367,92 +367,92 @@ NBPT_HD T f1_albedo_average(const ShadingConstants<T>& sc, const T roughness)
 // ---------------------------------------------------------------------------
 // BRDF terms
 
-// Schlick Fresnel (fresnel.h:37-45)
-template <int C, typename T>
-NBPT_HD Color<C> fresnel(const Color<C>& f0, const T h_l)
+// The scalar factors of one evaluation of brdf::f.  Every term of the BRDF
+// is a colour-channel-wise function of f0 and rho_ss with these factors,
+// converted to float as the reference converts them; brdf_channel() applies
+// them to one channel.  Both the full-colour evaluation below and the
+// channel-parallel evaluation of recorded paths go through brdf_channel(),
+// so they give the same floats.
+struct BrdfTerms final
 {
-        const float t = static_cast<float>(power<5>(1 - h_l));
-        Color<C> r;
-#pragma unroll
-        for (int i = 0; i < C; ++i)
-        {
-                r.c[i] = (1 - t) * f0.c[i] + t * 1.0f;
-        }
-        return r;
-}
+        float fresnel_t; // float(power<5>(1 - h.l)), Schlick Fresnel (fresnel.h:37-45)
+        float ggx;       // float(D * G2 / divisor), the GGX term without Fresnel
+        float bounce_d;  // multiple-bounce numerator factor (multiple_bounce.h:40-64)
+        float bounce_m;  // float(1 - average f1 albedo)
+        float diffuse;   // float(c / k), diffuse_disney_ws (subsurface.h:67-78)
+        int ggx_on;      // n.v > 0, n.l > 0 and h.l > 0: the GGX term is present
+};
 
-template <int N, int C, typename T>
-NBPT_HD Color<C> ggx_brdf(
+template <int N, typename T>
+NBPT_HD BrdfTerms brdf_terms(
         const ShadingConstants<T>& sc,
         const T roughness,
-        const Color<C>& f0,
-        const T n_v,
-        const T n_l,
-        const T n_h,
-        const T h_l)
+        const Vec<N, T>& n,
+        const Vec<N, T>& v,
+        const Vec<N, T>& l)
 {
-        if (n_v > 0 && n_l > 0 && h_l > 0)
+        const Vec<N, T> h = (l + v).normalized();
+        const T n_l = dot(n, l);
+        const T h_l = dot(h, l);
+        const T n_v = dot(n, v);
+        const T n_h = dot(n, h);
+        BrdfTerms r;
+        // ggx_brdf (ggx.h:360-380)
+        r.ggx_on = (n_v > 0 && n_l > 0 && h_l > 0) ? 1 : 0;
+        r.fresnel_t = 0;
+        r.ggx = 0;
+        if (r.ggx_on)
         {
                 const T alpha = square(roughness);
                 const T d = ggx_d<N>(n_h, alpha, sc.k);
                 const T g2 = ggx_g2(n_v, n_l, alpha);
                 const T divisor = (n_v * n_l * T(1 << (N - 1)) * power<N - 3>(h_l));
-                return fresnel(f0, h_l) * static_cast<float>(d * g2 / divisor);
+                r.fresnel_t = static_cast<float>(power<5>(1 - h_l));
+                r.ggx = static_cast<float>(d * g2 / divisor);
         }
-        return Color<C>::filled(0);
-}
-
-// multiple_bounce.h:40-64
-template <int C, typename T>
-NBPT_HD Color<C> multiple_bounce(
-        const ShadingConstants<T>& sc,
-        const Color<C>& f0,
-        const T roughness,
-        const T n_l,
-        const T n_v)
-{
+        // multiple_bounce_surface_reflection (multiple_bounce.h:40-64)
         const T rs_f1 = f1_albedo_average(sc, roughness);
         const T rs_f1_l = f1_albedo(sc, roughness, n_l);
         const T rs_f1_v = f1_albedo(sc, roughness, n_v);
-
-        Color<C> f;
-#pragma unroll
-        for (int i = 0; i < C; ++i)
-        {
-                f.c[i] = f0.c[i] * sc.fresnel_a + sc.fresnel_b;
-        }
-        const Color<C> d = f * static_cast<float>(rs_f1 * (1 - rs_f1_l) * (1 - rs_f1_v) / (sc.k * (1 - rs_f1)));
-        const Color<C> m = f * static_cast<float>(1 - rs_f1);
-        Color<C> r;
-#pragma unroll
-        for (int i = 0; i < C; ++i)
-        {
-                r.c[i] = d.c[i] / (1.0f - m.c[i]);
-        }
+        r.bounce_d = static_cast<float>(rs_f1 * (1 - rs_f1_l) * (1 - rs_f1_v) / (sc.k * (1 - rs_f1)));
+        r.bounce_m = static_cast<float>(1 - rs_f1);
+        // diffuse_disney_ws
+        const T lp = power<5>(1 - n_l);
+        const T vp = power<5>(1 - n_v);
+        const T f_d90 = 2 * roughness * square(h_l);
+        const T c = (1 + (f_d90 - 1) * lp) * (1 + (f_d90 - 1) * vp);
+        r.diffuse = static_cast<float>(c * sc.k_inv);
         return r;
 }
 
-// subsurface.h:67-78
-template <int C, typename T>
-NBPT_HD Color<C> diffuse_disney_ws(
-        const ShadingConstants<T>& sc,
-        const Color<C>& f0,
-        const Color<C>& rho_ss,
-        const T roughness,
-        const T n_l,
-        const T n_v,
-        const T h_l)
+// One channel of ggx + multiple bounce + diffuse, summed in that order
+// (brdf.h:48-71).
+NBPT_HD float brdf_channel(const BrdfTerms& t, const float f0, const float rho_ss, const float fresnel_a,
+                           const float fresnel_b)
 {
-        const T l = power<5>(1 - n_l);
-        const T v = power<5>(1 - n_v);
-        const T f_d90 = 2 * roughness * square(h_l);
-        const T c = (1 + (f_d90 - 1) * l) * (1 + (f_d90 - 1) * v);
-        const float ck = static_cast<float>(c * sc.k_inv);
+        float r = 0.0f;
+        if (t.ggx_on)
+        {
+                const float fresnel = (1 - t.fresnel_t) * f0 + t.fresnel_t * 1.0f;
+                r = fresnel * t.ggx;
+        }
+        const float f = f0 * fresnel_a + fresnel_b;
+        const float d = f * t.bounce_d;
+        const float m = f * t.bounce_m;
+        r += d / (1.0f - m);
+        r += ((1.0f - f0) * t.diffuse) * rho_ss;
+        return r;
+}
+
+template <int C, typename T>
+NBPT_HD Color<C> brdf_color(const ShadingConstants<T>& sc, const BrdfTerms& t, const Color<C>& f0,
+                            const Color<C>& rho_ss)
+{
         Color<C> r;
 #pragma unroll
         for (int i = 0; i < C; ++i)
         {
-                r.c[i] = ((1.0f - f0.c[i]) * ck) * rho_ss.c[i];
+                r.c[i] = brdf_channel(t, f0.c[i], rho_ss.c[i], sc.fresnel_a, sc.fresnel_b);
         }
         return r;
 }
@@ -465,17 +465,15 @@ NBPT_HD Color<C> brdf_f_unchecked(
         const Color<C>& rho_ss,
         const Vec<N, T>& n,
         const Vec<N, T>& v,
-        const Vec<N, T>& l)
+        const Vec<N, T>& l,
+        BrdfTerms* const terms = nullptr)
 {
-        const Vec<N, T> h = (l + v).normalized();
-        const T n_l = dot(n, l);
-        const T h_l = dot(h, l);
-        const T n_v = dot(n, v);
-        const T n_h = dot(n, h);
-        Color<C> ggx = ggx_brdf<N>(sc, roughness, f0, n_v, n_l, n_h, h_l);
-        ggx += multiple_bounce(sc, f0, roughness, n_l, n_v);
-        ggx += diffuse_disney_ws(sc, f0, rho_ss, roughness, n_l, n_v, h_l);
-        return ggx;
+        const BrdfTerms t = brdf_terms<N>(sc, roughness, n, v, l);
+        if (terms)
+        {
+                *terms = t;
+        }
+        return brdf_color<C>(sc, t, f0, rho_ss);
 }
 
 // brdf::f (brdf.h:146-171)
@@ -487,7 +485,8 @@ NBPT_HD Color<C> brdf_f(
         const Color<C>& rho_ss,
         const Vec<N, T>& n,
         const Vec<N, T>& v,
-        const Vec<N, T>& l)
+        const Vec<N, T>& l,
+        BrdfTerms* const terms = nullptr)
 {
         if (dot(n, v) <= 0)
         {
@@ -497,7 +496,7 @@ NBPT_HD Color<C> brdf_f(
         {
                 return Color<C>::filled(0);
         }
-        return brdf_f_unchecked<N>(sc, roughness, f0, rho_ss, n, v, l);
+        return brdf_f_unchecked<N>(sc, roughness, f0, rho_ss, n, v, l, terms);
 }
 
 template <int N, typename T>
@@ -549,7 +548,8 @@ NBPT_HD BrdfSample<N, C, T> brdf_sample(
         const Color<C>& f0,
         const Color<C>& rho_ss,
         const Vec<N, T>& n,
-        const Vec<N, T>& v)
+        const Vec<N, T>& v,
+        BrdfTerms* const terms = nullptr)
 {
         BrdfSample<N, C, T> s;
         s.pdf = 0;
@@ -583,7 +583,7 @@ NBPT_HD BrdfSample<N, C, T> brdf_sample(
                 s.brdf = Color<C>::filled(0);
                 return s;
         }
-        s.brdf = brdf_f_unchecked<N>(sc, roughness, f0, rho_ss, n, v, l);
+        s.brdf = brdf_f_unchecked<N>(sc, roughness, f0, rho_ss, n, v, l, terms);
         return s;
 }
 } // namespace nbpt

@@ -42,6 +42,7 @@ class Statistics(ctypes.Structure):
         ("nodes", ctypes.c_ulonglong),
         ("facets", ctypes.c_ulonglong),
         ("shapes", ctypes.c_ulonglong),
+        ("kernel_launches", ctypes.c_longlong),
     ]
 
     def as_dict(self) -> dict:
