@@ -97,7 +97,7 @@ struct Bpt final
         }
 
         // leave_sample: the emission direction is drawn before the point
-        __device__ LeaveSample<N, T, C> leave_sample(const Light<N, T, C>& l) const
+        NBPT_CALL LeaveSample<N, T, C> leave_sample(const Light<N, T, C>& l) const
         {
                 const Vec<N, T> dir = cosine_on_hemisphere(g, l.normal);
                 const Vec<N, T> org = sample_location(l);
@@ -111,7 +111,7 @@ struct Bpt final
                 return r;
         }
 
-        __device__ ArriveSample<N, T, C> arrive_sample(const Light<N, T, C>& l, const Vec<N, T>& point) const
+        NBPT_CALL ArriveSample<N, T, C> arrive_sample(const Light<N, T, C>& l, const Vec<N, T>& point) const
         {
                 ArriveSample<N, T, C> r;
                 if (!(dot(l.normal, point - l.org) > 0))
@@ -234,7 +234,7 @@ struct Bpt final
         }
 
         // compute_pdf (vertex_pdf.h:141-190)
-        __device__ T compute_pdf(const PathVertex<N, T, C>& prev, const PathVertex<N, T, C>& v,
+        NBPT_CALL T compute_pdf(const PathVertex<N, T, C>& prev, const PathVertex<N, T, C>& v,
                                  const PathVertex<N, T, C>& next) const
         {
                 Vec<N, T> to_prev;
@@ -264,7 +264,7 @@ struct Bpt final
         }
 
         // compute_light_pdf (vertex_pdf.h:88-115)
-        __device__ T compute_light_pdf(const PathVertex<N, T, C>& lv, const PathVertex<N, T, C>& next) const
+        NBPT_CALL T compute_light_pdf(const PathVertex<N, T, C>& lv, const PathVertex<N, T, C>& next) const
         {
                 if (lv.type == static_cast<int>(VertexType::LIGHT))
                 {
@@ -288,7 +288,7 @@ struct Bpt final
                 return cosine > EPSILON;
         }
 
-        __device__ bool move_and_intersect_any(const Vec<N, T>& gn, const Ray<N, T>& ray, const T distance) const
+        NBPT_CALL bool move_and_intersect_any(const Vec<N, T>& gn, const Ray<N, T>& ray, const T distance) const
         {
                 const Hit<N, T> h = q.intersect(&gn, ray, distance);
                 if (!h)
@@ -307,7 +307,7 @@ struct Bpt final
         }
 
         // occluded(scene, normals, ray, distance) (visibility.h:99-123)
-        __device__ bool occluded_ray(const Normals<N, T>& normals, const Ray<N, T>& ray, const T distance) const
+        NBPT_CALL bool occluded_ray(const Normals<N, T>& normals, const Ray<N, T>& ray, const T distance) const
         {
                 if (!directed_outside(dot(ray.dir, normals.shading)))
                 {
@@ -323,7 +323,7 @@ struct Bpt final
         }
 
         // occluded(scene, p1, n1, p2, n2) (visibility.h:125-172)
-        __device__ bool occluded_points(const Vec<N, T>& p1, const Normals<N, T>& n1, const Vec<N, T>& p2,
+        NBPT_CALL bool occluded_points(const Vec<N, T>& p1, const Normals<N, T>& n1, const Vec<N, T>& p2,
                                         const Normals<N, T>& n2) const
         {
                 const Vec<N, T> direction_1 = p2 - p1;
@@ -393,7 +393,7 @@ struct Bpt final
                 return abs_value(numerator / denominator);
         }
 
-        __device__ void walk(const bool camera_path, Color<C> beta, T pdf_forward, Ray<N, T> ray,
+        NBPT_CALL void walk(const bool camera_path, Color<C> beta, T pdf_forward, Ray<N, T> ray,
                              PathVertex<N, T, C>* path, int& size) const
         {
                 Normals<N, T> normals;
@@ -552,7 +552,7 @@ struct Bpt final
 
         // The light subpath is `lp` (light[] or the single resampled light
         // vertex of an s = 1 strategy).
-        __device__ T mis_weight(const PathVertex<N, T, C>* lp, const int s_count, const int t_count) const
+        NBPT_CALL T mis_weight(const PathVertex<N, T, C>* lp, const int s_count, const int t_count) const
         {
                 if (s_count + t_count == 2)
                 {
@@ -637,7 +637,7 @@ struct Bpt final
         // -----------------------------------------------------------------
         // connections (connect.cpp:48-375)
 
-        __device__ bool connect_strategy(const int s_count, const int t_count, Color<C>& out)
+        NBPT_CALL bool connect_strategy(const int s_count, const int t_count, Color<C>& out)
         {
                 const PathVertex<N, T, C>& cv = camera[t_count - 1];
                 if (s_count == 0)

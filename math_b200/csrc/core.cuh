@@ -14,8 +14,15 @@
 
 #if defined(__CUDACC__)
 #define NBPT_HD __host__ __device__ __forceinline__
+// Large functions called from several places of the path kernels are kept
+// out of line: inlined at every call site they multiply the kernel's code
+// beyond the instruction cache.
+#define NBPT_HD_CALL __host__ __device__ __noinline__
+#define NBPT_CALL __device__ __noinline__
 #else
 #define NBPT_HD inline
+#define NBPT_HD_CALL inline
+#define NBPT_CALL inline
 #endif
 
 namespace nbpt

@@ -180,6 +180,12 @@ __global__ void sj_points_kernel(
         }
 }
 
+// Minimum resident blocks of 128 threads per SM asked of the compiler for
+// the path kernels (caps their registers); set from launch-shape sweeps.
+#ifndef NBPT_PATHS_MIN_BLOCKS
+#define NBPT_PATHS_MIN_BLOCKS 16
+#endif
+
 // ---------------------------------------------------------------------------
 // paths: one thread per (pixel, sample), stream seed_seq{seed, pass, p, i+1}
 
@@ -214,7 +220,7 @@ NBPT_HD float luminance(const Color<C>& c, const float* y)
 }
 
 template <int N, typename T, int C>
-__global__ void __launch_bounds__(128) paths_kernel(
+__global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_kernel(
         const DeviceScene<N, T, C> scene,
         const long long begin,
         const long long end,
@@ -301,7 +307,7 @@ __global__ void __launch_bounds__(128) paths_kernel(
 // Writes the path's tape (words_per_path 32-bit words at tape + i *
 // words_per_path: words used, valid, records) and its validity.
 template <int N, typename T>
-__global__ void __launch_bounds__(128) paths_record_kernel(
+__global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_record_kernel(
         const DeviceScene<N, T, 1> scene,
         const long long begin,
         const long long end,

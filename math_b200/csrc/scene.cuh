@@ -222,7 +222,7 @@ struct SceneQueries final
 
         // Closest facet of one mesh hit by the ray with t < max_distance
         // (bvh.h:108-149 traversal, spatial/ray_intersection.h:30-54 leaves).
-        __device__ int mesh_closest(const MeshShape<N, T>& mesh, const Ray<N, T>& ray, T& distance) const
+        NBPT_CALL int mesh_closest(const MeshShape<N, T>& mesh, const Ray<N, T>& ray, T& distance) const
         {
                 Vec<N, T> rec;
                 unsigned neg = 0;
@@ -298,7 +298,7 @@ struct SceneQueries final
                 return result < 0 ? -1 : result + mesh.facet_offset;
         }
 
-        __device__ bool mesh_any(const MeshShape<N, T>& mesh, const Ray<N, T>& ray, const T max_distance) const
+        NBPT_CALL bool mesh_any(const MeshShape<N, T>& mesh, const Ray<N, T>& ray, const T max_distance) const
         {
                 Vec<N, T> rec;
                 unsigned neg = 0;
@@ -366,7 +366,7 @@ struct SceneQueries final
         // Closest hit of the ray against every shape with t < max_distance,
         // after moving the origin off the surface it leaves
         // (scene.cpp:70-95, 97-123, 161-178).
-        __device__ Hit<N, T> intersect(const Vec<N, T>* geometric_normal, Ray<N, T> ray, T max_distance) const
+        NBPT_CALL Hit<N, T> intersect(const Vec<N, T>* geometric_normal, Ray<N, T> ray, T max_distance) const
         {
                 ++counters.queries;
                 if (geometric_normal)
@@ -438,7 +438,7 @@ struct SceneQueries final
         }
 
         // Any hit with t < max_distance (scene.cpp:125-133, 180-189).
-        __device__ bool intersect_any(const Vec<N, T>* geometric_normal, Ray<N, T> ray, const T max_distance) const
+        NBPT_CALL bool intersect_any(const Vec<N, T>* geometric_normal, Ray<N, T> ray, const T max_distance) const
         {
                 ++counters.queries;
                 if (geometric_normal)
@@ -572,7 +572,7 @@ struct SceneQueries final
 
         // integrators/com/visibility.h:174-204: a hit whose shading normal
         // faces away from the ray is re-cast up to two more times.
-        __device__ Hit<N, T> scene_intersect(const Vec<N, T>* geometric_normal, const Ray<N, T>& ray, Normals<N, T>& normals)
+        NBPT_CALL Hit<N, T> scene_intersect(const Vec<N, T>* geometric_normal, const Ray<N, T>& ray, Normals<N, T>& normals)
                 const
         {
                 Hit<N, T> h = intersect(geometric_normal, ray, infinity<T>());

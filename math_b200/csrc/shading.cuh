@@ -384,7 +384,7 @@ struct BrdfTerms final
 };
 
 template <int N, typename T>
-NBPT_HD BrdfTerms brdf_terms(
+NBPT_HD_CALL BrdfTerms brdf_terms(
         const ShadingConstants<T>& sc,
         const T roughness,
         const Vec<N, T>& n,
@@ -515,7 +515,7 @@ NBPT_HD T pdf_ggx_cosine(
 
 // brdf::pdf (brdf.h:173-194)
 template <int N, typename T>
-NBPT_HD T brdf_pdf(
+NBPT_HD_CALL T brdf_pdf(
         const ShadingConstants<T>& sc,
         const T roughness,
         const Vec<N, T>& n,
@@ -541,7 +541,7 @@ struct BrdfSample final
 // brdf::sample_f (brdf.h:109-141, 196-238): a 50/50 mix of GGX
 // visible-normal and cosine sampling.
 template <int N, int C, typename T>
-NBPT_HD BrdfSample<N, C, T> brdf_sample(
+NBPT_HD_CALL BrdfSample<N, C, T> brdf_sample(
         Pcg& g,
         const ShadingConstants<T>& sc,
         const T roughness,
