@@ -223,16 +223,22 @@ struct PixelState final
 template <int C>
 struct ColorGroup final
 {
-        const float* colors; // the source pixel's sample colours [spp][C]
+        const float* colors; // the source pixel's sample colours [spp][stride]
         const float* weights;
         const float* contributions;
         const int* order;
         int n;
+        // channel c of this group is channel c * step + offset of the colours
+        // (one thread per pixel: all channels, step 1; one warp per pixel: a
+        // lane's channels, step 32 and offset the lane)
+        int stride;
+        int step;
+        int offset;
 
         NBPT_HD float color(const int k, const int c) const
         {
                 const int i = order[k];
-                return weights[i] * colors[i * C + c];
+                return weights[i] * colors[i * stride + c * step + offset];
         }
 };
 
@@ -832,7 +838,7 @@ NBPT_HD void accumulate_pixel(
                                 return contribution[a] > contribution[b];
                         };
                         order_group(color_order, nc, less, greater);
-                        const ColorGroup<C> g{colors + p * spp * C, w, contribution, color_order, nc};
+                        const ColorGroup<C> g{colors + p * spp * C, w, contribution, color_order, nc, C, 1, 0};
                         float g_sum[C];
                         float g_wsum = 0;
 #pragma unroll 8
@@ -905,6 +911,257 @@ __global__ void __launch_bounds__(128) accumulate_kernel(
         PixelState<C> st = state[t];
         accumulate_pixel<N, T, C>(screen, t, spp, points, colors, lum, valid, alpha, exp_radius, st);
         state[t] = st;
+}
+
+// Spectral colours: one warp per receiving pixel.  The lanes compute the
+// filter weights of a source's samples in parallel; lane 0 selects and
+// orders the group (the scalar part, in shared memory); then every lane runs
+// the same merge on the same scalars for its own channels (lane, lane + 32,
+// ...), so the merge decisions are the single-thread kernel's and each
+// channel's sums are formed in the same order.
+template <int N, typename T, int C>
+__global__ void __launch_bounds__(128) accumulate_warp_kernel(
+        const Screen<N> screen,
+        const long long pixel_count,
+        const int spp,
+        const T* __restrict__ points,
+        const float* __restrict__ colors,
+        const float* __restrict__ lum,
+        const unsigned char* __restrict__ valid,
+        const T alpha,
+        const T exp_radius,
+        PixelState<C>* __restrict__ state)
+{
+        static_assert(C % 32 == 0);
+        constexpr int K = C / 32;
+        constexpr int WARPS = 4;
+        __shared__ float s_weight[WARPS][MAX_GROUP];
+        __shared__ float s_contribution[WARPS][MAX_GROUP];
+        __shared__ int s_kind[WARPS][MAX_GROUP]; // 0 none, 1 colour, 2 background
+        __shared__ int s_order[WARPS][MAX_GROUP];
+        __shared__ float s_background[WARPS][MAX_GROUP];
+        __shared__ float s_sorted[WARPS][MAX_GROUP];
+        __shared__ int s_counts[WARPS][2];
+
+        const int warp = threadIdx.x / 32;
+        const int lane = threadIdx.x & 31;
+        const long long t = blockIdx.x * static_cast<long long>(WARPS) + warp;
+        if (t >= pixel_count)
+        {
+                return; // the whole warp
+        }
+        float* const w = s_weight[warp];
+        float* const contribution = s_contribution[warp];
+        int* const kind = s_kind[warp];
+        int* const order = s_order[warp];
+        float* const background = s_background[warp];
+        float* const sorted = s_sorted[warp];
+
+        // this lane's channels of the pixel state, and its scalars
+        PixelState<C>& global = state[t];
+        ColorSet<K> cs;
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+        {
+                cs.color_sum[k] = global.color.color_sum[lane + 32 * k];
+#pragma unroll
+                for (int j = 0; j < HELD_OUT; ++j)
+                {
+                        cs.colors[j][k] = global.color.colors[j][lane + 32 * k];
+                }
+        }
+        cs.weight_sum = global.color.weight_sum;
+#pragma unroll
+        for (int j = 0; j < HELD_OUT; ++j)
+        {
+                cs.weights[j] = global.color.weights[j];
+                cs.contributions[j] = global.color.contributions[j];
+        }
+        cs.count = global.color.count;
+        cs.full = global.color.full;
+        BackgroundSet bs = global.background;
+
+        int tc[N - 1];
+        {
+                long long rest = t;
+#pragma unroll
+                for (int d = 0; d < N - 1; ++d)
+                {
+                        tc[d] = static_cast<int>(rest % screen.size[d]);
+                        rest /= screen.size[d];
+                }
+        }
+        int neighbours = 1;
+#pragma unroll
+        for (int d = 0; d < N - 1; ++d)
+        {
+                neighbours *= 3;
+        }
+        for (int nb = 0; nb < neighbours; ++nb)
+        {
+                int pc[N - 1];
+                bool inside = true;
+                {
+                        int rest = nb;
+#pragma unroll
+                        for (int d = 0; d < N - 1; ++d)
+                        {
+                                pc[d] = tc[d] + (rest % 3) - 1;
+                                rest /= 3;
+                                inside = inside && pc[d] >= 0 && pc[d] < screen.size[d];
+                        }
+                }
+                if (!inside)
+                {
+                        continue;
+                }
+                long long p = 0;
+#pragma unroll
+                for (int d = N - 2; d >= 0; --d)
+                {
+                        p = p * screen.size[d] + pc[d];
+                }
+                // weights and selection (pixel_filter.h:57-69, com/select.h:28-47)
+                for (int j = lane; j < spp; j += 32)
+                {
+                        const long long sidx = p * spp + j;
+                        const T x0 = (static_cast<T>(tc[0] - pc[0]) + T(0.5)) - points[sidx * (N - 1)];
+                        T weight = max_value(T(0), exp(alpha * x0 * x0) - exp_radius);
+#pragma unroll
+                        for (int d = 1; d < N - 1; ++d)
+                        {
+                                const T x = (static_cast<T>(tc[d] - pc[d]) + T(0.5)) - points[sidx * (N - 1) + d];
+                                weight *= max_value(T(0), exp(alpha * x * x) - exp_radius);
+                        }
+                        int k = 0;
+                        if (weight > 0)
+                        {
+                                const float wf = static_cast<float>(weight);
+                                w[j] = wf;
+                                if (valid[sidx])
+                                {
+                                        contribution[j] = wf * lum[sidx];
+                                        k = 1;
+                                }
+                                else
+                                {
+                                        k = 2;
+                                }
+                        }
+                        kind[j] = k;
+                }
+                __syncwarp();
+                if (lane == 0)
+                {
+                        int nc = 0;
+                        int nbg = 0;
+                        for (int j = 0; j < spp; ++j)
+                        {
+                                if (kind[j] == 1)
+                                {
+                                        order[nc++] = j;
+                                }
+                                else if (kind[j] == 2)
+                                {
+                                        background[nbg++] = w[j];
+                                }
+                        }
+                        const auto less = [&](const int a, const int b)
+                        {
+                                return contribution[a] < contribution[b];
+                        };
+                        const auto greater = [&](const int a, const int b)
+                        {
+                                return contribution[a] > contribution[b];
+                        };
+                        order_group(order, nc, less, greater);
+                        if (nbg > 1)
+                        {
+                                // background samples are ordered by value; reuse
+                                // `kind` as the index array of the ordering
+                                int* const index = kind;
+                                for (int j = 0; j < nbg; ++j)
+                                {
+                                        index[j] = j;
+                                }
+                                const auto bless = [&](const int a, const int b)
+                                {
+                                        return background[a] < background[b];
+                                };
+                                const auto bgreater = [&](const int a, const int b)
+                                {
+                                        return background[a] > background[b];
+                                };
+                                order_group(index, nbg, bless, bgreater);
+                                for (int j = 0; j < nbg; ++j)
+                                {
+                                        sorted[j] = background[index[j]];
+                                }
+                        }
+                        else if (nbg == 1)
+                        {
+                                sorted[0] = background[0];
+                        }
+                        s_counts[warp][0] = nc;
+                        s_counts[warp][1] = nbg;
+                }
+                __syncwarp();
+                const int nc = s_counts[warp][0];
+                const int nbg = s_counts[warp][1];
+                if (nc > 0)
+                {
+                        const ColorGroup<K> g{colors + p * spp * C, w, contribution, order, nc, C, 32, lane};
+                        float g_sum[K];
+                        float g_wsum = 0;
+#pragma unroll
+                        for (int k = 0; k < K; ++k)
+                        {
+                                g_sum[k] = 0;
+                        }
+                        const bool g_full = nc > HELD_OUT;
+                        if (g_full)
+                        {
+                                for (int k = HELD_OUT / 2; k < nc - HELD_OUT / 2; ++k)
+                                {
+#pragma unroll
+                                        for (int c = 0; c < K; ++c)
+                                        {
+                                                g_sum[c] += g.color(k, c);
+                                        }
+                                        g_wsum += w[order[k]];
+                                }
+                        }
+                        merge_color_group(cs, g, g_sum, g_wsum, g_full);
+                }
+                if (nbg > 0)
+                {
+                        merge_background_group(bs, sorted, nbg);
+                }
+                __syncwarp();
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+        {
+                global.color.color_sum[lane + 32 * k] = cs.color_sum[k];
+#pragma unroll
+                for (int j = 0; j < HELD_OUT; ++j)
+                {
+                        global.color.colors[j][lane + 32 * k] = cs.colors[j][k];
+                }
+        }
+        if (lane == 0)
+        {
+                global.color.weight_sum = cs.weight_sum;
+#pragma unroll
+                for (int j = 0; j < HELD_OUT; ++j)
+                {
+                        global.color.weights[j] = cs.weights[j];
+                        global.color.contributions[j] = cs.contributions[j];
+                }
+                global.color.count = cs.count;
+                global.color.full = cs.full;
+                global.background = bs;
+        }
 }
 
 // ---------------------------------------------------------------------------

@@ -1592,9 +1592,18 @@ public:
                         const T width = radius / T(2.5);
                         const T alpha = -1 / (2 * width * width);
                         const T exp_radius = std::exp(alpha * radius * radius);
-                        accumulate_kernel<N, T, C><<<blocks_for(pixels_, 128), 128, 0, stream_>>>(
-                                screen, pixels_, spp_, points_.get(), colors_.get(), lum_.get(), valid_.get(), alpha,
-                                exp_radius, state_.get());
+                        if constexpr (C % 32 == 0)
+                        {
+                                accumulate_warp_kernel<N, T, C><<<blocks_for(pixels_ * 32, 128), 128, 0, stream_>>>(
+                                        screen, pixels_, spp_, points_.get(), colors_.get(), lum_.get(), valid_.get(),
+                                        alpha, exp_radius, state_.get());
+                        }
+                        else
+                        {
+                                accumulate_kernel<N, T, C><<<blocks_for(pixels_, 128), 128, 0, stream_>>>(
+                                        screen, pixels_, spp_, points_.get(), colors_.get(), lum_.get(), valid_.get(),
+                                        alpha, exp_radius, state_.get());
+                        }
                         NBPT_CUDA(cudaGetLastError());
                         NBPT_CUDA(cudaEventRecord(ev_end_, stream_));
                         launches_ = launches;
