@@ -77,12 +77,12 @@ struct Bpt final
         const DeviceScene<N, T, C>& s;
         Pcg& g;
         int max_depth;
+        // the subpaths: max_depth + 1 vertices each, in local or global memory
+        PathVertex<N, T, C>* camera;
+        PathVertex<N, T, C>* light;
+        int camera_size = 0;
+        int light_size = 0;
         mutable TapeWriter tape{};
-
-        PathVertex<N, T, C> camera[MAX_PATH_VERTICES];
-        PathVertex<N, T, C> light[MAX_PATH_VERTICES];
-        int camera_size;
-        int light_size;
 
         // -----------------------------------------------------------------
         // lights
@@ -660,6 +660,7 @@ struct Bpt final
                         out = c * mis;
                         if constexpr (RECORD)
                         {
+                                tape.n = tape_slot_offset(max_depth, t_count, s_count);
                                 tape.put(static_cast<int>(TapeRecord::STRATEGY_EMITTED));
                                 tape.put(t_count);
                                 tape.put(cv.light);
@@ -712,6 +713,7 @@ struct Bpt final
                         out = c * mis;
                         if constexpr (RECORD)
                         {
+                                tape.n = tape_slot_offset(max_depth, t_count, s_count);
                                 tape.put(static_cast<int>(TapeRecord::STRATEGY_LIGHT));
                                 tape.put(t_count);
                                 tape.put(cv.material);
@@ -758,6 +760,7 @@ struct Bpt final
                 out = c * mis;
                 if constexpr (RECORD)
                 {
+                        tape.n = tape_slot_offset(max_depth, t_count, s_count);
                         tape.put(static_cast<int>(TapeRecord::STRATEGY_CONNECT));
                         tape.put(s_count);
                         tape.put(t_count);
@@ -771,6 +774,34 @@ struct Bpt final
                 return true;
         }
 
+        // bpt() (bpt.cpp:267-292) up to the connections: BACKGROUND for a
+        // camera ray that leaves the scene (the reference's nullopt), NO_LIGHT
+        // when the camera subpath is the camera alone (black), CONNECT when
+        // the light subpath is traced and the strategies follow.
+        enum class Subpaths : int
+        {
+                BACKGROUND = 0,
+                NO_LIGHT = 1,
+                CONNECT = 2
+        };
+
+        __device__ Subpaths subpaths(const Ray<N, T>& ray)
+        {
+                camera_path(ray);
+                if (camera_size == 1)
+                {
+                        return Subpaths::NO_LIGHT;
+                }
+                if (camera_size == 2 && camera[1].type == static_cast<int>(VertexType::INFINITE))
+                {
+                        return Subpaths::BACKGROUND;
+                }
+                light_path();
+                return Subpaths::CONNECT;
+        }
+
+        // connect() (connect.cpp:318-375): the strategies in the reference's
+        // order, their contributions summed
         __device__ Color<C> connect()
         {
                 Color<C> color = Color<C>::filled(0);
@@ -792,21 +823,15 @@ struct Bpt final
                 return color;
         }
 
-        // bpt() (bpt.cpp:267-292): false for a background sample (nullopt).
+        // bpt(): false for a background sample
         __device__ bool run(const Ray<N, T>& ray, Color<C>& out)
         {
-                camera_path(ray);
-                if (camera_size == 1)
-                {
-                        out = Color<C>::filled(0);
-                        return true;
-                }
-                if (camera_size == 2 && camera[1].type == static_cast<int>(VertexType::INFINITE))
+                const Subpaths r = subpaths(ray);
+                if (r == Subpaths::BACKGROUND)
                 {
                         return false;
                 }
-                light_path();
-                out = connect();
+                out = r == Subpaths::CONNECT ? connect() : Color<C>::filled(0);
                 return true;
         }
 };

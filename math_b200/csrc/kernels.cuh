@@ -187,7 +187,22 @@ __global__ void sj_points_kernel(
 #endif
 
 // ---------------------------------------------------------------------------
-// paths: one thread per (pixel, sample), stream seed_seq{seed, pass, p, i+1}
+// Paths: one per pixel sample, with the random stream seed_seq{seed, pass,
+// p, i + 1}.  A chunk of pixels runs through four kernels:
+//   paths_walk_kernel     one thread per path: the camera and light subpaths
+//                         traced with colour channel 0 (tape.cuh), their
+//                         vertices kept in global memory, the bounce records
+//                         on the path's tape, and one task queued per
+//                         strategy with s != 1;
+//   paths_connect_kernel  one thread per queued strategy: its contribution
+//                         factors written to the strategy's tape slot;
+//   paths_light_kernel    one thread per path: the s = 1 strategies in t
+//                         order, since each draws a fresh light sample from
+//                         the path's stream where the light subpath left it;
+//   paths_replay_kernel   the colours of all channels from the tapes.
+// Strategies of one path are independent apart from that random stream, so
+// evaluating them on separate threads changes no result; the replay sums
+// them in the reference's order.
 
 struct PathStats final
 {
@@ -219,65 +234,9 @@ NBPT_HD float luminance(const Color<C>& c, const float* y)
         }
 }
 
-template <int N, typename T, int C>
-__global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_kernel(
-        const DeviceScene<N, T, C> scene,
-        const long long begin,
-        const long long end,
-        const int spp,
-        const int max_depth,
-        const std::uint32_t seed,
-        const std::uint32_t pass,
-        const T* __restrict__ points,
-        float* __restrict__ colors,
-        float* __restrict__ lum,
-        unsigned char* __restrict__ valid,
-        const float* __restrict__ cie_y,
-        PathStats* __restrict__ stats)
+// Warp-aggregated statistics; every thread of the block must call it.
+__device__ inline void add_counters(const QueryCounters& counters, PathStats* const stats)
 {
-        const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-        const long long paths = (end - begin) * spp;
-        QueryCounters counters{0, 0, 0, 0};
-        if (i < paths)
-        {
-                const long long local_pixel = i / spp;
-                const int sample = static_cast<int>(i - local_pixel * spp);
-                const long long p = begin + local_pixel;
-
-                Vec<N - 1, T> point;
-                {
-                        long long rest = p;
-#pragma unroll
-                        for (int d = 0; d < N - 1; ++d)
-                        {
-                                const int size = scene.projector.size[d];
-                                const long long q = rest / size;
-                                point[d] = static_cast<T>(static_cast<int>(rest - q * size)) + points[i * (N - 1) + d];
-                                rest = q;
-                        }
-                }
-                const Ray<N, T> ray = scene.projector.ray(point);
-
-                const std::uint32_t words[4] = {seed, pass, static_cast<std::uint32_t>(p),
-                                                static_cast<std::uint32_t>(sample + 1)};
-                Pcg g = seed_seq_pcg(words, 4);
-                const SceneQueries<N, T, C> q{scene, counters};
-                Bpt<N, T, C> bpt{q, scene, g, max_depth};
-                Color<C> color;
-                const bool has = bpt.run(ray, color);
-                valid[i] = has ? 1 : 0;
-                if (!has)
-                {
-                        color = Color<C>::filled(0);
-                }
-#pragma unroll 8
-                for (int c = 0; c < C; ++c)
-                {
-                        colors[i * C + c] = color.c[c];
-                }
-                lum[i] = has ? luminance(color, cie_y) : 0.0f;
-        }
-        // warp-aggregated statistics
         unsigned long long a = counters.queries;
         unsigned long long b = counters.nodes;
         unsigned long long c = counters.facets;
@@ -290,7 +249,7 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_kernel(
                 c += __shfl_down_sync(0xffffffffu, c, o);
                 d += __shfl_down_sync(0xffffffffu, d, o);
         }
-        if ((threadIdx.x & 31) == 0)
+        if ((threadIdx.x & 31) == 0 && (a | b | c | d) != 0)
         {
                 atomicAdd(&stats->queries, a);
                 atomicAdd(&stats->nodes, b);
@@ -299,15 +258,18 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_kernel(
         }
 }
 
-// ---------------------------------------------------------------------------
-// spectral paths in two kernels (tape.cuh): trace with channel 0 and record,
-// then colour all channels from the tapes
+// A queued strategy: the path's index in its chunk, t and s.
+inline constexpr int TASK_PATH_SHIFT = 8;
+inline constexpr long long TASK_MAX_PATHS = 1LL << (32 - TASK_PATH_SHIFT);
 
-// One thread per path, as paths_kernel, on the scene's channel-0 view.
-// Writes the path's tape (words_per_path 32-bit words at tape + i *
-// words_per_path: words used, valid, records) and its validity.
+NBPT_HD constexpr std::uint32_t make_task(const long long path, const int t, const int s)
+{
+        return (static_cast<std::uint32_t>(path) << TASK_PATH_SHIFT) | (static_cast<std::uint32_t>(t) << 4) |
+               static_cast<std::uint32_t>(s);
+}
+
 template <int N, typename T>
-__global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_record_kernel(
+__global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_walk_kernel(
         const DeviceScene<N, T, 1> scene,
         const long long begin,
         const long long end,
@@ -316,14 +278,21 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_record_kerne
         const std::uint32_t seed,
         const std::uint32_t pass,
         const T* __restrict__ points,
+        PathVertex<N, T, 1>* __restrict__ vertices,
+        Pcg* __restrict__ rng,
         std::uint32_t* __restrict__ tape,
         const int words_per_path,
         unsigned char* __restrict__ valid,
+        std::uint32_t* __restrict__ tasks,
+        unsigned* __restrict__ task_count,
         PathStats* __restrict__ stats)
 {
         const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
         const long long paths = (end - begin) * spp;
         QueryCounters counters{0, 0, 0, 0};
+        int camera_size = 0;
+        int light_size = 0;
+        int task_n = 0;
         if (i < paths)
         {
                 const long long local_pixel = i / spp;
@@ -348,46 +317,160 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_record_kerne
                                                 static_cast<std::uint32_t>(sample + 1)};
                 Pcg g = seed_seq_pcg(words, 4);
                 const SceneQueries<N, T, 1> q{scene, counters};
-                Bpt<N, T, 1, true> bpt{q, scene, g, max_depth};
+                PathVertex<N, T, 1>* const v = vertices + i * 2 * (max_depth + 1);
+                Bpt<N, T, 1, true> bpt{q, scene, g, max_depth, v, v + max_depth + 1};
                 std::uint32_t* const w = tape + i * static_cast<long long>(words_per_path);
                 bpt.tape.w = w;
-                Color<1> color;
-                const bool has = bpt.run(ray, color);
+                using S = typename Bpt<N, T, 1, true>::Subpaths;
+                const S r = bpt.subpaths(ray);
+                const bool connect = r == S::CONNECT;
                 w[0] = static_cast<std::uint32_t>(bpt.tape.n);
-                w[1] = has ? 1u : 0u;
-                valid[i] = has ? 1 : 0;
+                w[1] = r != S::BACKGROUND ? 1u : 0u;
+                w[2] = static_cast<std::uint32_t>(connect ? bpt.camera_size : 1);
+                w[3] = static_cast<std::uint32_t>(connect ? bpt.light_size : 0);
+                valid[i] = r != S::BACKGROUND ? 1 : 0;
+                rng[i] = g;
+                if (connect)
+                {
+                        camera_size = bpt.camera_size;
+                        light_size = bpt.light_size;
+                        for (int t = 2; t <= camera_size; ++t)
+                        {
+                                for (int sc = 0; sc <= light_size; ++sc)
+                                {
+                                        task_n += (sc != 1 && t + sc - 2 <= max_depth) ? 1 : 0;
+                                }
+                        }
+                }
         }
-        unsigned long long a = counters.queries;
-        unsigned long long b = counters.nodes;
-        unsigned long long c = counters.facets;
-        unsigned long long d = counters.shapes;
+        // reserve this warp's task range with one atomic
+        const int lane = threadIdx.x & 31;
+        int offset = task_n;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1)
+        for (int o = 1; o < 32; o <<= 1)
         {
-                a += __shfl_down_sync(0xffffffffu, a, o);
-                b += __shfl_down_sync(0xffffffffu, b, o);
-                c += __shfl_down_sync(0xffffffffu, c, o);
-                d += __shfl_down_sync(0xffffffffu, d, o);
+                const int x = __shfl_up_sync(0xffffffffu, offset, o);
+                offset += lane >= o ? x : 0;
         }
-        if ((threadIdx.x & 31) == 0)
+        const int total = __shfl_sync(0xffffffffu, offset, 31);
+        unsigned base = 0;
+        if (lane == 31 && total > 0)
         {
-                atomicAdd(&stats->queries, a);
-                atomicAdd(&stats->nodes, b);
-                atomicAdd(&stats->facets, c);
-                atomicAdd(&stats->shapes, d);
+                base = atomicAdd(task_count, static_cast<unsigned>(total));
         }
+        base = __shfl_sync(0xffffffffu, base, 31);
+        if (task_n > 0)
+        {
+                unsigned k = base + static_cast<unsigned>(offset - task_n);
+                for (int t = 2; t <= camera_size; ++t)
+                {
+                        for (int sc = 0; sc <= light_size; ++sc)
+                        {
+                                if (sc != 1 && t + sc - 2 <= max_depth)
+                                {
+                                        tasks[k++] = make_task(i, t, sc);
+                                }
+                        }
+                }
+        }
+        add_counters(counters, stats);
 }
 
-// One warp per path; lane l colours channels l, l + 32, ... (C / 32 of
-// them).  Every channel goes through the float operations of Bpt::walk,
-// light_path and connect_strategy in the recorded order.  Then lane 0 forms
-// the luminance by the reference's left-to-right dot product.
-template <int N, typename T, int C>
+// Persistent: the grid strides over the queued strategies.
+template <int N, typename T>
+__global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_connect_kernel(
+        const DeviceScene<N, T, 1> scene,
+        const int max_depth,
+        PathVertex<N, T, 1>* __restrict__ vertices,
+        std::uint32_t* __restrict__ tape,
+        const int words_per_path,
+        const std::uint32_t* __restrict__ tasks,
+        const unsigned* __restrict__ task_count,
+        PathStats* __restrict__ stats)
+{
+        QueryCounters counters{0, 0, 0, 0};
+        const unsigned total = *task_count;
+        const unsigned stride = gridDim.x * blockDim.x;
+        for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += stride)
+        {
+                const std::uint32_t task = tasks[k];
+                const long long i = task >> TASK_PATH_SHIFT;
+                const int t = static_cast<int>((task >> 4) & 15u);
+                const int sc = static_cast<int>(task & 15u);
+                PathVertex<N, T, 1>* const v = vertices + i * 2 * (max_depth + 1);
+                std::uint32_t* const w = tape + i * static_cast<long long>(words_per_path);
+                Pcg unused{0, 0}; // only s = 1 draws random numbers
+                const SceneQueries<N, T, 1> q{scene, counters};
+                Bpt<N, T, 1, true> bpt{q, scene, unused, max_depth, v, v + max_depth + 1};
+                bpt.camera_size = static_cast<int>(w[2]);
+                bpt.light_size = static_cast<int>(w[3]);
+                bpt.tape.w = w;
+                Color<1> c;
+                if (!bpt.connect_strategy(sc, t, c))
+                {
+                        w[tape_slot_offset(max_depth, t, sc)] = 0;
+                }
+        }
+        add_counters(counters, stats);
+}
+
+template <int N, typename T>
+__global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_light_kernel(
+        const DeviceScene<N, T, 1> scene,
+        const long long paths,
+        const int max_depth,
+        PathVertex<N, T, 1>* __restrict__ vertices,
+        const Pcg* __restrict__ rng,
+        std::uint32_t* __restrict__ tape,
+        const int words_per_path,
+        PathStats* __restrict__ stats)
+{
+        const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+        QueryCounters counters{0, 0, 0, 0};
+        if (i < paths)
+        {
+                std::uint32_t* const w = tape + i * static_cast<long long>(words_per_path);
+                const int camera_size = static_cast<int>(w[2]);
+                const int light_size = static_cast<int>(w[3]);
+                if (w[1] != 0 && light_size >= 1)
+                {
+                        Pcg g = rng[i];
+                        PathVertex<N, T, 1>* const v = vertices + i * 2 * (max_depth + 1);
+                        const SceneQueries<N, T, 1> q{scene, counters};
+                        Bpt<N, T, 1, true> bpt{q, scene, g, max_depth, v, v + max_depth + 1};
+                        bpt.camera_size = camera_size;
+                        bpt.light_size = light_size;
+                        bpt.tape.w = w;
+                        for (int t = 2; t <= camera_size; ++t)
+                        {
+                                if (t - 1 > max_depth)
+                                {
+                                        continue;
+                                }
+                                Color<1> c;
+                                if (!bpt.connect_strategy(1, t, c))
+                                {
+                                        w[tape_slot_offset(max_depth, t, 1)] = 0;
+                                }
+                        }
+                }
+        }
+        add_counters(counters, stats);
+}
+
+// Colours from the tapes: LANES threads per path (32: one warp per path,
+// lane l forms channels l, l + 32, ...; 1: one thread per path).  Every
+// channel goes through the float operations of Bpt::walk, light_path and
+// connect_strategy in the recorded order, the strategies summed in the
+// reference's (t, s) order; then the luminance by the reference's
+// left-to-right dot product.
+template <int N, typename T, int C, int LANES>
 __global__ void __launch_bounds__(128) paths_replay_kernel(
         const Material<T, C>* __restrict__ materials,
         const Light<N, T, C>* __restrict__ lights,
         const float fresnel_a,
         const float fresnel_b,
+        const int max_depth,
         const long long paths,
         const std::uint32_t* __restrict__ tape,
         const int words_per_path,
@@ -395,17 +478,19 @@ __global__ void __launch_bounds__(128) paths_replay_kernel(
         float* __restrict__ lum,
         const float* __restrict__ cie_y)
 {
-        static_assert(C % 32 == 0);
-        constexpr int K = C / 32;
-        const long long i = (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) / 32;
-        const int lane = threadIdx.x & 31;
+        static_assert(C % LANES == 0 && 32 % LANES == 0);
+        constexpr int K = C / LANES;
+        const long long i = (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) / LANES;
+        const int lane = static_cast<int>(threadIdx.x % LANES);
         if (i >= paths)
         {
-                return;
+                return; // all LANES threads of the path
         }
         TapeReader r{tape + i * static_cast<long long>(words_per_path)};
         const int used = static_cast<int>(r.w[0]);
         const bool has = r.w[1] != 0;
+        const int camera_size = static_cast<int>(r.w[2]);
+        const int light_size = static_cast<int>(r.w[3]);
 
         float camera_beta[MAX_PATH_VERTICES + 1][K];
         float light_beta[MAX_PATH_VERTICES + 1][K];
@@ -418,12 +503,11 @@ __global__ void __launch_bounds__(128) paths_replay_kernel(
         }
         int camera_vertex = 1;
         int light_vertex = 1;
+        r.n = TAPE_HEADER;
         while (r.n < used)
         {
                 const TapeRecord kind = static_cast<TapeRecord>(r.get_int());
-                switch (kind)
-                {
-                case TapeRecord::CAMERA_BOUNCE:
+                if (kind == TapeRecord::CAMERA_BOUNCE)
                 {
                         const Material<T, C>& m = materials[r.get_int()];
                         const BrdfTerms t = r.get_terms();
@@ -431,26 +515,24 @@ __global__ void __launch_bounds__(128) paths_replay_kernel(
 #pragma unroll
                         for (int k = 0; k < K; ++k)
                         {
-                                const int ch = lane + 32 * k;
+                                const int ch = lane + LANES * k;
                                 const float b = brdf_channel(t, m.f0.c[ch], m.rho_ss.c[ch], fresnel_a, fresnel_b);
                                 camera_beta[camera_vertex + 1][k] = camera_beta[camera_vertex][k] * (b * sk);
                         }
                         ++camera_vertex;
-                        break;
                 }
-                case TapeRecord::LIGHT_START:
+                else if (kind == TapeRecord::LIGHT_START)
                 {
                         const Light<N, T, C>& l = lights[r.get_int()];
                         const float sk = r.get_float();
 #pragma unroll
                         for (int k = 0; k < K; ++k)
                         {
-                                light_beta[1][k] = l.radiance.c[lane + 32 * k] * sk;
+                                light_beta[1][k] = l.radiance.c[lane + LANES * k] * sk;
                         }
                         light_vertex = 1;
-                        break;
                 }
-                case TapeRecord::LIGHT_BOUNCE:
+                else if (kind == TapeRecord::LIGHT_BOUNCE)
                 {
                         const Material<T, C>& m = materials[r.get_int()];
                         const BrdfTerms t = r.get_terms();
@@ -459,93 +541,118 @@ __global__ void __launch_bounds__(128) paths_replay_kernel(
 #pragma unroll
                         for (int k = 0; k < K; ++k)
                         {
-                                const int ch = lane + 32 * k;
+                                const int ch = lane + LANES * k;
                                 const float b = brdf_channel(t, m.f0.c[ch], m.rho_ss.c[ch], fresnel_a, fresnel_b);
                                 const float beta = light_beta[light_vertex][k] * (b * sk);
                                 light_beta[light_vertex + 1][k] = beta * nk;
                         }
                         ++light_vertex;
-                        break;
                 }
-                case TapeRecord::STRATEGY_EMITTED:
+                else
                 {
-                        const int t_count = r.get_int();
-                        const Light<N, T, C>& l = lights[r.get_int()];
-                        const float mis = r.get_float();
-#pragma unroll
-                        for (int k = 0; k < K; ++k)
-                        {
-                                const float c = l.radiance.c[lane + 32 * k] * camera_beta[t_count - 1][k];
-                                color[k] += c * mis;
-                        }
-                        break;
+                        break; // not a bounce record: tapes are written by paths_walk_kernel only
                 }
-                case TapeRecord::STRATEGY_LIGHT:
+        }
+        for (int t_count = 2; t_count <= camera_size; ++t_count)
+        {
+                for (int s_count = 0; s_count <= light_size; ++s_count)
                 {
-                        const int t_count = r.get_int();
-                        const Material<T, C>& m = materials[r.get_int()];
-                        const BrdfTerms t = r.get_terms();
-                        const Light<N, T, C>& l = lights[r.get_int()];
-                        const float lk = r.get_float();
-                        const float mis = r.get_float();
-#pragma unroll
-                        for (int k = 0; k < K; ++k)
+                        if (t_count + s_count - 2 > max_depth)
                         {
-                                const int ch = lane + 32 * k;
-                                const float b = brdf_channel(t, m.f0.c[ch], m.rho_ss.c[ch], fresnel_a, fresnel_b);
-                                const float c = ((camera_beta[t_count - 1][k] * b) * l.radiance.c[ch]) * lk;
-                                color[k] += c * mis;
+                                continue;
                         }
-                        break;
-                }
-                case TapeRecord::STRATEGY_CONNECT:
-                {
-                        const int s_count = r.get_int();
-                        const int t_count = r.get_int();
-                        const Material<T, C>& mc = materials[r.get_int()];
-                        const BrdfTerms tc = r.get_terms();
-                        const Material<T, C>& ml = materials[r.get_int()];
-                        const BrdfTerms tl = r.get_terms();
-                        const float gk = r.get_float();
-                        const float mis = r.get_float();
-#pragma unroll
-                        for (int k = 0; k < K; ++k)
+                        r.n = tape_slot_offset(max_depth, t_count, s_count);
+                        const int kind = r.get_int();
+                        if (kind == static_cast<int>(TapeRecord::STRATEGY_EMITTED))
                         {
-                                const int ch = lane + 32 * k;
-                                const float bc = brdf_channel(tc, mc.f0.c[ch], mc.rho_ss.c[ch], fresnel_a, fresnel_b);
-                                const float bl = brdf_channel(tl, ml.f0.c[ch], ml.rho_ss.c[ch], fresnel_a, fresnel_b);
-                                const float c0 = ((camera_beta[t_count - 1][k] * bc) * bl) * light_beta[s_count - 1][k];
-                                const float c = c0 * gk;
-                                color[k] += c * mis;
+                                r.get_int(); // t
+                                const Light<N, T, C>& l = lights[r.get_int()];
+                                const float mis = r.get_float();
+#pragma unroll
+                                for (int k = 0; k < K; ++k)
+                                {
+                                        const float c = l.radiance.c[lane + LANES * k] * camera_beta[t_count - 1][k];
+                                        color[k] += c * mis;
+                                }
                         }
-                        break;
-                }
-                default:
-                        r.n = used; // unknown record: stop (tapes are written by paths_record_kernel only)
-                        break;
+                        else if (kind == static_cast<int>(TapeRecord::STRATEGY_LIGHT))
+                        {
+                                r.get_int(); // t
+                                const Material<T, C>& m = materials[r.get_int()];
+                                const BrdfTerms t = r.get_terms();
+                                const Light<N, T, C>& l = lights[r.get_int()];
+                                const float lk = r.get_float();
+                                const float mis = r.get_float();
+#pragma unroll
+                                for (int k = 0; k < K; ++k)
+                                {
+                                        const int ch = lane + LANES * k;
+                                        const float b = brdf_channel(t, m.f0.c[ch], m.rho_ss.c[ch], fresnel_a, fresnel_b);
+                                        const float c = ((camera_beta[t_count - 1][k] * b) * l.radiance.c[ch]) * lk;
+                                        color[k] += c * mis;
+                                }
+                        }
+                        else if (kind == static_cast<int>(TapeRecord::STRATEGY_CONNECT))
+                        {
+                                r.get_int(); // s
+                                r.get_int(); // t
+                                const Material<T, C>& mc = materials[r.get_int()];
+                                const BrdfTerms tc = r.get_terms();
+                                const Material<T, C>& ml = materials[r.get_int()];
+                                const BrdfTerms tl = r.get_terms();
+                                const float gk = r.get_float();
+                                const float mis = r.get_float();
+#pragma unroll
+                                for (int k = 0; k < K; ++k)
+                                {
+                                        const int ch = lane + LANES * k;
+                                        const float bc =
+                                                brdf_channel(tc, mc.f0.c[ch], mc.rho_ss.c[ch], fresnel_a, fresnel_b);
+                                        const float bl =
+                                                brdf_channel(tl, ml.f0.c[ch], ml.rho_ss.c[ch], fresnel_a, fresnel_b);
+                                        const float c0 =
+                                                ((camera_beta[t_count - 1][k] * bc) * bl) * light_beta[s_count - 1][k];
+                                        const float c = c0 * gk;
+                                        color[k] += c * mis;
+                                }
+                        }
                 }
         }
         float* const out = colors + i * C;
 #pragma unroll
         for (int k = 0; k < K; ++k)
         {
-                out[lane + 32 * k] = has ? color[k] : 0.0f;
+                out[lane + LANES * k] = has ? color[k] : 0.0f;
         }
-        // luminance: max(0, c_j) * y_j summed for j = 0, 1, ..., C - 1 in order
-        float sum = 0.0f;
+        if constexpr (LANES == 1)
+        {
+                Color<C> c;
 #pragma unroll
-        for (int k = 0; k < K; ++k)
-        {
-                const float mine = max_value(0.0f, color[k]) * cie_y[lane + 32 * k];
-                for (int j = 0; j < 32; ++j)
+                for (int k = 0; k < C; ++k)
                 {
-                        const float v = __shfl_sync(0xffffffffu, mine, j);
-                        sum = (k == 0 && j == 0) ? v : sum + v;
+                        c.c[k] = color[k];
                 }
+                lum[i] = has ? luminance(c, cie_y) : 0.0f;
         }
-        if (lane == 0)
+        else
         {
-                lum[i] = has ? sum : 0.0f;
+                static_assert(LANES == 32);
+                // max(0, c_j) * y_j summed for j = 0, 1, ..., C - 1 in order
+                float sum = 0.0f;
+#pragma unroll
+                for (int k = 0; k < K; ++k)
+                {
+                        const float mine = max_value(0.0f, color[k]) * cie_y[lane + 32 * k];
+                        for (int j = 0; j < 32; ++j)
+                        {
+                                const float v = __shfl_sync(0xffffffffu, mine, j);
+                                sum = (k == 0 && j == 0) ? v : sum + v;
+                        }
+                }
+                if (lane == 0)
+                {
+                        lum[i] = has ? sum : 0.0f;
+                }
         }
 }
 

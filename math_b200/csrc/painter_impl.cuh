@@ -372,8 +372,8 @@ class SceneT final : public Scene
         long long node_total_ = 0;
 
         DeviceScene<N, T, C> device_{};
-        // channel-0 view of the materials and lights, for tracing spectral
-        // paths with one channel (tape.cuh)
+        // channel-0 view of the materials and lights, for tracing paths with
+        // one colour channel (tape.cuh)
         DeviceArray<Material<T, 1>> d_materials_1_;
         DeviceArray<Light<N, T, 1>> d_lights_1_;
         DeviceScene<N, T, 1> device_1_{};
@@ -1121,7 +1121,6 @@ public:
                 device_.shading.f1_albedo = d_f1_albedo_.get();
                 device_.shading.f1_average = d_f1_average_.get();
 
-                if constexpr (C > 3)
                 {
                         std::vector<Material<T, 1>> m1(materials_.size());
                         for (std::size_t i = 0; i < materials_.size(); ++i)
@@ -1382,7 +1381,7 @@ __global__ void light_sample_kernel(
         Pcg g = seed_seq_pcg(seed, seed_words);
         QueryCounters counters{0, 0, 0, 0};
         const SceneQueries<N, T, C> q{scene, counters};
-        const Bpt<N, T, C> b{q, scene, g, 1};
+        const Bpt<N, T, C> b{q, scene, g, 1, nullptr, nullptr};
         const Light<N, T, C>& l = scene.lights[light];
         if (kind == 0)
         {
@@ -1444,15 +1443,21 @@ class PainterT final : public Painter
         DeviceArray<PathStats> stats_;
         DeviceArray<float> rgb_;
         DeviceArray<float> rgba_;
-        // spectral colour: path tapes of one chunk of pixels (tape.cuh)
+        // per-path buffers of one chunk of pixels: subpath vertices, random
+        // stream states, tapes (tape.cuh) and the queued strategies
         int tape_words_ = 0;
         long long chunk_pixels_ = 0;
+        DeviceArray<PathVertex<N, T, 1>> vertices_;
+        DeviceArray<Pcg> rng_;
         DeviceArray<std::uint32_t> tape_;
+        DeviceArray<std::uint32_t> tasks_;
+        DeviceArray<unsigned> task_count_;
+        int connect_blocks_ = 0;
         long long launches_ = 0;
         Statistics statistics_{};
 
-        // device memory for the tapes of one chunk
-        static constexpr long long TAPE_BUDGET = 4LL << 30;
+        // device memory for the per-path buffers of one chunk
+        static constexpr long long CHUNK_BUDGET = 4LL << 30;
 
 public:
         PainterT(const SceneT<N, T, C>* scene, const int spp, const int max_depth, const std::uint32_t seed)
@@ -1500,12 +1505,25 @@ public:
                 stats_.allocate(1);
                 rgb_.allocate(pixels_ * 3);
                 rgba_.allocate(pixels_ * 4);
-                if constexpr (C > 3)
                 {
                         tape_words_ = tape_words(max_depth_);
-                        const long long per_pixel = static_cast<long long>(spp_) * tape_words_ * 4;
-                        chunk_pixels_ = std::max(1LL, std::min(pixels_, TAPE_BUDGET / per_pixel));
-                        tape_.allocate(chunk_pixels_ * spp_ * tape_words_);
+                        const long long per_path = static_cast<long long>(tape_words_) * 4 +
+                                                   2LL * (max_depth_ + 1) * sizeof(PathVertex<N, T, 1>) +
+                                                   sizeof(Pcg) + 4LL * tape_slot_count(max_depth_);
+                        const long long per_pixel = per_path * spp_;
+                        chunk_pixels_ = std::max(1LL, std::min(pixels_, CHUNK_BUDGET / per_pixel));
+                        chunk_pixels_ = std::min(chunk_pixels_, (TASK_MAX_PATHS - 1) / spp_);
+                        const long long paths = chunk_pixels_ * spp_;
+                        tape_.allocate(paths * tape_words_);
+                        vertices_.allocate(paths * 2 * (max_depth_ + 1));
+                        rng_.allocate(paths);
+                        tasks_.allocate(paths * tape_slot_count(max_depth_));
+                        task_count_.allocate(1);
+                        int device = 0;
+                        int sms = 0;
+                        NBPT_CUDA(cudaGetDevice(&device));
+                        NBPT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+                        connect_blocks_ = sms * NBPT_PATHS_MIN_BLOCKS;
                 }
 
                 NBPT_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
@@ -1551,36 +1569,37 @@ public:
                         NBPT_CUDA(cudaGetLastError());
                         NBPT_CUDA(cudaEventRecord(ev_paths_, stream_));
                         long long launches = 2;
-                        if constexpr (C > 3)
                         {
-                                // trace with channel 0 and record, then colour every
-                                // channel from the tapes, one chunk of pixels at a time
+                                // per chunk of pixels: subpaths, strategies, the s = 1
+                                // strategies, then the colours (kernels.cuh)
                                 const DeviceScene<N, T, 1>& scene_1 = scene_->device_channel_0();
                                 for (long long b = 0; b < pixels_; b += chunk_pixels_)
                                 {
                                         const long long e = std::min(pixels_, b + chunk_pixels_);
                                         const long long n = (e - b) * spp_;
-                                        paths_record_kernel<N, T><<<blocks_for(n, 128), 128, 0, stream_>>>(
+                                        NBPT_CUDA(cudaMemsetAsync(task_count_.get(), 0, sizeof(unsigned), stream_));
+                                        paths_walk_kernel<N, T><<<blocks_for(n, 128), 128, 0, stream_>>>(
                                                 scene_1, b, e, spp_, max_depth_, seed_, pass, points_.get() + b * spp_ * (N - 1),
-                                                tape_.get(), tape_words_, valid_.get() + b * spp_, stats_.get());
+                                                vertices_.get(), rng_.get(), tape_.get(), tape_words_, valid_.get() + b * spp_,
+                                                tasks_.get(), task_count_.get(), stats_.get());
                                         NBPT_CUDA(cudaGetLastError());
-                                        paths_replay_kernel<N, T, C><<<blocks_for(n * 32, 128), 128, 0, stream_>>>(
+                                        paths_connect_kernel<N, T><<<connect_blocks_, 128, 0, stream_>>>(
+                                                scene_1, max_depth_, vertices_.get(), tape_.get(), tape_words_, tasks_.get(),
+                                                task_count_.get(), stats_.get());
+                                        NBPT_CUDA(cudaGetLastError());
+                                        paths_light_kernel<N, T><<<blocks_for(n, 128), 128, 0, stream_>>>(
+                                                scene_1, n, max_depth_, vertices_.get(), rng_.get(), tape_.get(), tape_words_,
+                                                stats_.get());
+                                        NBPT_CUDA(cudaGetLastError());
+                                        constexpr int LANES = C % 32 == 0 ? 32 : 1;
+                                        paths_replay_kernel<N, T, C, LANES><<<blocks_for(n * LANES, 128), 128, 0, stream_>>>(
                                                 scene_->device_materials(), scene_->device_lights(),
-                                                scene.shading.fresnel_a, scene.shading.fresnel_b, n, tape_.get(),
+                                                scene.shading.fresnel_a, scene.shading.fresnel_b, max_depth_, n, tape_.get(),
                                                 tape_words_, colors_.get() + b * spp_ * C, lum_.get() + b * spp_,
                                                 scene_->cie() + 64);
                                         NBPT_CUDA(cudaGetLastError());
-                                        launches += 2;
+                                        launches += 4;
                                 }
-                        }
-                        else
-                        {
-                                const long long paths = pixels_ * spp_;
-                                paths_kernel<N, T, C><<<blocks_for(paths, 128), 128, 0, stream_>>>(
-                                        scene, 0, pixels_, spp_, max_depth_, seed_, pass, points_.get(), colors_.get(),
-                                        lum_.get(), valid_.get(), scene_->cie() + 64, stats_.get());
-                                NBPT_CUDA(cudaGetLastError());
-                                launches += 1;
                         }
                         NBPT_CUDA(cudaEventRecord(ev_paths_end_, stream_));
                         Screen<N> screen;

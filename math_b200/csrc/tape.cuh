@@ -31,7 +31,9 @@ enum class TapeRecord : int
         STRATEGY_CONNECT = 6  // s, t, material_c, terms_c, material_l, terms_l, g, mis
 };
 
-inline constexpr int TAPE_HEADER = 2; // words used, valid
+// header: end of the bounce records, valid (not a background sample),
+// camera subpath size, light subpath size
+inline constexpr int TAPE_HEADER = 4;
 inline constexpr int TAPE_TERMS = 6;  // words of a BrdfTerms
 inline constexpr int TAPE_CAMERA_BOUNCE = 3 + TAPE_TERMS;
 inline constexpr int TAPE_LIGHT_START = 3;
@@ -40,15 +42,39 @@ inline constexpr int TAPE_STRATEGY_EMITTED = 4;
 inline constexpr int TAPE_STRATEGY_LIGHT = 6 + TAPE_TERMS;
 inline constexpr int TAPE_STRATEGY_CONNECT = 7 + 2 * TAPE_TERMS;
 
-// Words of one path's tape for a maximum depth: at most max_depth bounces on
-// each subpath and one record per (s, t) strategy with t >= 2 and
-// s + t - 2 <= max_depth.
+// Layout of one path's tape for a maximum depth D: the header; the bounce
+// records in the order they happen (at most D per subpath and the light
+// start); then one fixed slot of TAPE_STRATEGY_CONNECT words per (s, t)
+// strategy with 2 <= t <= D + 1, 0 <= s and s + t - 2 <= D, in the
+// reference's loop order (t outer, s inner).  A slot whose first word is 0
+// holds no contribution.
+NBPT_HD constexpr int tape_slots_begin(const int max_depth)
+{
+        return TAPE_HEADER + max_depth * TAPE_CAMERA_BOUNCE + TAPE_LIGHT_START + max_depth * TAPE_LIGHT_BOUNCE;
+}
+
+NBPT_HD constexpr int tape_slot_count(const int max_depth)
+{
+        return (max_depth + 1) * (max_depth + 2) / 2 - 1;
+}
+
+// index of strategy (s, t): slots of t' = 2 .. t - 1 (D + 3 - t' each), then s
+NBPT_HD constexpr int tape_slot(const int max_depth, const int t, const int s)
+{
+        return (t - 2) * (max_depth + 3) - ((t - 1) * t / 2 - 1) + s;
+}
+
+NBPT_HD constexpr int tape_slot_offset(const int max_depth, const int t, const int s)
+{
+        return tape_slots_begin(max_depth) + tape_slot(max_depth, t, s) * TAPE_STRATEGY_CONNECT;
+}
+
 NBPT_HD constexpr int tape_words(const int max_depth)
 {
-        const int strategies = (max_depth + 1) * (max_depth + 2) / 2;
-        return TAPE_HEADER + max_depth * TAPE_CAMERA_BOUNCE + TAPE_LIGHT_START + max_depth * TAPE_LIGHT_BOUNCE +
-               strategies * TAPE_STRATEGY_CONNECT;
+        return tape_slots_begin(max_depth) + tape_slot_count(max_depth) * TAPE_STRATEGY_CONNECT;
 }
+
+static_assert(tape_slot(6, 2, 6) == 6 && tape_slot(6, 3, 0) == 7 && tape_slot(6, 7, 1) == tape_slot_count(6) - 1);
 
 // Appends records to one path's tape (a contiguous slot of 32-bit words).
 struct TapeWriter final
