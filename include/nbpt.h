@@ -74,6 +74,12 @@ typedef struct nbpt_statistics
 const char* nbpt_last_error(void);
 int nbpt_device_count(void);
 
+/* Device buffers released by scenes and painters are cached by the library
+ * and reused by later scenes and painters of the same sizes, which spares
+ * jobs that follow one another the cost of cudaMalloc and cudaFree.  This
+ * returns the cached buffers to the driver; returns the bytes freed. */
+long long nbpt_release_cached_memory(void);
+
 /* ---- scene (scenes::create_storage_scene and the shape/light/projector factories) ---- */
 
 nbpt_scene* nbpt_scene_create(int dimension, int precision, int color);

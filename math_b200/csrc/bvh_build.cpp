@@ -1,6 +1,10 @@
 #include "bvh_build.h"
 
+#include <algorithm>
 #include <array>
+#include <thread>
+#include <future>
+#include <memory>
 #include <limits>
 #include <optional>
 #include <span>
@@ -12,6 +16,29 @@ namespace nbpt::host
 namespace
 {
 constexpr unsigned BUCKET_COUNT = 32;
+
+// Nodes of at least this many objects are binned by several threads.
+constexpr std::size_t PARALLEL_BINNING = 32768;
+constexpr unsigned THREADS = 8;
+
+// f(thread, begin, end) over [0, count) in THREADS parts
+template <typename F>
+void run_parallel(const std::size_t count, const F& f)
+{
+        std::vector<std::thread> threads;
+        const std::size_t step = (count + THREADS - 1) / THREADS;
+        for (unsigned t = 1; t < THREADS; ++t)
+        {
+                const std::size_t b = std::min(count, t * step);
+                const std::size_t e = std::min(count, b + step);
+                threads.emplace_back([&f, t, b, e] { f(t, b, e); });
+        }
+        f(0, 0, std::min(count, step));
+        for (std::thread& th : threads)
+        {
+                th.join();
+        }
+}
 
 template <int N, typename T>
 struct Box final
@@ -151,9 +178,28 @@ struct CenterBounds final
         explicit CenterBounds(const std::span<const Object<N, T>> objects)
         {
                 box = Box<N, T>::point(objects[0].center.data());
-                for (std::size_t i = 1; i < objects.size(); ++i)
+                if (objects.size() >= PARALLEL_BINNING)
                 {
-                        box.merge(objects[i].center.data());
+                        // component-wise min and max: the order of merging does not matter
+                        std::vector<Box<N, T>> part(THREADS, box);
+                        run_parallel(objects.size(), [&](const unsigned t, const std::size_t b, const std::size_t e)
+                                     {
+                                             for (std::size_t i = b; i < e; ++i)
+                                             {
+                                                     part[t].merge(objects[i].center.data());
+                                             }
+                                     });
+                        for (const Box<N, T>& p : part)
+                        {
+                                box.merge(p);
+                        }
+                }
+                else
+                {
+                        for (std::size_t i = 1; i < objects.size(); ++i)
+                        {
+                                box.merge(objects[i].center.data());
+                        }
                 }
                 axis = box.maximum_extent();
                 length_r = 1 / (box.hi[axis] - box.lo[axis]);
@@ -182,8 +228,13 @@ struct Split final
 };
 
 // bvh_split.h:273-314
+// uniform_sums: when every object has the same cost c, uniform_sums[k] is
+// the double sum of k copies of c added one at a time (the value the
+// sequential loop below forms for k objects), which lets large nodes be
+// binned in parallel with the same sums.
 template <int N, typename T>
-std::optional<Split<N, T>> split(std::span<Object<N, T>> objects, const Box<N, T>& bounds, const T interior_cost)
+std::optional<Split<N, T>> split(std::span<Object<N, T>> objects, const Box<N, T>& bounds, const T interior_cost,
+                                 const std::vector<double>* const uniform_sums)
 {
         if (objects.size() == 1)
         {
@@ -198,20 +249,79 @@ std::optional<Split<N, T>> split(std::span<Object<N, T>> objects, const Box<N, T
         std::array<double, BUCKET_COUNT> sum{};
         std::array<std::optional<Bucket<N, T>>, BUCKET_COUNT> buckets;
         double total = 0;
-        for (const Object<N, T>& o : objects)
+        if (uniform_sums && objects.size() >= PARALLEL_BINNING)
         {
-                total += o.cost;
-                const unsigned i = cb.bucket(o);
-                if (buckets[i])
+                // per-thread buckets over contiguous ranges, merged in range
+                // order: each bucket's bounds are the same component-wise min
+                // and max, its count the same, and its cost sum is looked up
+                struct Part final
                 {
-                        buckets[i]->bounds.merge(o.bounds);
-                        sum[i] += o.cost;
+                        std::array<std::optional<Box<N, T>>, BUCKET_COUNT> bounds;
+                        std::array<std::size_t, BUCKET_COUNT> count{};
+                };
+                std::vector<Part> parts(THREADS);
+                run_parallel(objects.size(), [&](const unsigned t, const std::size_t b, const std::size_t e)
+                             {
+                                     Part& part = parts[t];
+                                     for (std::size_t k = b; k < e; ++k)
+                                     {
+                                             const Object<N, T>& o = objects[k];
+                                             const unsigned i = cb.bucket(o);
+                                             if (part.bounds[i])
+                                             {
+                                                     part.bounds[i]->merge(o.bounds);
+                                             }
+                                             else
+                                             {
+                                                     part.bounds[i] = o.bounds;
+                                             }
+                                             ++part.count[i];
+                                     }
+                             });
+                std::array<std::size_t, BUCKET_COUNT> count{};
+                for (const Part& part : parts)
+                {
+                        for (unsigned i = 0; i < BUCKET_COUNT; ++i)
+                        {
+                                if (!part.bounds[i])
+                                {
+                                        continue;
+                                }
+                                if (buckets[i])
+                                {
+                                        buckets[i]->bounds.merge(*part.bounds[i]);
+                                }
+                                else
+                                {
+                                        buckets[i].emplace();
+                                        buckets[i]->bounds = *part.bounds[i];
+                                }
+                                count[i] += part.count[i];
+                        }
                 }
-                else
+                for (unsigned i = 0; i < BUCKET_COUNT; ++i)
                 {
-                        buckets[i].emplace();
-                        buckets[i]->bounds = o.bounds;
-                        sum[i] = o.cost;
+                        sum[i] = (*uniform_sums)[count[i]];
+                }
+                total = (*uniform_sums)[objects.size()];
+        }
+        else
+        {
+                for (const Object<N, T>& o : objects)
+                {
+                        total += o.cost;
+                        const unsigned i = cb.bucket(o);
+                        if (buckets[i])
+                        {
+                                buckets[i]->bounds.merge(o.bounds);
+                                sum[i] += o.cost;
+                        }
+                        else
+                        {
+                                buckets[i].emplace();
+                                buckets[i]->bounds = o.bounds;
+                                sum[i] = o.cost;
+                        }
                 }
         }
         for (unsigned i = 0; i < BUCKET_COUNT; ++i)
@@ -326,10 +436,65 @@ std::optional<Split<N, T>> split(std::span<Object<N, T>> objects, const Box<N, T
         return Split<N, T>{first, forward[index].bounds, backward[index].bounds, cb.axis};
 }
 
+// The tree is built with subtrees of large nodes on separate threads (a
+// node's split depends only on its own objects, and sibling subtrees
+// partition disjoint ranges), then laid out depth first in one pass, so the
+// result is the same node for node as a sequential depth-first build.
 template <int N, typename T>
-struct Builder final
+struct TreeNode final
 {
-        T interior_cost;
+        Box<N, T> bounds;
+        unsigned axis = 0;
+        std::unique_ptr<TreeNode> first;
+        std::unique_ptr<TreeNode> second;
+        std::span<Object<N, T>> objects; // leaves
+};
+
+inline constexpr std::size_t PARALLEL_OBJECTS = 8192;
+inline constexpr int PARALLEL_DEPTH = 5; // up to 2^5 concurrent subtrees
+
+template <int N, typename T>
+std::unique_ptr<TreeNode<N, T>> build_tree(
+        const std::span<Object<N, T>> objects,
+        const Box<N, T>& bounds,
+        const T interior_cost,
+        const std::vector<double>* const uniform_sums,
+        const int depth)
+{
+        auto node = std::make_unique<TreeNode<N, T>>();
+        node->bounds = bounds;
+        const std::optional<Split<N, T>> s = split(objects, bounds, interior_cost, uniform_sums);
+        if (!s)
+        {
+                node->objects = objects;
+                return node;
+        }
+        node->axis = s->axis;
+        const std::span<Object<N, T>> a = objects.subspan(0, s->middle);
+        const std::span<Object<N, T>> b = objects.subspan(s->middle);
+        if (depth < PARALLEL_DEPTH && objects.size() >= PARALLEL_OBJECTS)
+        {
+                std::future<std::unique_ptr<TreeNode<N, T>>> f = std::async(
+                        std::launch::async, [&]
+                        {
+                                return build_tree(a, s->bounds_min, interior_cost, uniform_sums, depth + 1);
+                        });
+                node->second = build_tree(b, s->bounds_max, interior_cost, uniform_sums, depth + 1);
+                node->first = f.get();
+        }
+        else
+        {
+                node->first = build_tree(a, s->bounds_min, interior_cost, uniform_sums, depth + 1);
+                node->second = build_tree(b, s->bounds_max, interior_cost, uniform_sums, depth + 1);
+        }
+        return node;
+}
+
+// Depth-first layout (bvh.cpp:35-67): a node, its first subtree, its second
+// subtree; an interior node stores the index of its second child.
+template <int N, typename T>
+struct Layout final
+{
         BuiltBvh<N, T>* out;
 
         unsigned push_node(const Box<N, T>& b)
@@ -346,25 +511,22 @@ struct Builder final
                 return index;
         }
 
-        // Builds the subtree of `objects` in depth-first order and returns its
-        // root node index (bvh.cpp:35-67).
-        unsigned build(const std::span<Object<N, T>> objects, const Box<N, T>& bounds)
+        unsigned place(const TreeNode<N, T>& t)
         {
-                const unsigned node = push_node(bounds);
-                const std::optional<Split<N, T>> s = split(objects, bounds, interior_cost);
-                if (!s)
+                const unsigned node = push_node(t.bounds);
+                if (!t.first)
                 {
                         out->offset[node] = out->indices.size();
-                        out->count[node] = objects.size();
-                        for (const Object<N, T>& o : objects)
+                        out->count[node] = t.objects.size();
+                        for (const Object<N, T>& o : t.objects)
                         {
                                 out->indices.push_back(o.index);
                         }
                         return node;
                 }
-                out->axis[node] = s->axis;
-                build(objects.subspan(0, s->middle), s->bounds_min);
-                const unsigned second = build(objects.subspan(s->middle), s->bounds_max);
+                out->axis[node] = t.axis;
+                place(*t.first);
+                const unsigned second = place(*t.second);
                 out->offset[node] = second;
                 return node;
         }
@@ -401,10 +563,22 @@ BuiltBvh<N, T> build_facet_bvh(const std::vector<T>& vertices, const std::vector
                 root.merge(objects[f].bounds);
         }
 
+        // every facet costs the same: the running sums of that cost
+        std::vector<double> uniform_sums(count + 1);
+        uniform_sums[0] = 0;
+        uniform_sums[1] = facet_cost;
+        for (std::size_t k = 2; k <= count; ++k)
+        {
+                uniform_sums[k] = uniform_sums[k - 1] + facet_cost;
+        }
+        const std::unique_ptr<TreeNode<N, T>> tree = build_tree(
+                std::span<Object<N, T>>(objects), root, static_cast<T>(2 * box_r_cost), &uniform_sums, 0);
         BuiltBvh<N, T> out;
         out.indices.reserve(count);
-        Builder<N, T> builder{static_cast<T>(2 * box_r_cost), &out};
-        builder.build(std::span<Object<N, T>>(objects), root);
+        out.lo.reserve(4 * count * N);
+        out.hi.reserve(4 * count * N);
+        Layout<N, T> layout{&out};
+        layout.place(*tree);
         return out;
 }
 

@@ -3,6 +3,7 @@
 #include "../../include/nbpt.h"
 
 #include "core.cuh"
+#include "device_pool.h"
 #include "painter_api.h"
 
 #include <cuda_runtime.h>
@@ -216,6 +217,18 @@ extern "C"
 const char* nbpt_last_error(void)
 {
         return g_error.c_str();
+}
+
+long long nbpt_release_cached_memory(void)
+{
+        long long r = NBPT_ERROR;
+        guarded(
+                [&]
+                {
+                        r = static_cast<long long>(nbpt::pool::trim());
+                        return 0;
+                });
+        return r;
 }
 
 int nbpt_device_count(void)

@@ -12,6 +12,7 @@
 #pragma once
 
 #include "bvh_build.h"
+#include "device_pool.h"
 #include "estimator.cuh"
 #include "host_math.h"
 #include "kernels.cuh"
@@ -20,6 +21,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <array>
 #include <cmath>
 #include <cstring>
@@ -27,6 +29,7 @@
 #include <stdexcept>
 #include <string>
 #include <type_traits>
+#include <thread>
 #include <vector>
 
 namespace nbpt
@@ -46,6 +49,16 @@ class DeviceArray final
 {
         X* ptr_ = nullptr;
         std::size_t size_ = 0;
+        int device_ = 0;
+
+        void release()
+        {
+                if (ptr_)
+                {
+                        pool::release(ptr_, size_ * sizeof(X), device_);
+                        ptr_ = nullptr;
+                }
+        }
 
 public:
         DeviceArray() = default;
@@ -54,23 +67,16 @@ public:
 
         ~DeviceArray()
         {
-                if (ptr_)
-                {
-                        cudaFree(ptr_);
-                }
+                release();
         }
 
         void allocate(const std::size_t n)
         {
-                if (ptr_)
-                {
-                        cudaFree(ptr_);
-                        ptr_ = nullptr;
-                }
+                release();
                 size_ = n;
                 if (n > 0)
                 {
-                        NBPT_CUDA(cudaMalloc(&ptr_, n * sizeof(X)));
+                        ptr_ = static_cast<X*>(pool::allocate(n * sizeof(X), &device_));
                 }
         }
 
@@ -190,30 +196,104 @@ std::array<T, M * M> inverse(std::array<T, M * M> a)
         return b;
 }
 
+// Runs f(begin, end) over [0, count) split across the host's threads.
+template <typename F>
+void parallel_ranges(const std::size_t count, const F& f)
+{
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+        const std::size_t parts = std::min<std::size_t>(hw, std::max<std::size_t>(1, count / 4096));
+        if (parts <= 1)
+        {
+                f(std::size_t{0}, count);
+                return;
+        }
+        std::vector<std::thread> threads;
+        threads.reserve(parts - 1);
+        const std::size_t step = (count + parts - 1) / parts;
+        for (std::size_t p = 1; p < parts; ++p)
+        {
+                const std::size_t b = std::min(count, p * step);
+                const std::size_t e = std::min(count, b + step);
+                threads.emplace_back(
+                        [&f, b, e]
+                        {
+                                f(b, e);
+                        });
+        }
+        f(std::size_t{0}, std::min(count, step));
+        for (std::thread& t : threads)
+        {
+                t.join();
+        }
+}
+
 // Vertex normals of a simplex mesh: per vertex, the facet normals around it
 // weighted by the facet's solid angle at the vertex (n = 3, 4) or 1
 // (n >= 5), oriented consistently and averaged
-// (after src/model/mesh/normals.cpp:46-195).
+// (after src/model/mesh/normals.cpp:46-195).  Facet normals and angles are
+// computed in parallel; the sums run over the facets in order.
 template <int N>
 std::vector<float> vertex_normals(const std::vector<float>& points, const std::vector<int>& facets)
 {
         const std::size_t vcount = points.size() / N;
         const std::size_t fcount = facets.size() / N;
         std::vector<Vec<N, double>> fn(fcount);
-        for (std::size_t f = 0; f < fcount; ++f)
-        {
-                Vec<N, double> e[N - 1];
-                const int i0 = facets[f * N];
-                for (int k = 0; k < N - 1; ++k)
+        std::vector<double> weight(fcount * N, 1.0);
+        parallel_ranges(
+                fcount,
+                [&](const std::size_t begin, const std::size_t end)
                 {
-                        for (int d = 0; d < N; ++d)
+                        for (std::size_t f = begin; f < end; ++f)
                         {
-                                e[k][d] = static_cast<double>(points[facets[f * N + k + 1] * static_cast<std::size_t>(N) + d]) -
-                                          static_cast<double>(points[i0 * static_cast<std::size_t>(N) + d]);
+                                Vec<N, double> e[N - 1];
+                                const int i0 = facets[f * N];
+                                for (int k = 0; k < N - 1; ++k)
+                                {
+                                        for (int d = 0; d < N; ++d)
+                                        {
+                                                e[k][d] = static_cast<double>(
+                                                                  points[facets[f * N + k + 1] * static_cast<std::size_t>(N) + d]) -
+                                                          static_cast<double>(points[i0 * static_cast<std::size_t>(N) + d]);
+                                        }
+                                }
+                                fn[f] = orthogonal_complement(e).normalized();
+                                if constexpr (N == 3 || N == 4)
+                                {
+                                        for (int k = 0; k < N; ++k)
+                                        {
+                                                const int v = facets[f * N + k];
+                                                Vec<N, double> a[N - 1];
+                                                for (int j = 0; j < N - 1; ++j)
+                                                {
+                                                        const int o = facets[f * N + (k + 1 + j) % N];
+                                                        for (int d = 0; d < N; ++d)
+                                                        {
+                                                                a[j][d] = static_cast<double>(points[o * static_cast<std::size_t>(N) + d]) -
+                                                                          static_cast<double>(points[v * static_cast<std::size_t>(N) + d]);
+                                                        }
+                                                        a[j] = a[j].normalized();
+                                                }
+                                                if constexpr (N == 3)
+                                                {
+                                                        weight[f * N + k] = std::acos(std::fmax(-1.0, std::fmin(1.0, dot(a[0], a[1]))));
+                                                }
+                                                else
+                                                {
+                                                        // solid angle of the spherical triangle
+                                                        // (Van Oosterom-Strackee); |det| of the three unit
+                                                        // vectors within their 3-space is the norm of their
+                                                        // orthogonal complement
+                                                        Vec<N, double> c3[N - 1] = {a[0], a[1], a[2]};
+                                                        const double det = orthogonal_complement(c3).norm();
+                                                        const double d01 = dot(a[0], a[1]);
+                                                        const double d02 = dot(a[0], a[2]);
+                                                        const double d12 = dot(a[1], a[2]);
+                                                        weight[f * N + k] = 2 * std::atan2(det, 1 + d01 + d02 + d12);
+                                                }
+                                        }
+                                }
                         }
-                }
-                fn[f] = orthogonal_complement(e).normalized();
-        }
+                });
         std::vector<Vec<N, double>> sum(vcount, Vec<N, double>::filled(0));
         std::vector<Vec<N, double>> reference(vcount, Vec<N, double>::filled(0));
         std::vector<char> has_reference(vcount, 0);
@@ -222,46 +302,12 @@ std::vector<float> vertex_normals(const std::vector<float>& points, const std::v
                 for (int k = 0; k < N; ++k)
                 {
                         const int v = facets[f * N + k];
-                        double w = 1;
-                        if constexpr (N == 3 || N == 4)
-                        {
-                                Vec<N, double> a[N - 1];
-                                for (int j = 0; j < N - 1; ++j)
-                                {
-                                        const int o = facets[f * N + (k + 1 + j) % N];
-                                        for (int d = 0; d < N; ++d)
-                                        {
-                                                a[j][d] = static_cast<double>(points[o * static_cast<std::size_t>(N) + d]) -
-                                                          static_cast<double>(points[v * static_cast<std::size_t>(N) + d]);
-                                        }
-                                        a[j] = a[j].normalized();
-                                }
-                                if constexpr (N == 3)
-                                {
-                                        w = std::acos(std::fmax(-1.0, std::fmin(1.0, dot(a[0], a[1]))));
-                                }
-                                else
-                                {
-                                        // solid angle of the spherical triangle (Van Oosterom-Strackee)
-                                        const Vec<3, double> p{{a[0][0], a[0][1], a[0][2]}};
-                                        (void)p;
-                                        Vec<N, double> c3[N - 1] = {a[0], a[1], a[2]};
-                                        Vec<N, double> n4 = orthogonal_complement(c3);
-                                        // |det| of the three unit vectors within their 3-space: the
-                                        // norm of their orthogonal complement
-                                        const double det = n4.norm();
-                                        const double d01 = dot(a[0], a[1]);
-                                        const double d02 = dot(a[0], a[2]);
-                                        const double d12 = dot(a[1], a[2]);
-                                        w = 2 * std::atan2(det, 1 + d01 + d02 + d12);
-                                }
-                        }
                         if (!has_reference[v])
                         {
                                 reference[v] = fn[f];
                                 has_reference[v] = 1;
                         }
-                        const Vec<N, double> wn = fn[f] * w;
+                        const Vec<N, double> wn = fn[f] * weight[f * N + k];
                         if (dot(fn[f], reference[v]) >= 0)
                         {
                                 sum[v] = sum[v] + wn;

@@ -52,6 +52,7 @@ class Statistics(ctypes.Structure):
 # (name, restype, argtypes) of every exported function, in include/nbpt.h order
 SIGNATURES = [
     ("nbpt_last_error", ctypes.c_char_p, []),
+    ("nbpt_release_cached_memory", ctypes.c_longlong, []),
     ("nbpt_device_count", ctypes.c_int, []),
     ("nbpt_scene_create", _P, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("nbpt_scene_destroy", None, [_P]),
