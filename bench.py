@@ -145,11 +145,11 @@ def cpu_baseline(small: bool, seconds_hint: float = 20.0) -> dict:
                        f"ray_count {stats['ray_count']})")}
 
 
-# DRAM bytes (read + write) per path of one paths_kernel launch on this
-# workload in float, from the ncu capture summarised in
-# profiles/paths_kernel_cornell4d_32.md (a 32^3 screen of the same scene;
+# DRAM bytes (read + write) per path of the path kernels (walk, connect,
+# light, replay) on this workload in float, from the ncu capture summarised
+# in profiles/path_kernels_cornell4d_32.md (a 32^3 screen of the same scene;
 # traffic scales with the number of paths)
-TRAFFIC_PER_PATH = {"float": 18496.0}
+TRAFFIC_PER_PATH = {"float": 28115.0}
 
 
 def record_bytes(n: int, precision: str) -> dict:
@@ -303,8 +303,8 @@ def run_nbpt(args, rank: int, world: int, local: int):
                 "frac": (achieved / peak) if achieved else None,
                 "traffic": (TRAFFIC_PER_PATH[args.precision] * paths_per_step
                             if args.precision in TRAFFIC_PER_PATH and not args.small else None),
-                "traffic_source": "profiles/paths_kernel_cornell4d_32.md (per path, scaled to one launch)",
-                "kernel": "paths_kernel",
+                "traffic_source": "profiles/path_kernels_cornell4d_32.md (per path, scaled to one pass)",
+                "kernel": "path kernels (walk, connect, light, replay)",
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 "algorithmic_bytes_per_path": algorithmic / (paths_per_step * args.steps),
                 "node_visits_per_path": nodes / (paths_per_step * args.steps),
