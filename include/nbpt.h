@@ -174,6 +174,49 @@ int nbpt_painter_statistics(nbpt_painter* painter, nbpt_statistics* statistics);
  * that order their own work or events with it */
 void* nbpt_painter_stream(nbpt_painter* painter);
 
+/* ---- job server: continuous batching of renders on one GPU ----
+ *
+ * No single reference function: the reference runs one painter per render,
+ * each with its own worker threads (src/painter/painter.cpp:77-134).  The
+ * server runs the passes of many painters at once, each on its own CUDA
+ * stream, keeping one pass of every admitted job in flight; jobs submitted
+ * while others run are admitted as soon as a slot and device memory allow.
+ * Results do not depend on what runs beside a job. */
+typedef struct nbpt_server nbpt_server;
+
+enum nbpt_job_state
+{
+        NBPT_JOB_QUEUED = 0,
+        NBPT_JOB_RUNNING = 1,
+        NBPT_JOB_DONE = 2,
+        NBPT_JOB_FAILED = 3
+};
+
+typedef struct nbpt_job_info
+{
+        int state;            /* nbpt_job_state */
+        int passes;
+        int passes_done;
+        long long footprint;  /* device bytes of the painter and its scene */
+        double submitted;     /* seconds since the server started */
+        double started;       /* admitted; -1 while queued */
+        double finished;      /* done or failed; -1 before */
+} nbpt_job_info;
+
+/* max_jobs jobs run at once within memory_budget device bytes (0: 80 % of
+ * the free device memory); a job larger than the budget runs alone. */
+nbpt_server* nbpt_server_create(int max_jobs, long long memory_budget);
+/* finishes the running jobs, fails the queued ones */
+void nbpt_server_destroy(nbpt_server* server);
+/* queues `passes` passes of a painter; returns the job id.  The painter and
+ * its scene must stay alive and unused by the caller until the job is done. */
+long long nbpt_server_submit(nbpt_server* server, nbpt_painter* painter, int passes);
+int nbpt_server_job(nbpt_server* server, long long job, nbpt_job_info* info);
+/* blocks until the job is done or failed; NBPT_ERROR (with the message) if it failed */
+int nbpt_server_wait(nbpt_server* server, long long job, nbpt_job_info* info);
+/* seconds since the server started, on the clock of nbpt_job_info */
+double nbpt_server_time(nbpt_server* server);
+
 /* ---- verification entry points (same arithmetic as the render path) ---- */
 
 /* closest hit (any = 0): kind (0 none, 1 flat, 2 solid, 3 facet), index,

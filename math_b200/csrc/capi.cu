@@ -5,6 +5,7 @@
 #include "core.cuh"
 #include "device_pool.h"
 #include "painter_api.h"
+#include "server.h"
 
 #include <cuda_runtime.h>
 
@@ -24,6 +25,11 @@ struct nbpt_scene
 struct nbpt_painter
 {
         std::unique_ptr<nbpt::Painter> impl;
+};
+
+struct nbpt_server
+{
+        std::unique_ptr<nbpt::Server> impl;
 };
 
 namespace
@@ -88,6 +94,30 @@ void require(const void* p, const char* what)
         {
                 throw std::runtime_error(std::string("null ") + what);
         }
+}
+
+nbpt::Server& server_of(nbpt_server* s)
+{
+        if (!s || !s->impl)
+        {
+                throw std::runtime_error("null server");
+        }
+        return *s->impl;
+}
+
+void copy_info(const nbpt::JobInfo& j, nbpt_job_info* info)
+{
+        if (!info)
+        {
+                return;
+        }
+        info->state = static_cast<int>(j.state);
+        info->passes = j.passes;
+        info->passes_done = j.passes_done;
+        info->footprint = j.footprint;
+        info->submitted = j.submitted;
+        info->started = j.started;
+        info->finished = j.finished;
 }
 
 void require_device()
@@ -612,6 +642,77 @@ void* nbpt_painter_stream(nbpt_painter* painter)
                         return 0;
                 });
         return s;
+}
+
+nbpt_server* nbpt_server_create(const int max_jobs, const long long memory_budget)
+{
+        nbpt_server* out = nullptr;
+        guarded(
+                [&]
+                {
+                        require_device();
+                        auto s = std::make_unique<nbpt_server>();
+                        s->impl = std::make_unique<nbpt::Server>(max_jobs, memory_budget);
+                        out = s.release();
+                        return 0;
+                });
+        return out;
+}
+
+void nbpt_server_destroy(nbpt_server* server)
+{
+        delete server;
+}
+
+
+long long nbpt_server_submit(nbpt_server* server, nbpt_painter* painter, const int passes)
+{
+        long long id = NBPT_ERROR;
+        guarded(
+                [&]
+                {
+                        id = server_of(server).submit(&painter_of(painter), passes);
+                        return 0;
+                });
+        return id;
+}
+
+int nbpt_server_job(nbpt_server* server, const long long job, nbpt_job_info* info)
+{
+        return guarded(
+                [&]
+                {
+                        require(info, "info");
+                        copy_info(server_of(server).info(job), info);
+                        return 0;
+                });
+}
+
+int nbpt_server_wait(nbpt_server* server, const long long job, nbpt_job_info* info)
+{
+        return guarded(
+                [&]
+                {
+                        const nbpt::JobInfo j = server_of(server).wait(job);
+                        copy_info(j, info);
+                        if (j.state == nbpt::JobState::FAILED)
+                        {
+                                throw std::runtime_error("job " + std::to_string(job) + " failed: " + j.error);
+                        }
+                        return 0;
+                });
+}
+
+double nbpt_server_time(nbpt_server* server)
+{
+        double t = -1;
+        guarded(
+                [&]
+                {
+                        t = server_of(server).now();
+                        return 0;
+                });
+        return t;
 }
 
 int nbpt_scene_trace(

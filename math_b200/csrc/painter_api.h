@@ -32,6 +32,8 @@ public:
         virtual void samples(double* points, float* colors, unsigned char* valid) = 0;
         virtual Statistics statistics() = 0;
         virtual void* stream() = 0;
+        // device bytes of the painter's buffers plus those of its scene
+        virtual long long device_bytes() const = 0;
 };
 
 class Scene

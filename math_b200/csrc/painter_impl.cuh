@@ -1597,6 +1597,15 @@ public:
                 }
         }
 
+        long long device_bytes() const override
+        {
+                const std::size_t own = offsets_.bytes() + points_.bytes() + colors_.bytes() + lum_.bytes() +
+                                        valid_.bytes() + state_.bytes() + stats_.bytes() + rgb_.bytes() +
+                                        rgba_.bytes() + vertices_.bytes() + rng_.bytes() + tape_.bytes() +
+                                        tasks_.bytes() + task_count_.bytes();
+                return static_cast<long long>(own) + scene_->device_bytes();
+        }
+
         void* stream() override
         {
                 return stream_;

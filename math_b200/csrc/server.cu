@@ -1,0 +1,283 @@
+// Render-job server (server.h).
+#include "server.h"
+
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <stdexcept>
+
+namespace nbpt
+{
+namespace
+{
+double steady_seconds()
+{
+        return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+} // namespace
+
+struct Server::Job final
+{
+        long long id;
+        Painter* painter;
+        int device;
+        JobInfo info;
+        cudaEvent_t done = nullptr; // marks the end of the pass in flight
+        bool pass_in_flight = false;
+};
+
+Server::Server(const int max_jobs, const long long memory_budget)
+        : max_jobs_(max_jobs),
+          budget_(memory_budget),
+          start_(steady_seconds())
+{
+        if (max_jobs < 1)
+        {
+                throw std::runtime_error("server needs at least one job slot");
+        }
+        if (memory_budget <= 0)
+        {
+                std::size_t free = 0;
+                std::size_t total = 0;
+                if (cudaMemGetInfo(&free, &total) != cudaSuccess)
+                {
+                        cudaGetLastError();
+                        throw std::runtime_error("no CUDA device for the server");
+                }
+                budget_ = static_cast<long long>(free * 0.8);
+        }
+        worker_ = std::thread(&Server::run, this);
+}
+
+Server::~Server()
+{
+        {
+                const std::lock_guard lock(mutex_);
+                stop_ = true;
+        }
+        changed_.notify_all();
+        worker_.join();
+}
+
+double Server::now() const
+{
+        return steady_seconds() - start_;
+}
+
+long long Server::submit(Painter* const painter, const int passes)
+{
+        if (!painter)
+        {
+                throw std::runtime_error("null painter");
+        }
+        if (passes < 1)
+        {
+                throw std::runtime_error("a job needs at least one pass");
+        }
+        auto job = std::make_shared<Job>();
+        job->painter = painter;
+        if (cudaGetDevice(&job->device) != cudaSuccess)
+        {
+                cudaGetLastError();
+                throw std::runtime_error("no CUDA device for the job");
+        }
+        job->info.state = JobState::QUEUED;
+        job->info.passes = passes;
+        job->info.passes_done = 0;
+        job->info.footprint = painter->device_bytes();
+        job->info.submitted = now();
+        job->info.started = -1;
+        job->info.finished = -1;
+        long long id = 0;
+        {
+                const std::lock_guard lock(mutex_);
+                if (stop_)
+                {
+                        throw std::runtime_error("the server is stopping");
+                }
+                id = next_id_++;
+                job->id = id;
+                jobs_[id] = job;
+                queue_.push_back(job);
+        }
+        changed_.notify_all();
+        return id;
+}
+
+JobInfo Server::info(const long long job) const
+{
+        const std::lock_guard lock(mutex_);
+        const auto i = jobs_.find(job);
+        if (i == jobs_.end())
+        {
+                throw std::runtime_error("unknown job " + std::to_string(job));
+        }
+        return i->second->info;
+}
+
+JobInfo Server::wait(const long long job)
+{
+        std::unique_lock lock(mutex_);
+        const auto i = jobs_.find(job);
+        if (i == jobs_.end())
+        {
+                throw std::runtime_error("unknown job " + std::to_string(job));
+        }
+        const std::shared_ptr<Job> j = i->second;
+        changed_.wait(lock,
+                      [&]
+                      {
+                              return j->info.state == JobState::DONE || j->info.state == JobState::FAILED;
+                      });
+        return j->info;
+}
+
+// Admits queued jobs in arrival order while a slot and the memory budget
+// allow; a job larger than the whole budget is admitted when nothing runs.
+bool Server::admit_locked()
+{
+        bool any = false;
+        while (!queue_.empty() && static_cast<int>(running_.size()) < max_jobs_)
+        {
+                const std::shared_ptr<Job>& j = queue_.front();
+                if (!running_.empty() && used_ + j->info.footprint > budget_)
+                {
+                        break;
+                }
+                used_ += j->info.footprint;
+                j->info.state = JobState::RUNNING;
+                j->info.started = now();
+                running_.push_back(j);
+                queue_.pop_front();
+                any = true;
+        }
+        return any;
+}
+
+void Server::finish_locked(Job& job, const JobState state, const std::string& error)
+{
+        job.info.state = state;
+        job.info.error = error;
+        job.info.finished = now();
+        used_ -= job.info.footprint;
+        if (job.done)
+        {
+                cudaSetDevice(job.device);
+                cudaEventDestroy(job.done);
+                job.done = nullptr;
+        }
+}
+
+// The worker keeps one pass of every running job in flight, on the job's own
+// stream, and retires passes as their events complete.
+void Server::run()
+{
+        while (true)
+        {
+                std::deque<std::shared_ptr<Job>> running;
+                {
+                        std::unique_lock lock(mutex_);
+                        if (stop_ && running_.empty())
+                        {
+                                for (const std::shared_ptr<Job>& j : queue_)
+                                {
+                                        j->info.state = JobState::FAILED;
+                                        j->info.error = "server stopped";
+                                        j->info.finished = now();
+                                }
+                                queue_.clear();
+                                changed_.notify_all();
+                                return;
+                        }
+                        if (!stop_)
+                        {
+                                admit_locked();
+                        }
+                        if (running_.empty())
+                        {
+                                changed_.wait_for(lock, std::chrono::milliseconds(5));
+                                continue;
+                        }
+                        running = running_;
+                }
+
+                bool progressed = false;
+                for (const std::shared_ptr<Job>& j : running)
+                {
+                        std::string error;
+                        bool finished = false;
+                        try
+                        {
+                                cudaSetDevice(j->device);
+                                if (j->pass_in_flight)
+                                {
+                                        const cudaError_t e = cudaEventQuery(j->done);
+                                        if (e == cudaErrorNotReady)
+                                        {
+                                                continue;
+                                        }
+                                        if (e != cudaSuccess)
+                                        {
+                                                throw std::runtime_error(std::string("pass failed: ") +
+                                                                         cudaGetErrorString(e));
+                                        }
+                                        j->pass_in_flight = false;
+                                        progressed = true;
+                                        {
+                                                const std::lock_guard lock(mutex_);
+                                                ++j->info.passes_done;
+                                        }
+                                        if (j->info.passes_done == j->info.passes)
+                                        {
+                                                j->painter->wait(); // statistics of the last pass
+                                                finished = true;
+                                        }
+                                }
+                                if (!finished && !j->pass_in_flight)
+                                {
+                                        if (!j->done)
+                                        {
+                                                if (cudaEventCreateWithFlags(&j->done, cudaEventDisableTiming) !=
+                                                    cudaSuccess)
+                                                {
+                                                        throw std::runtime_error("cudaEventCreate failed");
+                                                }
+                                        }
+                                        j->painter->enqueue_passes(1);
+                                        if (cudaEventRecord(j->done, static_cast<cudaStream_t>(j->painter->stream())) !=
+                                            cudaSuccess)
+                                        {
+                                                throw std::runtime_error("cudaEventRecord failed");
+                                        }
+                                        j->pass_in_flight = true;
+                                        progressed = true;
+                                }
+                        }
+                        catch (const std::exception& e)
+                        {
+                                error = e.what();
+                                cudaGetLastError();
+                        }
+                        if (finished || !error.empty())
+                        {
+                                const std::lock_guard lock(mutex_);
+                                finish_locked(*j, error.empty() ? JobState::DONE : JobState::FAILED, error);
+                                for (auto i = running_.begin(); i != running_.end(); ++i)
+                                {
+                                        if (i->get() == j.get())
+                                        {
+                                                running_.erase(i);
+                                                break;
+                                        }
+                                }
+                                admit_locked();
+                                changed_.notify_all();
+                        }
+                }
+                if (!progressed)
+                {
+                        std::this_thread::sleep_for(std::chrono::microseconds(50));
+                }
+        }
+}
+} // namespace nbpt

@@ -1,0 +1,82 @@
+// Render-job server: continuous batching of painters on one GPU.
+//
+// The reference renders one scene per painter, each painter with its own
+// worker threads (src/painter/painter.cpp:77-134).  On one GPU many small
+// renders would each leave most of the device idle, so the server runs many
+// painters' passes at once: every admitted job has its own CUDA stream (the
+// painter's), the server keeps one pass of every admitted job in flight, and
+// jobs that arrive while others run are admitted as soon as a slot and
+// device memory free up.  A job's result does not depend on what runs beside
+// it: every path's random stream is fixed by (seed, pass, pixel, sample).
+#pragma once
+
+#include "painter_api.h"
+
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+
+namespace nbpt
+{
+enum class JobState : int
+{
+        QUEUED = 0,
+        RUNNING = 1,
+        DONE = 2,
+        FAILED = 3
+};
+
+struct JobInfo final
+{
+        JobState state;
+        int passes;
+        int passes_done;
+        long long footprint; // device bytes counted against the budget
+        double submitted;    // seconds since the server started
+        double started;      // admitted (-1 while queued)
+        double finished;     // done or failed (-1 before)
+        std::string error;
+};
+
+class Server final
+{
+public:
+        // max_jobs: jobs admitted at once; memory_budget: device bytes the
+        // admitted jobs may hold (a job larger than the budget runs alone)
+        Server(int max_jobs, long long memory_budget);
+        ~Server();
+        Server(const Server&) = delete;
+        Server& operator=(const Server&) = delete;
+
+        // The painter (and its scene) must stay alive and untouched by the
+        // caller until the job is done or failed.
+        long long submit(Painter* painter, int passes);
+        JobInfo info(long long job) const;
+        JobInfo wait(long long job);
+        double now() const;
+
+private:
+        struct Job;
+
+        void run();
+        bool admit_locked();
+        void finish_locked(Job& job, JobState state, const std::string& error);
+
+        int max_jobs_;
+        long long budget_;
+        long long used_ = 0;
+        double start_;
+        mutable std::mutex mutex_;
+        std::condition_variable changed_;
+        std::map<long long, std::shared_ptr<Job>> jobs_;
+        std::deque<std::shared_ptr<Job>> queue_;
+        std::deque<std::shared_ptr<Job>> running_;
+        long long next_id_ = 0;
+        bool stop_ = false;
+        std::thread worker_;
+};
+} // namespace nbpt

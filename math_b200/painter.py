@@ -31,6 +31,21 @@ _B = ctypes.POINTER(ctypes.c_ubyte)
 _L = ctypes.POINTER(ctypes.c_longlong)
 
 
+class JobInfo(ctypes.Structure):
+    _fields_ = [
+        ("state", ctypes.c_int),
+        ("passes", ctypes.c_int),
+        ("passes_done", ctypes.c_int),
+        ("footprint", ctypes.c_longlong),
+        ("submitted", ctypes.c_double),
+        ("started", ctypes.c_double),
+        ("finished", ctypes.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class Statistics(ctypes.Structure):
     _fields_ = [
         ("pass_number", ctypes.c_longlong),
@@ -79,6 +94,12 @@ SIGNATURES = [
     ("nbpt_painter_samples", ctypes.c_int, [_P, _D, _F, _B]),
     ("nbpt_painter_statistics", ctypes.c_int, [_P, ctypes.POINTER(Statistics)]),
     ("nbpt_painter_stream", _P, [_P]),
+    ("nbpt_server_create", _P, [ctypes.c_int, ctypes.c_longlong]),
+    ("nbpt_server_destroy", None, [_P]),
+    ("nbpt_server_submit", ctypes.c_longlong, [_P, _P, ctypes.c_int]),
+    ("nbpt_server_job", ctypes.c_int, [_P, ctypes.c_longlong, ctypes.POINTER(JobInfo)]),
+    ("nbpt_server_wait", ctypes.c_int, [_P, ctypes.c_longlong, ctypes.POINTER(JobInfo)]),
+    ("nbpt_server_time", ctypes.c_double, [_P]),
     ("nbpt_scene_trace", ctypes.c_int, [_P, _D, ctypes.c_longlong, ctypes.c_int, _I, _I, _D, _D]),
     ("nbpt_scene_trace_noalloc", ctypes.c_int, [_P, _D, ctypes.c_longlong, ctypes.c_int, _I, _I, _D, _D]),
     ("nbpt_scene_mesh_export", ctypes.c_int, [_P, ctypes.c_int, _L, _D, _D, _D, _U, _U, _I]),
@@ -379,3 +400,39 @@ def test_sj_points(dimension: int, spp: int, seed_words, double: bool = True) ->
     out = np.zeros((count, dimension))
     _check(lib().nbpt_test_sj_points(dimension, 1 if double else 0, spp, _p(w, _U), k, _p(out, _D)))
     return out
+
+
+class Server:
+    """Continuous batching of renders on one GPU (nbpt_server_*): every
+    admitted job keeps one pass in flight on its painter's stream; jobs
+    submitted while others run are admitted as slots and memory free up."""
+
+    def __init__(self, max_jobs: int = 16, memory_budget: int = 0):
+        self.h = lib().nbpt_server_create(max_jobs, memory_budget)
+        if not self.h:
+            raise PainterError(lib().nbpt_last_error().decode())
+
+    def submit(self, painter: "Painter", passes: int = 1) -> int:
+        return _check(lib().nbpt_server_submit(self.h, painter.h, passes))
+
+    def job(self, job: int) -> dict:
+        info = JobInfo()
+        _check(lib().nbpt_server_job(self.h, job, ctypes.byref(info)))
+        return info.as_dict()
+
+    def wait(self, job: int) -> dict:
+        info = JobInfo()
+        _check(lib().nbpt_server_wait(self.h, job, ctypes.byref(info)))
+        return info.as_dict()
+
+    def time(self) -> float:
+        return lib().nbpt_server_time(self.h)
+
+    def close(self):
+        h = getattr(self, "h", None)
+        if h and _lib is not None:
+            _lib.nbpt_server_destroy(h)
+        self.h = None
+
+    def __del__(self):
+        self.close()

@@ -295,6 +295,56 @@ def cornell_5d(size=(16, 16, 16, 16), points: int = 2000, seed: int = 4) -> dict
             "projector": camera(n, 3.0, size), "background": [0.0, 0.0, 0.0]}
 
 
+def mixed_scene(n: int, points: int, size, seed: int) -> dict:
+    """A member of the mixed-scene batch: a box of parallelotope walls open
+    on one side, one parallelotope ceiling light, and the convex-hull simplex
+    mesh of `points` points on the unit (n-1)-sphere, RGB."""
+    rng = np.random.default_rng(seed)
+    colors = {"default": (0.7, 0.7, 0.7), (0, -1): (0.75, 0.15, 0.15), (0, 1): (0.15, 0.75, 0.15)}
+    shapes = box_walls(n, 1.0, colors, open_axis=n - 1, open_side=-1)
+    carrier, light = ceiling_light(n, 1.0, 0.5, up_axis=1, radiance=float(10 * 2 ** (n - 3)))
+    shapes.append(carrier)
+    light["shape"] = len(shapes) - 1
+    p, f = convex_hull_mesh(sphere_points(n, points, seed))
+    center = [0.0] * n
+    center[1] = -0.55
+    shapes.append({"type": "mesh", "objects": [{
+        "points": p, "facets": f, "matrix": transform_matrix(n, 0.4, center),
+        "metalness": 0.0, "roughness": float(rng.uniform(0.2, 0.6)),
+        "color": [0.8, 0.8, 0.8], "alpha": 1.0}]})
+    return {"n": n, "shapes": shapes, "lights": [light],
+            "projector": camera(n, 3.0, list(size)), "background": [0.0, 0.0, 0.0]}
+
+
+# screen edge ranges and the largest hull per dimension of the mixed batch
+MIXED_SCREENS = {3: (128, 512), 4: (32, 96), 5: (16, 32)}
+MIXED_POINTS = {3: (2000, 200000), 4: (2000, 200000), 5: (2000, 50000)}
+
+
+def mixed_batch(count: int = 64, seed: int = 4, points_scale: float = 1.0, screen_scale: float = 1.0,
+                spp=(4, 64), depth=(5, 8)) -> list[dict]:
+    """Jobs of the batched mixed-scene workload: dimension uniform in
+    {3, 4, 5}; hull of N points on the unit sphere with N log-uniform in the
+    dimension's range (MIXED_POINTS: 2k-200k, at most 50k in 5-space, where
+    hulls grow fastest); screen edge uniform in MIXED_SCREENS; samples per
+    pixel log-uniform in `spp`; maximum depth uniform in `depth`.  The scale
+    arguments shrink hulls and screens for quick runs."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for k in range(count):
+        n = int(rng.integers(3, 6))
+        lo, hi = MIXED_POINTS[n]
+        points = int(round(math.exp(rng.uniform(math.log(lo), math.log(hi))) * points_scale))
+        points = max(points, 4 * n)
+        a, b = MIXED_SCREENS[n]
+        edge = max(4, int(round(rng.uniform(a, b) * screen_scale)))
+        job_spp = int(round(math.exp(rng.uniform(math.log(spp[0]), math.log(spp[1])))))
+        job_depth = int(rng.integers(depth[0], depth[1] + 1))
+        jobs.append({"desc": mixed_scene(n, points, [edge] * (n - 1), seed * 1000 + k),
+                     "spp": job_spp, "max_depth": job_depth, "points": points})
+    return jobs
+
+
 CONFIGS = {
     "cornell3d": cornell_3d,
     "cornell4d": cornell_4d,

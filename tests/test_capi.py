@@ -57,3 +57,11 @@ def test_painter_requires_a_finalized_scene():
         assert L.nbpt_painter_create(h, 16, 5, 1) is None
     finally:
         L.nbpt_scene_destroy(h)
+
+
+def test_server_needs_a_device():
+    L = painter.lib()
+    if painter.device_count() > 0:
+        pytest.skip("a GPU is present")
+    assert L.nbpt_server_create(4, 0) is None
+    assert b"device" in L.nbpt_last_error()

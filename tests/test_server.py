@@ -1,0 +1,70 @@
+"""The job server (nbpt_server_*): renders that run together through it give
+the same images, bit for bit, as each render alone, since every path's
+random stream depends only on (seed, pass, pixel, sample)."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from math_b200 import painter as P
+from math_b200 import scenes
+
+
+@pytest.mark.gpu
+def test_server_results_match_renders_alone(painter):
+    jobs = scenes.mixed_batch(6, seed=7, points_scale=0.02, screen_scale=0.1)
+    passes = 2
+    alone = []
+    for j in jobs:
+        s = P.Scene(j["desc"], "float", False)
+        p = s.painter(j["spp"], j["max_depth"], seed=3)
+        p.run(passes)
+        alone.append(p.images())
+        p.close()
+        s.close()
+
+    server = P.Server(max_jobs=4)
+    held = []
+    ids = []
+    for j in jobs:
+        s = P.Scene(j["desc"], "float", False)
+        p = s.painter(j["spp"], j["max_depth"], seed=3)
+        held.append((s, p))
+        ids.append(server.submit(p, passes))
+    for k, (job_id, (s, p)) in enumerate(zip(ids, held)):
+        info = server.wait(job_id)
+        assert info["state"] == 2  # NBPT_JOB_DONE
+        assert info["passes_done"] == passes
+        assert 0 <= info["submitted"] <= info["started"] <= info["finished"]
+        assert info["footprint"] > 0
+        rgb, rgba = p.images()
+        assert np.array_equal(rgb, alone[k][0])
+        assert np.array_equal(rgba, alone[k][1])
+        assert p.statistics()["pass_number"] == passes
+    server.close()
+    for s, p in held:
+        p.close()
+        s.close()
+
+
+@pytest.mark.gpu
+def test_server_admits_jobs_within_its_slots(painter):
+    jobs = scenes.mixed_batch(5, seed=9, points_scale=0.01, screen_scale=0.08)
+    server = P.Server(max_jobs=2)
+    held = [(s := P.Scene(j["desc"], "float", False), s.painter(j["spp"], j["max_depth"], seed=1)) for j in jobs]
+    ids = [server.submit(p, 3) for _, p in held]
+    infos = [server.wait(i) for i in ids]
+    # never more than two jobs between admission and completion at once
+    events = sorted([(i["started"], 1) for i in infos] + [(i["finished"], -1) for i in infos],
+                    key=lambda e: (e[0], e[1]))
+    running = 0
+    for _, d in events:
+        running += d
+        assert running <= 2
+    with pytest.raises(P.PainterError):
+        server.submit(held[0][1], 0)
+    server.close()
+    for s, p in held:
+        p.close()
+        s.close()
