@@ -21,6 +21,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
@@ -48,6 +49,17 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--screen", type=int, default=None,
                    help="edge of the voxel screen (default: the workload's 64), for smaller profiling runs")
+    p.add_argument("--workload", default="cornell4d", choices=["cornell4d", "batch", "serve"],
+                   help="cornell4d: the headline benchmark; batch: the mixed-scene batch, FP32 through the "
+                        "job server against plain FP64 one job at a time; serve: Poisson arrivals of renders "
+                        "into the job server, with completion latencies")
+    p.add_argument("--jobs", type=int, default=64, help="batch: scenes in the batch")
+    p.add_argument("--points-scale", type=float, default=1.0, help="batch/serve: scale of the hull point counts")
+    p.add_argument("--screen-scale", type=float, default=1.0, help="batch/serve: scale of the screen edges")
+    p.add_argument("--rate", type=float, default=40.0, help="serve: arrivals per second")
+    p.add_argument("--duration", type=float, default=20.0, help="serve: seconds of arrivals")
+    p.add_argument("--pool", type=int, default=16, help="serve: distinct scenes the jobs draw from")
+    p.add_argument("--max-jobs", type=int, default=16, help="batch/serve: jobs the server runs at once")
     return p.parse_args()
 
 
@@ -350,11 +362,205 @@ def painter_stream(painter) -> int:
     return P.painter_stream(painter)
 
 
+def rel_rmse(a, b) -> float:
+    den = float((b.astype(np.float64) ** 2).sum())
+    return float(np.sqrt(((a.astype(np.float64) - b) ** 2).sum() / den)) if den > 0 else 0.0
+
+
+def run_batch(args):
+    """The mixed-scene batch: every job rendered once (one pass of its
+    samples per pixel) in FP64 one job at a time, then in FP32 through the
+    job server, all jobs submitted at once; wall time of each whole batch
+    with the scenes resident."""
+    from math_b200 import painter as P
+    from math_b200 import scenes
+
+    t0 = time.perf_counter()
+    jobs = scenes.mixed_batch(args.jobs, seed=4, points_scale=args.points_scale, screen_scale=args.screen_scale)
+    generate_s = time.perf_counter() - t0
+    fp64 = [P.Scene(j["desc"], "double", False) for j in jobs]
+    fp32 = [P.Scene(j["desc"], "float", False) for j in jobs]
+    paths = sum(s.pixels * s.actual_spp(j["spp"]) for s, j in zip(fp32, jobs))
+
+    def plain():
+        images = []
+        for s, j in zip(fp64, jobs):
+            p = s.painter(j["spp"], j["max_depth"], seed=1)
+            p.run(1)
+            images.append(p.images()[0])
+            p.close()
+        return images
+
+    server = P.Server(max_jobs=args.max_jobs)
+    try:
+        batch_timed(args, server, jobs, fp64, fp32, paths, generate_s, plain)
+    finally:
+        server.close()
+
+
+def batch_timed(args, server, jobs, fp64, fp32, paths, generate_s, plain):
+    from math_b200 import scenes
+
+    def batched():
+        ids = [server.submit_render(s, j["spp"], j["max_depth"], seed=1, passes=1) for s, j in zip(fp32, jobs)]
+        images = []
+        for s, i in zip(fp32, ids):
+            server.wait(i)
+            images.append(server.images(i, s.pixels)[0])
+            server.release(i)
+        return images
+
+    for _ in range(max(1, args.warmup)):
+        batched()
+    plain()
+    t0 = time.perf_counter()
+    ref = plain()
+    plain_s = time.perf_counter() - t0
+    best = None
+    for _ in range(max(1, args.steps)):
+        t0 = time.perf_counter()
+        img = batched()
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    rmse = [rel_rmse(a, b) for a, b in zip(img, ref)]
+    dims = [j["desc"]["n"] for j in jobs]
+    line = {
+        "metric": "batched_fp32_paths_per_second", "value": paths / best, "unit": "paths/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "plain_fp64": {"value": paths / plain_s, "seconds": plain_s,
+                       "note": "one job at a time: painter, one pass, image read back"},
+        "batched_fp32": {"value": paths / best, "seconds": best,
+                         "note": f"all jobs submitted to the job server ({args.max_jobs} at once), "
+                                 "created at admission, images read back; best of the timed batches"},
+        "speedup_vs_plain_fp64": plain_s / best,
+        "same_seed_rel_rmse_fp32_vs_fp64": {
+            "median": float(np.median(rmse)), "max": float(np.max(rmse)),
+            "note": "one pass each: float rounding moves paths off their double twins, so this is sample "
+                    "noise, not bias; bias is tested against converged double images in tests/"},
+        "dtype": "f32 (batched) / f64 (plain)", "data": "synthetic (seeded generators)",
+        "config": {"workload": "mixed-scene batch: box, ceiling light and sphere hull in 3/4/5-space, RGB",
+                   "jobs": len(jobs), "dims": {str(n): dims.count(n) for n in (3, 4, 5)},
+                   "paths": paths, "facets_max": max(scenes.describe(j["desc"])["facets"] for j in jobs),
+                   "points_scale": args.points_scale, "screen_scale": args.screen_scale,
+                   "generate_s": generate_s},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(args):
+    """Poisson arrivals of renders into the job server: each job draws a
+    scene from a pool of mixed-batch scenes (resident, FP32) and a sample
+    budget log-uniform in [16, 256] samples per pixel; the server creates the
+    render when it admits the job.  Latency is completion minus arrival."""
+    from math_b200 import painter as P
+    from math_b200 import scenes
+
+    def note(msg):
+        print(f"serve: {msg}", file=sys.stderr, flush=True)
+
+    pool = scenes.mixed_batch(args.pool, seed=5, points_scale=args.points_scale, screen_scale=args.screen_scale)
+    built = [P.Scene(j["desc"], "float", False) for j in pool]
+    note(f"{len(built)} pool scenes built")
+    rng = np.random.default_rng(5)
+    arrivals = []
+    t = 0.0
+    while True:
+        t += rng.exponential(1.0 / args.rate)
+        if t > args.duration:
+            break
+        k = int(rng.integers(0, len(pool)))
+        spp = int(round(math.exp(rng.uniform(math.log(16), math.log(256)))))
+        # one pass renders at most 256 samples per pixel after the stratified
+        # sampler rounds the count up to a power of the screen dimension
+        while built[k].actual_spp(spp) > 256:
+            spp -= 1
+        arrivals.append((t, k, spp))
+    server = P.Server(max_jobs=args.max_jobs)
+    try:
+        run_arrivals(args, server, pool, built, arrivals, note)
+    finally:
+        server.close()
+
+
+def wait_with_watchdog(server, job, all_jobs, note, limit: float = 60.0):
+    """Waits for a job by polling; if no job of the run progresses for
+    `limit` seconds, reports every job's state and gives up."""
+    last_change = time.perf_counter()
+    last = None
+    while True:
+        info = server.job(job)
+        if info["state"] in (2, 3):
+            return server.wait(job)
+        snapshot = [(j, server.job(j)["state"], server.job(j)["passes_done"]) for j in all_jobs]
+        if snapshot != last:
+            last = snapshot
+            last_change = time.perf_counter()
+        elif time.perf_counter() - last_change > limit:
+            note("no progress: " + ", ".join(f"{j}:{st}/{pd}" for j, st, pd in snapshot))
+            raise RuntimeError(f"job {job} made no progress for {limit} s")
+        time.sleep(0.01)
+
+
+def run_arrivals(args, server, pool, built, arrivals, note):
+    """Submits the arrivals on their schedule, waits for every job and
+    prints the serve line."""
+    # warm-up: one render of every pool scene
+    for s, j in zip(built, pool):
+        i = server.submit_render(s, 4, j["max_depth"], seed=1)
+        server.wait(i)
+        server.release(i)
+    note("warm-up done")
+    t_start = server.time()
+    submitted = []
+    for a, k, spp in arrivals:
+        while server.time() - t_start < a:
+            time.sleep(min(0.001, max(0.0, a - (server.time() - t_start))))
+        s = built[k]
+        i = server.submit_render(s, spp, pool[k]["max_depth"], seed=len(submitted) + 1)
+        submitted.append((i, t_start + a, s.pixels * s.actual_spp(spp)))
+    note(f"{len(submitted)} jobs submitted")
+    latencies, waits = [], []
+    last = t_start
+    pending = [j for j, _, _ in submitted]
+    for i, arrival, _ in submitted:
+        info = wait_with_watchdog(server, i, pending, note)
+        pending.remove(i)
+        latencies.append(info["finished"] - arrival)
+        waits.append(info["started"] - arrival)
+        last = max(last, info["finished"])
+        server.release(i)
+    paths = sum(p for _, _, p in submitted)
+    lat = np.array(latencies)
+    line = {
+        "metric": "served_job_latency_p99", "value": float(np.percentile(lat, 99)), "unit": "s",
+        "higher_is_better": False, "n_gpus": 1,
+        "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+        "mean_queue_wait_s": float(np.mean(waits)),
+        "jobs": len(submitted), "throughput_paths_per_second": paths / (last - t_start),
+        "offered_paths_per_second": paths / args.duration,
+        "makespan_s": last - t_start,
+        "dtype": "f32", "data": "synthetic (seeded generators)",
+        "config": {"workload": "Poisson render arrivals into the job server", "rate_per_s": args.rate,
+                   "duration_s": args.duration, "pool_scenes": len(pool), "spp": "log-uniform 16-256",
+                   "max_jobs": args.max_jobs, "points_scale": args.points_scale,
+                   "screen_scale": args.screen_scale},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.workload == "batch":
+        if rank == 0:
+            run_batch(args)
+        return
+    if args.workload == "serve":
+        if rank == 0:
+            run_serve(args)
         return
     run_nbpt(args, rank, world, local)
 

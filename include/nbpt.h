@@ -211,6 +211,17 @@ void nbpt_server_destroy(nbpt_server* server);
 /* queues `passes` passes of a painter; returns the job id.  The painter and
  * its scene must stay alive and unused by the caller until the job is done. */
 long long nbpt_server_submit(nbpt_server* server, nbpt_painter* painter, int passes);
+/* queues a render (nbpt_painter_create's arguments and `passes` passes) that
+ * the server creates when it admits the job, so a queued job holds no device
+ * memory; the scene must stay alive until the job is released */
+long long nbpt_server_submit_render(
+        nbpt_server* server, nbpt_scene* scene, int samples_per_pixel, int max_depth, unsigned seed, int passes);
+/* images and statistics of a done job (nbpt_painter_images / _statistics) */
+int nbpt_server_images(nbpt_server* server, long long job, float* rgb, float* rgba);
+int nbpt_server_statistics(nbpt_server* server, long long job, nbpt_statistics* statistics);
+/* forgets a done or failed job and frees the render the server created for
+ * it; until then a done render keeps its device memory */
+int nbpt_server_release(nbpt_server* server, long long job);
 int nbpt_server_job(nbpt_server* server, long long job, nbpt_job_info* info);
 /* blocks until the job is done or failed; NBPT_ERROR (with the message) if it failed */
 int nbpt_server_wait(nbpt_server* server, long long job, nbpt_job_info* info);

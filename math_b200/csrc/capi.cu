@@ -120,6 +120,20 @@ void copy_info(const nbpt::JobInfo& j, nbpt_job_info* info)
         info->finished = j.finished;
 }
 
+void copy_statistics(const nbpt::Statistics& s, nbpt_statistics* statistics)
+{
+        statistics->pass_number = s.pass_number;
+        statistics->pixel_count = s.pixel_count;
+        statistics->ray_count = s.ray_count;
+        statistics->sample_count = s.sample_count;
+        statistics->previous_pass_duration = s.previous_pass_duration;
+        statistics->paths_seconds = s.paths_seconds;
+        statistics->nodes = s.nodes;
+        statistics->facets = s.facets;
+        statistics->shapes = s.shapes;
+        statistics->kernel_launches = s.kernel_launches;
+}
+
 void require_device()
 {
         int count = 0;
@@ -617,17 +631,7 @@ int nbpt_painter_statistics(nbpt_painter* painter, nbpt_statistics* statistics)
                 [&]
                 {
                         require(statistics, "statistics");
-                        const nbpt::Statistics s = painter_of(painter).statistics();
-                        statistics->pass_number = s.pass_number;
-                        statistics->pixel_count = s.pixel_count;
-                        statistics->ray_count = s.ray_count;
-                        statistics->sample_count = s.sample_count;
-                        statistics->previous_pass_duration = s.previous_pass_duration;
-                        statistics->paths_seconds = s.paths_seconds;
-                        statistics->nodes = s.nodes;
-                        statistics->facets = s.facets;
-                        statistics->shapes = s.shapes;
-                        statistics->kernel_launches = s.kernel_launches;
+                        copy_statistics(painter_of(painter).statistics(), statistics);
                         return 0;
                 });
 }
@@ -675,6 +679,51 @@ long long nbpt_server_submit(nbpt_server* server, nbpt_painter* painter, const i
                         return 0;
                 });
         return id;
+}
+
+long long nbpt_server_submit_render(nbpt_server* server, nbpt_scene* scene, const int samples_per_pixel,
+                                    const int max_depth, const unsigned seed, const int passes)
+{
+        long long id = NBPT_ERROR;
+        guarded(
+                [&]
+                {
+                        id = server_of(server).submit_render(&scene_of(scene), samples_per_pixel, max_depth, seed,
+                                                             passes);
+                        return 0;
+                });
+        return id;
+}
+
+int nbpt_server_images(nbpt_server* server, const long long job, float* rgb, float* rgba)
+{
+        return guarded(
+                [&]
+                {
+                        server_of(server).images(job, rgb, rgba);
+                        return 0;
+                });
+}
+
+int nbpt_server_statistics(nbpt_server* server, const long long job, nbpt_statistics* statistics)
+{
+        return guarded(
+                [&]
+                {
+                        require(statistics, "statistics");
+                        copy_statistics(server_of(server).statistics(job), statistics);
+                        return 0;
+                });
+}
+
+int nbpt_server_release(nbpt_server* server, const long long job)
+{
+        return guarded(
+                [&]
+                {
+                        server_of(server).release(job);
+                        return 0;
+                });
 }
 
 int nbpt_server_job(nbpt_server* server, const long long job, nbpt_job_info* info)

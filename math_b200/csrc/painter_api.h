@@ -71,6 +71,8 @@ public:
         virtual long long upload_bytes() const = 0;
 
         virtual std::unique_ptr<Painter> create_painter(int samples_per_pixel, int max_depth, std::uint32_t seed) = 0;
+        // device bytes create_painter would allocate
+        virtual long long painter_bytes(int samples_per_pixel, int max_depth) const = 0;
 
         // verification: closest hit (any == 0) or any hit of rays [n][2N]
         virtual void trace(const double* rays, long long count, int any, int* kind, int* index, double* t,

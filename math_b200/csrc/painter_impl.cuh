@@ -98,6 +98,27 @@ public:
                 }
         }
 
+        // copies on `stream` and waits for them (no legacy default stream, so
+        // painters driven from different host threads do not order each other)
+        void upload_on(const std::vector<X>& v, const cudaStream_t stream)
+        {
+                allocate(v.size());
+                if (!v.empty())
+                {
+                        NBPT_CUDA(cudaMemcpyAsync(ptr_, v.data(), v.size() * sizeof(X), cudaMemcpyHostToDevice, stream));
+                        NBPT_CUDA(cudaStreamSynchronize(stream));
+                }
+        }
+
+        void download_on(X* out, const std::size_t n, const cudaStream_t stream) const
+        {
+                if (n > 0)
+                {
+                        NBPT_CUDA(cudaMemcpyAsync(out, ptr_, n * sizeof(X), cudaMemcpyDeviceToHost, stream));
+                        NBPT_CUDA(cudaStreamSynchronize(stream));
+                }
+        }
+
         void download(X* out, const std::size_t n) const
         {
                 if (n > 0)
@@ -1304,6 +1325,7 @@ public:
         }
 
         std::unique_ptr<Painter> create_painter(int spp, int max_depth, std::uint32_t seed) override;
+        long long painter_bytes(int spp, int max_depth) const override;
 
         void trace(const double* rays, long long count, int any, int* kind, int* index, double* t, double* point) override;
         void trace_device(const double* rays, long long count, int any, int* kind, int* index, double* t,
@@ -1505,7 +1527,33 @@ class PainterT final : public Painter
         // device memory for the per-path buffers of one chunk
         static constexpr long long CHUNK_BUDGET = 4LL << 30;
 
+        // device bytes of one path's buffers in a chunk (vertices, tape,
+        // random stream state, strategy tasks)
+        static long long chunk_path_bytes(const int max_depth)
+        {
+                return static_cast<long long>(tape_words(max_depth)) * 4 +
+                       2LL * (max_depth + 1) * sizeof(PathVertex<N, T, 1>) + sizeof(Pcg) +
+                       4LL * tape_slot_count(max_depth);
+        }
+
+        static long long chunk_pixels(const long long pixels, const int spp, const int max_depth)
+        {
+                const long long per_pixel = chunk_path_bytes(max_depth) * spp;
+                long long c = std::max(1LL, std::min(pixels, CHUNK_BUDGET / per_pixel));
+                return std::min(c, (TASK_MAX_PATHS - 1) / spp);
+        }
+
 public:
+        // device bytes a painter of these parameters allocates
+        static long long estimate_bytes(const long long pixels, const int spp, const int max_depth, const int strata)
+        {
+                const long long samples = pixels * spp;
+                const long long per_sample = (N - 1) * sizeof(T) + C * 4 + 4 + 1;
+                const long long per_pixel = sizeof(PixelState<C>) + 12 + 16;
+                return (strata + 1) * sizeof(T) + samples * per_sample + pixels * per_pixel + sizeof(PathStats) +
+                       chunk_pixels(pixels, spp, max_depth) * spp * chunk_path_bytes(max_depth);
+        }
+
         PainterT(const SceneT<N, T, C>* scene, const int spp, const int max_depth, const std::uint32_t seed)
                 : scene_(scene),
                   spp_request_(spp),
@@ -1531,6 +1579,8 @@ public:
                 }
                 pixels_ = scene_->pixel_count();
 
+                NBPT_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+
                 // offsets of the strata (sj_sampler.h:75-114)
                 std::vector<T> offsets(strata_ + 1);
                 const T offset_size = (T(1) - T(0)) / static_cast<T>(strata_);
@@ -1540,7 +1590,7 @@ public:
                         offsets[i] = T(0) + static_cast<T>(i) * offset_size;
                 }
                 offsets[strata_] = 1;
-                offsets_.upload(offsets);
+                offsets_.upload_on(offsets, stream_);
 
                 const long long samples = pixels_ * spp_;
                 points_.allocate(samples * (N - 1));
@@ -1553,12 +1603,7 @@ public:
                 rgba_.allocate(pixels_ * 4);
                 {
                         tape_words_ = tape_words(max_depth_);
-                        const long long per_path = static_cast<long long>(tape_words_) * 4 +
-                                                   2LL * (max_depth_ + 1) * sizeof(PathVertex<N, T, 1>) +
-                                                   sizeof(Pcg) + 4LL * tape_slot_count(max_depth_);
-                        const long long per_pixel = per_path * spp_;
-                        chunk_pixels_ = std::max(1LL, std::min(pixels_, CHUNK_BUDGET / per_pixel));
-                        chunk_pixels_ = std::min(chunk_pixels_, (TASK_MAX_PATHS - 1) / spp_);
+                        chunk_pixels_ = chunk_pixels(pixels_, spp_, max_depth_);
                         const long long paths = chunk_pixels_ * spp_;
                         tape_.allocate(paths * tape_words_);
                         vertices_.allocate(paths * 2 * (max_depth_ + 1));
@@ -1572,7 +1617,6 @@ public:
                         connect_blocks_ = sms * NBPT_PATHS_MIN_BLOCKS;
                 }
 
-                NBPT_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
                 NBPT_CUDA(cudaEventCreate(&ev_start_));
                 NBPT_CUDA(cudaEventCreate(&ev_paths_));
                 NBPT_CUDA(cudaEventCreate(&ev_paths_end_));
@@ -1689,7 +1733,7 @@ public:
         {
                 NBPT_CUDA(cudaStreamSynchronize(stream_));
                 PathStats s{};
-                stats_.download(&s, 1);
+                stats_.download_on(&s, 1, stream_);
                 float ms = 0;
                 float paths_ms = 0;
                 NBPT_CUDA(cudaEventElapsedTime(&ms, ev_start_, ev_end_));
@@ -1713,11 +1757,11 @@ public:
                 NBPT_CUDA(cudaStreamSynchronize(stream_));
                 if (rgb)
                 {
-                        rgb_.download(rgb, pixels_ * 3);
+                        rgb_.download_on(rgb, pixels_ * 3, stream_);
                 }
                 if (rgba)
                 {
-                        rgba_.download(rgba, pixels_ * 4);
+                        rgba_.download_on(rgba, pixels_ * 4, stream_);
                 }
         }
 
@@ -1728,7 +1772,7 @@ public:
                 if (points)
                 {
                         std::vector<T> p(samples * (N - 1));
-                        points_.download(p.data(), p.size());
+                        points_.download_on(p.data(), p.size(), stream_);
                         for (std::size_t i = 0; i < p.size(); ++i)
                         {
                                 points[i] = static_cast<double>(p[i]);
@@ -1736,11 +1780,11 @@ public:
                 }
                 if (colors)
                 {
-                        colors_.download(colors, samples * C);
+                        colors_.download_on(colors, samples * C, stream_);
                 }
                 if (valid)
                 {
-                        valid_.download(valid, samples);
+                        valid_.download_on(valid, samples, stream_);
                 }
         }
 
@@ -1754,6 +1798,16 @@ template <int N, typename T, int C>
 std::unique_ptr<Painter> SceneT<N, T, C>::create_painter(const int spp, const int max_depth, const std::uint32_t seed)
 {
         return std::make_unique<PainterT<N, T, C>>(this, spp, max_depth, seed);
+}
+
+template <int N, typename T, int C>
+long long SceneT<N, T, C>::painter_bytes(const int spp, const int max_depth) const
+{
+        if (spp < 1 || max_depth < 1)
+        {
+                throw std::runtime_error("painter samples per pixel and maximum depth must be positive");
+        }
+        return PainterT<N, T, C>::estimate_bytes(pixel_count(), actual_spp(spp), max_depth, strata(spp));
 }
 
 template <int N, typename T, int C>

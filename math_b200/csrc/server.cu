@@ -4,6 +4,9 @@
 #include <cuda_runtime.h>
 
 #include <chrono>
+#include <cstdlib>
+#include <set>
+#include <vector>
 #include <stdexcept>
 
 namespace nbpt
@@ -14,12 +17,39 @@ double steady_seconds()
 {
         return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
+
+// Servers alive in the process: stopped at exit, before the CUDA runtime
+// tears down, so that no worker thread is left issuing CUDA calls.
+std::mutex g_live_mutex;
+std::set<Server*>* g_live = nullptr;
+
+void stop_live_servers()
+{
+        std::vector<Server*> live;
+        {
+                const std::lock_guard lock(g_live_mutex);
+                if (g_live)
+                {
+                        live.assign(g_live->begin(), g_live->end());
+                }
+        }
+        for (Server* s : live)
+        {
+                s->shutdown();
+        }
+}
 } // namespace
 
 struct Server::Job final
 {
         long long id;
-        Painter* painter;
+        Painter* painter = nullptr;
+        // a render the server creates at admission
+        Scene* scene = nullptr;
+        int spp = 0;
+        int max_depth = 0;
+        std::uint32_t seed = 0;
+        std::unique_ptr<Painter> owned;
         int device;
         JobInfo info;
         cudaEvent_t done = nullptr; // marks the end of the pass in flight
@@ -35,6 +65,12 @@ Server::Server(const int max_jobs, const long long memory_budget)
         {
                 throw std::runtime_error("server needs at least one job slot");
         }
+        int device = 0;
+        if (cudaGetDevice(&device) != cudaSuccess)
+        {
+                cudaGetLastError();
+                throw std::runtime_error("no CUDA device for the server");
+        }
         if (memory_budget <= 0)
         {
                 std::size_t free = 0;
@@ -46,17 +82,41 @@ Server::Server(const int max_jobs, const long long memory_budget)
                 }
                 budget_ = static_cast<long long>(free * 0.8);
         }
+        {
+                // registered after the CUDA runtime initialised above, so it
+                // runs before the runtime's own exit handlers
+                const std::lock_guard lock(g_live_mutex);
+                if (!g_live)
+                {
+                        g_live = new std::set<Server*>;
+                        std::atexit(stop_live_servers);
+                }
+                g_live->insert(this);
+        }
         worker_ = std::thread(&Server::run, this);
 }
 
-Server::~Server()
+void Server::shutdown()
 {
         {
                 const std::lock_guard lock(mutex_);
                 stop_ = true;
         }
         changed_.notify_all();
-        worker_.join();
+        if (worker_.joinable() && worker_.get_id() != std::this_thread::get_id())
+        {
+                worker_.join();
+        }
+}
+
+Server::~Server()
+{
+        shutdown();
+        const std::lock_guard lock(g_live_mutex);
+        if (g_live)
+        {
+                g_live->erase(this);
+        }
 }
 
 double Server::now() const
@@ -104,26 +164,118 @@ long long Server::submit(Painter* const painter, const int passes)
         return id;
 }
 
-JobInfo Server::info(const long long job) const
+long long Server::submit_render(Scene* const scene, const int spp, const int max_depth, const std::uint32_t seed,
+                               const int passes)
 {
-        const std::lock_guard lock(mutex_);
+        if (!scene)
+        {
+                throw std::runtime_error("null scene");
+        }
+        if (passes < 1)
+        {
+                throw std::runtime_error("a job needs at least one pass");
+        }
+        auto job = std::make_shared<Job>();
+        job->scene = scene;
+        job->spp = spp;
+        job->max_depth = max_depth;
+        job->seed = seed;
+        if (cudaGetDevice(&job->device) != cudaSuccess)
+        {
+                cudaGetLastError();
+                throw std::runtime_error("no CUDA device for the job");
+        }
+        job->info.state = JobState::QUEUED;
+        job->info.passes = passes;
+        job->info.passes_done = 0;
+        job->info.footprint = scene->painter_bytes(spp, max_depth) + scene->device_bytes();
+        job->info.submitted = now();
+        job->info.started = -1;
+        job->info.finished = -1;
+        long long id = 0;
+        {
+                const std::lock_guard lock(mutex_);
+                if (stop_)
+                {
+                        throw std::runtime_error("the server is stopping");
+                }
+                id = next_id_++;
+                job->id = id;
+                jobs_[id] = job;
+                queue_.push_back(job);
+        }
+        changed_.notify_all();
+        return id;
+}
+
+std::shared_ptr<Server::Job> Server::find_locked(const long long job) const
+{
         const auto i = jobs_.find(job);
         if (i == jobs_.end())
         {
                 throw std::runtime_error("unknown job " + std::to_string(job));
         }
-        return i->second->info;
+        return i->second;
+}
+
+JobInfo Server::info(const long long job) const
+{
+        const std::lock_guard lock(mutex_);
+        return find_locked(job)->info;
+}
+
+void Server::images(const long long job, float* const rgb, float* const rgba)
+{
+        std::shared_ptr<Job> j;
+        {
+                const std::lock_guard lock(mutex_);
+                j = find_locked(job);
+                if (j->info.state != JobState::DONE)
+                {
+                        throw std::runtime_error("job " + std::to_string(job) + " is not done");
+                }
+        }
+        cudaSetDevice(j->device);
+        j->painter->images(rgb, rgba);
+}
+
+Statistics Server::statistics(const long long job)
+{
+        std::shared_ptr<Job> j;
+        {
+                const std::lock_guard lock(mutex_);
+                j = find_locked(job);
+                if (j->info.state != JobState::DONE)
+                {
+                        throw std::runtime_error("job " + std::to_string(job) + " is not done");
+                }
+        }
+        return j->painter->statistics();
+}
+
+void Server::release(const long long job)
+{
+        std::shared_ptr<Job> j;
+        {
+                const std::lock_guard lock(mutex_);
+                j = find_locked(job);
+                if (j->info.state != JobState::DONE && j->info.state != JobState::FAILED)
+                {
+                        throw std::runtime_error("job " + std::to_string(job) + " is not finished");
+                }
+                jobs_.erase(job);
+        }
+        if (j->owned)
+        {
+                cudaSetDevice(j->device);
+                j->owned.reset();
+        }
 }
 
 JobInfo Server::wait(const long long job)
 {
         std::unique_lock lock(mutex_);
-        const auto i = jobs_.find(job);
-        if (i == jobs_.end())
-        {
-                throw std::runtime_error("unknown job " + std::to_string(job));
-        }
-        const std::shared_ptr<Job> j = i->second;
+        const std::shared_ptr<Job> j = find_locked(job);
         changed_.wait(lock,
                       [&]
                       {
@@ -209,6 +361,12 @@ void Server::run()
                         try
                         {
                                 cudaSetDevice(j->device);
+                                if (!j->painter)
+                                {
+                                        // a render created at admission
+                                        j->owned = j->scene->create_painter(j->spp, j->max_depth, j->seed);
+                                        j->painter = j->owned.get();
+                                }
                                 if (j->pass_in_flight)
                                 {
                                         const cudaError_t e = cudaEventQuery(j->done);

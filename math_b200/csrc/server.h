@@ -13,6 +13,7 @@
 #include "painter_api.h"
 
 #include <condition_variable>
+#include <cstdint>
 #include <deque>
 #include <map>
 #include <memory>
@@ -55,12 +56,26 @@ public:
         // The painter (and its scene) must stay alive and untouched by the
         // caller until the job is done or failed.
         long long submit(Painter* painter, int passes);
+        // A render the server creates when it admits the job (so a queued job
+        // holds no device memory) and owns until release(); the scene must
+        // stay alive until then.
+        long long submit_render(Scene* scene, int spp, int max_depth, std::uint32_t seed, int passes);
+        // the images and statistics of a done job
+        void images(long long job, float* rgb, float* rgba);
+        Statistics statistics(long long job);
+        // forgets a finished job and frees the painter the server created
+        void release(long long job);
         JobInfo info(long long job) const;
         JobInfo wait(long long job);
         double now() const;
+        // finishes the running jobs, fails the queued ones and stops the
+        // worker; the destructor calls it, and so does process exit for a
+        // server never destroyed (before the CUDA runtime shuts down)
+        void shutdown();
 
 private:
         struct Job;
+        std::shared_ptr<Job> find_locked(long long job) const;
 
         void run();
         bool admit_locked();

@@ -97,6 +97,10 @@ SIGNATURES = [
     ("nbpt_server_create", _P, [ctypes.c_int, ctypes.c_longlong]),
     ("nbpt_server_destroy", None, [_P]),
     ("nbpt_server_submit", ctypes.c_longlong, [_P, _P, ctypes.c_int]),
+    ("nbpt_server_submit_render", ctypes.c_longlong, [_P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.c_int]),
+    ("nbpt_server_images", ctypes.c_int, [_P, ctypes.c_longlong, _F, _F]),
+    ("nbpt_server_statistics", ctypes.c_int, [_P, ctypes.c_longlong, ctypes.POINTER(Statistics)]),
+    ("nbpt_server_release", ctypes.c_int, [_P, ctypes.c_longlong]),
     ("nbpt_server_job", ctypes.c_int, [_P, ctypes.c_longlong, ctypes.POINTER(JobInfo)]),
     ("nbpt_server_wait", ctypes.c_int, [_P, ctypes.c_longlong, ctypes.POINTER(JobInfo)]),
     ("nbpt_server_time", ctypes.c_double, [_P]),
@@ -414,6 +418,24 @@ class Server:
 
     def submit(self, painter: "Painter", passes: int = 1) -> int:
         return _check(lib().nbpt_server_submit(self.h, painter.h, passes))
+
+    def submit_render(self, scene: "Scene", samples_per_pixel: int, max_depth: int, seed: int = 1,
+                      passes: int = 1) -> int:
+        return _check(lib().nbpt_server_submit_render(self.h, scene.h, samples_per_pixel, max_depth, seed, passes))
+
+    def images(self, job: int, pixels: int):
+        rgb = np.zeros((pixels, 3), np.float32)
+        rgba = np.zeros((pixels, 4), np.float32)
+        _check(lib().nbpt_server_images(self.h, job, _p(rgb, _F), _p(rgba, _F)))
+        return rgb, rgba
+
+    def statistics(self, job: int) -> dict:
+        st = Statistics()
+        _check(lib().nbpt_server_statistics(self.h, job, ctypes.byref(st)))
+        return st.as_dict()
+
+    def release(self, job: int):
+        _check(lib().nbpt_server_release(self.h, job))
 
     def job(self, job: int) -> dict:
         info = JobInfo()

@@ -68,3 +68,29 @@ def test_server_admits_jobs_within_its_slots(painter):
     for s, p in held:
         p.close()
         s.close()
+
+
+@pytest.mark.gpu
+def test_server_created_renders_match_renders_alone(painter):
+    jobs = scenes.mixed_batch(4, seed=11, points_scale=0.02, screen_scale=0.1)
+    built = [P.Scene(j["desc"], "float", False) for j in jobs]
+    alone = []
+    for s, j in zip(built, jobs):
+        p = s.painter(j["spp"], j["max_depth"], seed=5)
+        p.run(1)
+        alone.append(p.images()[0])
+        p.close()
+    server = P.Server(max_jobs=3)
+    ids = [server.submit_render(s, j["spp"], j["max_depth"], seed=5, passes=1) for s, j in zip(built, jobs)]
+    for k, job_id in enumerate(ids):
+        info = server.wait(job_id)
+        assert info["state"] == 2
+        rgb, _ = server.images(job_id, built[k].pixels)
+        assert np.array_equal(rgb, alone[k])
+        assert server.statistics(job_id)["sample_count"] == built[k].pixels * built[k].actual_spp(jobs[k]["spp"])
+        server.release(job_id)
+    with pytest.raises(P.PainterError):
+        server.job(ids[0])  # released
+    server.close()
+    for s in built:
+        s.close()
