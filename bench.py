@@ -34,8 +34,21 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-WORKLOAD = {"scene": "cornell4d", "screen": [64, 64, 64], "spp": 16, "max_depth": 6,
-            "points": 20000, "color": "spectrum64"}
+# The single-scene workloads (the headline one first): scene, screen,
+# samples per pixel, maximum depth, colour and the default precision.
+WORKLOADS = {
+    "cornell4d": {"screen": [64, 64, 64], "spp": 16, "max_depth": 6, "spectrum": True, "precision": "float",
+                  "label": "4-space Cornell box, hull of 20000 points on S^3, spectrum64"},
+    "cornell3d": {"screen": [256, 256], "spp": 16, "max_depth": 5, "spectrum": False, "precision": "double",
+                  "label": "3-space Cornell box, icosphere of 20480 triangles, RGB"},
+    "sphere4d": {"screen": [96, 96, 96], "spp": 8, "max_depth": 8, "spectrum": False, "precision": "float",
+                 "label": "4-space hull of 150000 noisy points on S^3 (about 1M facets), ball light, "
+                          "parallel projection, RGB"},
+}
+
+
+def workload_of(args) -> dict:
+    return WORKLOADS[args.workload if args.workload in WORKLOADS else "cornell4d"]
 
 
 def parse():
@@ -44,13 +57,15 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="nbpt", choices=["nbpt", "reference"])
-    p.add_argument("--precision", default="float", choices=["float", "double"])
+    p.add_argument("--precision", default=None, choices=["float", "double"],
+                   help="default: the workload's (float; double for cornell3d)")
     p.add_argument("--small", action="store_true", help="a small configuration for smoke runs")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--screen", type=int, default=None,
                    help="edge of the voxel screen (default: the workload's 64), for smaller profiling runs")
-    p.add_argument("--workload", default="cornell4d", choices=["cornell4d", "batch", "serve"],
-                   help="cornell4d: the headline benchmark; batch: the mixed-scene batch, FP32 through the "
+    p.add_argument("--workload", default="cornell4d", choices=["cornell4d", "cornell3d", "sphere4d", "batch", "serve"],
+                   help="cornell4d: the headline benchmark; cornell3d, sphere4d: the other single-scene "
+                        "workloads; batch: the mixed-scene batch, FP32 through the "
                         "job server against plain FP64 one job at a time; serve: Poisson arrivals of renders "
                         "into the job server, with completion latencies")
     p.add_argument("--jobs", type=int, default=64, help="batch: scenes in the batch")
@@ -60,7 +75,10 @@ def parse():
     p.add_argument("--duration", type=float, default=20.0, help="serve: seconds of arrivals")
     p.add_argument("--pool", type=int, default=16, help="serve: distinct scenes the jobs draw from")
     p.add_argument("--max-jobs", type=int, default=16, help="batch/serve: jobs the server runs at once")
-    return p.parse_args()
+    args = p.parse_args()
+    if args.precision is None:
+        args.precision = workload_of(args)["precision"]
+    return args
 
 
 def dist_env():
@@ -70,13 +88,20 @@ def dist_env():
     return rank, world, local
 
 
-def scene_desc(small: bool, screen: int | None = None):
+def scene_desc(small: bool, screen: int | None = None, name: str = "cornell4d"):
     from math_b200 import scenes
 
+    w = WORKLOADS[name]
+    dims = len(w["screen"])
     if small:
-        return scenes.cornell_4d(size=(16, 16, 16), points=2000)
-    size = tuple(WORKLOAD["screen"]) if screen is None else (screen, screen, screen)
-    return scenes.cornell_4d(size=size, points=WORKLOAD["points"])
+        size = tuple(max(4, e // 4) for e in w["screen"])
+    else:
+        size = tuple(w["screen"]) if screen is None else (screen,) * dims
+    if name == "cornell4d":
+        return scenes.cornell_4d(size=size, points=2000 if small else 20000)
+    if name == "cornell3d":
+        return scenes.cornell_3d(size=size, subdivisions=3 if small else 5)
+    return scenes.sphere_4d(size=size, points=15000 if small else 150000)
 
 
 class ClockSampler:
@@ -134,7 +159,7 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(small: bool, seconds_hint: float = 20.0) -> dict:
+def cpu_baseline(small: bool, name: str = "cornell4d", precision: str = "float") -> dict:
     """The reference's own painter (create_painter, BPT, float, spectrum),
     unmodified, on the host cores: one pass over a bounded slab of the
     workload's screen."""
@@ -145,11 +170,12 @@ def cpu_baseline(small: bool, seconds_hint: float = 20.0) -> dict:
         return {"value": None, "unit": "paths/s", "cores": 0, "kind": "reference",
                 "sample": "oracle library not built"}
     # the whole workload: one pass over the full screen
-    desc = scene_desc(small)
+    w = WORKLOADS[name]
+    desc = scene_desc(small, None, name)
     slab = desc["projector"]["size"]
-    s = oracle.Scene(desc, "float", True)
+    s = oracle.Scene(desc, precision, w["spectrum"])
     cores = os.cpu_count() or 1
-    stats, _ = s.paint(WORKLOAD["spp"], WORKLOAD["max_depth"], passes=1, threads=cores)
+    stats, _ = s.paint(w["spp"], w["max_depth"], passes=1, threads=cores)
     value = stats["sample_count"] / stats["pass_duration"]
     return {"value": value, "unit": "paths/s", "cores": cores, "kind": "reference",
             "sample": (f"one pass of the reference painter over the whole {'x'.join(map(str, slab))} screen "
@@ -180,16 +206,17 @@ def run_reference(args, rank: int):
         return
     # --steps timed passes of the bounded slab (warm-up passes untimed)
 
-    desc = scene_desc(args.small, args.screen)
+    w = workload_of(args)
+    desc = scene_desc(args.small, args.screen, args.workload if args.workload in WORKLOADS else "cornell4d")
     slab = desc["projector"]["size"]
-    s = oracle.Scene(desc, "float", True)
+    s = oracle.Scene(desc, args.precision, w["spectrum"])
     cores = os.cpu_count() or 1
     for _ in range(args.warmup):
-        s.paint(WORKLOAD["spp"], WORKLOAD["max_depth"], passes=1, threads=cores)
+        s.paint(w["spp"], w["max_depth"], passes=1, threads=cores)
     samples = 0
     seconds = 0.0
     for _ in range(args.steps):
-        st, _ = s.paint(WORKLOAD["spp"], WORKLOAD["max_depth"], passes=1, threads=cores)
+        st, _ = s.paint(w["spp"], w["max_depth"], passes=1, threads=cores)
         samples += st["sample_count"]
         seconds += st["pass_duration"]
     value = samples / seconds
@@ -198,9 +225,10 @@ def run_reference(args, rank: int):
         "metric": "bpt_paths_per_second", "value": value, "unit": "paths/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000 * seconds / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
-        "config": {"workload": "cornell4d 4-space Cornell box, hull of 20000 points on S^3, spectrum64, "
-                               "16 spp (27 rendered), depth 6", "screen": slab, "precision": "float"},
+        "vs_baseline": None, "dtype": "f64" if args.precision == "double" else "f32",
+        "data": "synthetic (seeded generators)",
+        "config": {"workload": f"{args.workload} {w['label']}, {w['spp']} spp, depth {w['max_depth']}",
+                   "screen": slab, "precision": args.precision},
         "cpu_baseline": {"value": value, "unit": "paths/s", "cores": cores, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": value, "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -217,14 +245,15 @@ def run_nbpt(args, rank: int, world: int, local: int):
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     from math_b200 import painter as P
 
-    desc = scene_desc(args.small, args.screen)
-    spectrum = True
+    w = workload_of(args)
+    desc = scene_desc(args.small, args.screen, args.workload)
+    spectrum = w["spectrum"]
     t0 = time.perf_counter()
     scene = P.Scene(desc, args.precision, spectrum)
     build_s = time.perf_counter() - t0
     # every rank renders its own pass sequence of the whole screen
     # (independent samples: weak scaling, no data-path collective)
-    painter = scene.painter(WORKLOAD["spp"], WORKLOAD["max_depth"], seed=1 + rank)
+    painter = scene.painter(w["spp"], w["max_depth"], seed=1 + rank)
     stream = torch.cuda.ExternalStream(painter_stream(painter))
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
 
@@ -280,7 +309,7 @@ def run_nbpt(args, rank: int, world: int, local: int):
     for _ in range(args.steps):
         e0 = time.perf_counter()
         job_scene = P.Scene(desc, args.precision, spectrum)
-        job = job_scene.painter(WORKLOAD["spp"], WORKLOAD["max_depth"], seed=1 + rank)
+        job = job_scene.painter(w["spp"], w["max_depth"], seed=1 + rank)
         job.run(1)
         P._check(P.lib().nbpt_painter_images(job.h, P._p(rgb, P._F), P._p(rgba, P._F)))
         e2e_times.append(time.perf_counter() - e0)
@@ -314,7 +343,8 @@ def run_nbpt(args, rank: int, world: int, local: int):
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None,
                 "traffic": (TRAFFIC_PER_PATH[args.precision] * paths_per_step
-                            if args.precision in TRAFFIC_PER_PATH and not args.small else None),
+                            if args.precision in TRAFFIC_PER_PATH and args.workload == "cornell4d"
+                            and not args.small and args.screen is None else None),
                 "traffic_source": "profiles/path_kernels_cornell4d_32.md (per path, scaled to one pass)",
                 "kernel": "path kernels (walk, connect, light, replay)",
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
@@ -325,16 +355,17 @@ def run_nbpt(args, rank: int, world: int, local: int):
                 "paths_kernel_share": paths_s / (ms / 1000) if ms > 0 else None}
 
     if rank == 0:
-        cpu = None if (args.no_cpu_baseline or world > 1) else cpu_baseline(args.small)
+        cpu = (None if (args.no_cpu_baseline or world > 1)
+               else cpu_baseline(args.small, args.workload, args.precision))
         line = {
             "metric": "bpt_paths_per_second", "value": value, "unit": "paths/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if args.precision == "float" else "f64",
             "data": "synthetic (seeded generators)",
-            "config": {"workload": "cornell4d 4-space Cornell box, hull of 20000 points on S^3 "
-                                   f"({scene.pixels} voxels), spectrum64, 16 spp ({painter.spp} rendered), "
-                                   "depth 6", "screen": desc["projector"]["size"],
+            "config": {"workload": f"{args.workload} {w['label']} ({scene.pixels} pixels), {w['spp']} spp "
+                                   f"({painter.spp} rendered), depth {w['max_depth']}",
+                       "screen": desc["projector"]["size"],
                        "paths_per_step": paths_per_step, "precision": args.precision,
                        "l2": "flushed (256 MiB write) between timed steps",
                        "scene_build_s": build_s},
