@@ -637,6 +637,66 @@ struct Bpt final
         // -----------------------------------------------------------------
         // connections (connect.cpp:48-375)
 
+        // The s = 1 strategy in two parts (connect.cpp:135-185): the light
+        // sample, the only part that draws from the path's random stream, and
+        // the connection to it.  false: the sample is unusable.
+        __device__ bool light_arrival(const int t_count, int& li, ArriveSample<N, T, C>& as) const
+        {
+                const PathVertex<N, T, C>& cv = camera[t_count - 1];
+                li = sample_light();
+                as = arrive_sample(s.lights[li], cv.pos);
+                return as.usable();
+        }
+
+        NBPT_CALL bool connect_light(const int t_count, const int li, const ArriveSample<N, T, C>& as,
+                                     Color<C>& out) const
+        {
+                const PathVertex<N, T, C>& cv = camera[t_count - 1];
+                const Light<N, T, C>& l = s.lights[li];
+                PathVertex<N, T, C> lv;
+                lv.type = static_cast<int>(VertexType::LIGHT);
+                lv.light = li;
+                lv.has_pos = true;
+                lv.has_normal = false;
+                lv.pos = cv.pos + as.l * as.distance;
+                lv.dir = (-as.l).normalized();
+                lv.pdf_fwd = l.distribution_pdf * l.pdf;
+                lv.pdf_rev = 0;
+
+                const Ray<N, T> ray_to_light = Ray<N, T>::make(cv.pos, as.l);
+                const T n_l = dot(cv.nrm.shading, ray_to_light.dir);
+                if (!(n_l > 0))
+                {
+                        return false;
+                }
+                BrdfTerms terms;
+                const float light_k = static_cast<float>(n_l / (as.pdf * l.distribution_pdf));
+                const Color<C> c = cv.beta * vertex_brdf(cv, cv.dir, ray_to_light.dir, RECORD ? &terms : nullptr) *
+                                   as.radiance * light_k;
+                if (c.is_black())
+                {
+                        return false;
+                }
+                if (occluded_ray(cv.nrm, ray_to_light, as.distance))
+                {
+                        return false;
+                }
+                const float mis = static_cast<float>(mis_weight(&lv, 1, t_count));
+                out = c * mis;
+                if constexpr (RECORD)
+                {
+                        tape.n = tape_slot_offset(max_depth, t_count, 1);
+                        tape.put(static_cast<int>(TapeRecord::STRATEGY_LIGHT));
+                        tape.put(t_count);
+                        tape.put(cv.material);
+                        tape.put(terms);
+                        tape.put(li);
+                        tape.put(light_k);
+                        tape.put(mis);
+                }
+                return true;
+        }
+
         NBPT_CALL bool connect_strategy(const int s_count, const int t_count, Color<C>& out)
         {
                 const PathVertex<N, T, C>& cv = camera[t_count - 1];
@@ -674,55 +734,13 @@ struct Bpt final
                 }
                 if (s_count == 1)
                 {
-                        const int li = sample_light();
-                        const Light<N, T, C>& l = s.lights[li];
-                        const ArriveSample<N, T, C> as = arrive_sample(l, cv.pos);
-                        if (!as.usable())
+                        int li;
+                        ArriveSample<N, T, C> as;
+                        if (!light_arrival(t_count, li, as))
                         {
                                 return false;
                         }
-                        PathVertex<N, T, C> lv;
-                        lv.type = static_cast<int>(VertexType::LIGHT);
-                        lv.light = li;
-                        lv.has_pos = true;
-                        lv.has_normal = false;
-                        lv.pos = cv.pos + as.l * as.distance;
-                        lv.dir = (-as.l).normalized();
-                        lv.pdf_fwd = l.distribution_pdf * l.pdf;
-                        lv.pdf_rev = 0;
-
-                        const Ray<N, T> ray_to_light = Ray<N, T>::make(cv.pos, as.l);
-                        const T n_l = dot(cv.nrm.shading, ray_to_light.dir);
-                        if (!(n_l > 0))
-                        {
-                                return false;
-                        }
-                        BrdfTerms terms;
-                        const float light_k = static_cast<float>(n_l / (as.pdf * l.distribution_pdf));
-                        const Color<C> c = cv.beta * vertex_brdf(cv, cv.dir, ray_to_light.dir, RECORD ? &terms : nullptr) *
-                                           as.radiance * light_k;
-                        if (c.is_black())
-                        {
-                                return false;
-                        }
-                        if (occluded_ray(cv.nrm, ray_to_light, as.distance))
-                        {
-                                return false;
-                        }
-                        const float mis = static_cast<float>(mis_weight(&lv, 1, t_count));
-                        out = c * mis;
-                        if constexpr (RECORD)
-                        {
-                                tape.n = tape_slot_offset(max_depth, t_count, s_count);
-                                tape.put(static_cast<int>(TapeRecord::STRATEGY_LIGHT));
-                                tape.put(t_count);
-                                tape.put(cv.material);
-                                tape.put(terms);
-                                tape.put(li);
-                                tape.put(light_k);
-                                tape.put(mis);
-                        }
-                        return true;
+                        return connect_light(t_count, li, as, out);
                 }
 
                 const PathVertex<N, T, C>& lv = light[s_count - 1];

@@ -194,11 +194,13 @@ __global__ void sj_points_kernel(
 //                         vertices kept in global memory, the bounce records
 //                         on the path's tape, and one task queued per
 //                         strategy with s != 1;
+//   paths_light_kernel    one thread per path: the light samples of the
+//                         s = 1 strategies in t order, since each draws from
+//                         the path's stream where the light subpath left it;
+//                         the usable ones are kept and their strategies
+//                         queued;
 //   paths_connect_kernel  one thread per queued strategy: its contribution
 //                         factors written to the strategy's tape slot;
-//   paths_light_kernel    one thread per path: the s = 1 strategies in t
-//                         order, since each draws a fresh light sample from
-//                         the path's stream where the light subpath left it;
 //   paths_replay_kernel   the colours of all channels from the tapes.
 // Strategies of one path are independent apart from that random stream, so
 // evaluating them on separate threads changes no result; the replay sums
@@ -376,6 +378,17 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_walk_kernel(
         add_counters(counters, stats);
 }
 
+// The light sample of an s = 1 strategy (Bpt::light_arrival), kept for the
+// connect kernel.
+template <int N, typename T>
+struct Arrival final
+{
+        Vec<N, T> l;
+        T pdf;
+        T distance;
+        int light;
+};
+
 // Persistent: the grid strides over the queued strategies.
 template <int N, typename T>
 __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_connect_kernel(
@@ -384,6 +397,7 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_connect_kern
         PathVertex<N, T, 1>* __restrict__ vertices,
         std::uint32_t* __restrict__ tape,
         const int words_per_path,
+        const Arrival<N, T>* __restrict__ arrivals,
         const std::uint32_t* __restrict__ tasks,
         const unsigned* __restrict__ task_count,
         PathStats* __restrict__ stats)
@@ -399,14 +413,29 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_connect_kern
                 const int sc = static_cast<int>(task & 15u);
                 PathVertex<N, T, 1>* const v = vertices + i * 2 * (max_depth + 1);
                 std::uint32_t* const w = tape + i * static_cast<long long>(words_per_path);
-                Pcg unused{0, 0}; // only s = 1 draws random numbers
+                Pcg unused{0, 0}; // the random numbers of s = 1 were drawn by paths_light_kernel
                 const SceneQueries<N, T, 1> q{scene, counters};
                 Bpt<N, T, 1, true> bpt{q, scene, unused, max_depth, v, v + max_depth + 1};
                 bpt.camera_size = static_cast<int>(w[2]);
                 bpt.light_size = static_cast<int>(w[3]);
                 bpt.tape.w = w;
                 Color<1> c;
-                if (!bpt.connect_strategy(sc, t, c))
+                bool contributes;
+                if (sc == 1)
+                {
+                        const Arrival<N, T>& a = arrivals[i * max_depth + (t - 2)];
+                        ArriveSample<N, T, 1> as;
+                        as.l = a.l;
+                        as.pdf = a.pdf;
+                        as.distance = a.distance;
+                        as.radiance = scene.lights[a.light].radiance;
+                        contributes = bpt.connect_light(t, a.light, as, c);
+                }
+                else
+                {
+                        contributes = bpt.connect_strategy(sc, t, c);
+                }
+                if (!contributes)
                 {
                         w[tape_slot_offset(max_depth, t, sc)] = 0;
                 }
@@ -414,6 +443,9 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_connect_kern
         add_counters(counters, stats);
 }
 
+// One thread per path: the light samples of the s = 1 strategies, drawn in
+// t order from the path's stream where the light subpath left it; each
+// usable sample is kept and its strategy queued for the connect kernel.
 template <int N, typename T>
 __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_light_kernel(
         const DeviceScene<N, T, 1> scene,
@@ -423,10 +455,12 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_light_kernel
         const Pcg* __restrict__ rng,
         std::uint32_t* __restrict__ tape,
         const int words_per_path,
-        PathStats* __restrict__ stats)
+        Arrival<N, T>* __restrict__ arrivals,
+        std::uint32_t* __restrict__ tasks,
+        unsigned* __restrict__ task_count)
 {
         const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-        QueryCounters counters{0, 0, 0, 0};
+        unsigned queued = 0; // bit t - 2: strategy (1, t) queued
         if (i < paths)
         {
                 std::uint32_t* const w = tape + i * static_cast<long long>(words_per_path);
@@ -436,26 +470,58 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_light_kernel
                 {
                         Pcg g = rng[i];
                         PathVertex<N, T, 1>* const v = vertices + i * 2 * (max_depth + 1);
+                        QueryCounters counters{0, 0, 0, 0};
                         const SceneQueries<N, T, 1> q{scene, counters};
                         Bpt<N, T, 1, true> bpt{q, scene, g, max_depth, v, v + max_depth + 1};
                         bpt.camera_size = camera_size;
                         bpt.light_size = light_size;
-                        bpt.tape.w = w;
                         for (int t = 2; t <= camera_size; ++t)
                         {
                                 if (t - 1 > max_depth)
                                 {
                                         continue;
                                 }
-                                Color<1> c;
-                                if (!bpt.connect_strategy(1, t, c))
+                                int li = 0;
+                                ArriveSample<N, T, 1> as;
+                                if (v[t - 1].type == static_cast<int>(VertexType::INFINITE) ||
+                                    !bpt.light_arrival(t, li, as))
                                 {
                                         w[tape_slot_offset(max_depth, t, 1)] = 0;
+                                        continue;
                                 }
+                                Arrival<N, T>& a = arrivals[i * max_depth + (t - 2)];
+                                a.l = as.l;
+                                a.pdf = as.pdf;
+                                a.distance = as.distance;
+                                a.light = li;
+                                queued |= 1u << (t - 2);
                         }
                 }
         }
-        add_counters(counters, stats);
+        // reserve this warp's task range with one atomic
+        const int task_n = __popc(queued);
+        const int lane = threadIdx.x & 31;
+        int offset = task_n;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+        {
+                const int x = __shfl_up_sync(0xffffffffu, offset, o);
+                offset += lane >= o ? x : 0;
+        }
+        const int total = __shfl_sync(0xffffffffu, offset, 31);
+        unsigned base = 0;
+        if (lane == 31 && total > 0)
+        {
+                base = atomicAdd(task_count, static_cast<unsigned>(total));
+        }
+        base = __shfl_sync(0xffffffffu, base, 31);
+        unsigned k = base + static_cast<unsigned>(offset - task_n);
+        while (queued != 0)
+        {
+                const int b = __ffs(queued) - 1;
+                queued &= queued - 1;
+                tasks[k++] = make_task(i, b + 2, 1);
+        }
 }
 
 // Colours from the tapes: LANES threads per path (32: one warp per path,

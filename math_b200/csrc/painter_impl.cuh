@@ -1520,6 +1520,7 @@ class PainterT final : public Painter
         DeviceArray<std::uint32_t> tape_;
         DeviceArray<std::uint32_t> tasks_;
         DeviceArray<unsigned> task_count_;
+        DeviceArray<Arrival<N, T>> arrivals_;
         int connect_blocks_ = 0;
         long long launches_ = 0;
         Statistics statistics_{};
@@ -1533,7 +1534,7 @@ class PainterT final : public Painter
         {
                 return static_cast<long long>(tape_words(max_depth)) * 4 +
                        2LL * (max_depth + 1) * sizeof(PathVertex<N, T, 1>) + sizeof(Pcg) +
-                       4LL * tape_slot_count(max_depth);
+                       4LL * tape_slot_count(max_depth) + static_cast<long long>(max_depth) * sizeof(Arrival<N, T>);
         }
 
         static long long chunk_pixels(const long long pixels, const int spp, const int max_depth)
@@ -1610,6 +1611,7 @@ public:
                         rng_.allocate(paths);
                         tasks_.allocate(paths * tape_slot_count(max_depth_));
                         task_count_.allocate(1);
+                        arrivals_.allocate(paths * max_depth_);
                         int device = 0;
                         int sms = 0;
                         NBPT_CUDA(cudaGetDevice(&device));
@@ -1646,7 +1648,7 @@ public:
                 const std::size_t own = offsets_.bytes() + points_.bytes() + colors_.bytes() + lum_.bytes() +
                                         valid_.bytes() + state_.bytes() + stats_.bytes() + rgb_.bytes() +
                                         rgba_.bytes() + vertices_.bytes() + rng_.bytes() + tape_.bytes() +
-                                        tasks_.bytes() + task_count_.bytes();
+                                        tasks_.bytes() + task_count_.bytes() + arrivals_.bytes();
                 return static_cast<long long>(own) + scene_->device_bytes();
         }
 
@@ -1682,13 +1684,13 @@ public:
                                                 vertices_.get(), rng_.get(), tape_.get(), tape_words_, valid_.get() + b * spp_,
                                                 tasks_.get(), task_count_.get(), stats_.get());
                                         NBPT_CUDA(cudaGetLastError());
-                                        paths_connect_kernel<N, T><<<connect_blocks_, 128, 0, stream_>>>(
-                                                scene_1, max_depth_, vertices_.get(), tape_.get(), tape_words_, tasks_.get(),
-                                                task_count_.get(), stats_.get());
-                                        NBPT_CUDA(cudaGetLastError());
                                         paths_light_kernel<N, T><<<blocks_for(n, 128), 128, 0, stream_>>>(
                                                 scene_1, n, max_depth_, vertices_.get(), rng_.get(), tape_.get(), tape_words_,
-                                                stats_.get());
+                                                arrivals_.get(), tasks_.get(), task_count_.get());
+                                        NBPT_CUDA(cudaGetLastError());
+                                        paths_connect_kernel<N, T><<<connect_blocks_, 128, 0, stream_>>>(
+                                                scene_1, max_depth_, vertices_.get(), tape_.get(), tape_words_, arrivals_.get(),
+                                                tasks_.get(), task_count_.get(), stats_.get());
                                         NBPT_CUDA(cudaGetLastError());
                                         constexpr int LANES = C % 32 == 0 ? 32 : 1;
                                         paths_replay_kernel<N, T, C, LANES><<<blocks_for(n * LANES, 128), 128, 0, stream_>>>(
