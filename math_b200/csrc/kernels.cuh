@@ -10,10 +10,14 @@
 #include "shading.cuh"
 #include "tape.cuh"
 
+#include <cooperative_groups.h>
+#include <cooperative_groups/scan.h>
 #include <cstdint>
 
 namespace nbpt
 {
+namespace cg = cooperative_groups;
+
 // ---------------------------------------------------------------------------
 // facet setup at scene load, in double precision (hyperplane_simplex.h:82-111,
 // mesh/facet.cpp:83-125), stored in the path precision T.
@@ -270,6 +274,25 @@ NBPT_HD constexpr std::uint32_t make_task(const long long path, const int t, con
                static_cast<std::uint32_t>(s);
 }
 
+// Reserves `n` consecutive slots of a counter for each calling thread with
+// one atomic per group of threads that call it together.
+__device__ inline unsigned reserve_together(unsigned* const counter, const unsigned n)
+{
+        const cg::coalesced_group g = cg::coalesced_threads();
+        const unsigned before = cg::exclusive_scan(g, n);
+        unsigned base = 0;
+        if (g.thread_rank() == g.size() - 1)
+        {
+                const unsigned total = before + n;
+                base = total > 0 ? atomicAdd(counter, total) : 0;
+        }
+        base = g.shfl(base, g.size() - 1);
+        return base + before;
+}
+
+// Persistent: every thread takes paths from a shared counter until the
+// chunk is done, so lanes whose paths end early start new ones instead of
+// idling while the rest of their warp walks on.
 template <int N, typename T>
 __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_walk_kernel(
         const DeviceScene<N, T, 1> scene,
@@ -287,16 +310,18 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_walk_kernel(
         unsigned char* __restrict__ valid,
         std::uint32_t* __restrict__ tasks,
         unsigned* __restrict__ task_count,
+        unsigned* __restrict__ next_path,
         PathStats* __restrict__ stats)
 {
-        const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
         const long long paths = (end - begin) * spp;
         QueryCounters counters{0, 0, 0, 0};
-        int camera_size = 0;
-        int light_size = 0;
-        int task_n = 0;
-        if (i < paths)
+        while (true)
         {
+                const long long i = reserve_together(next_path, 1);
+                if (i >= paths)
+                {
+                        break;
+                }
                 const long long local_pixel = i / spp;
                 const int sample = static_cast<int>(i - local_pixel * spp);
                 const long long p = begin + local_pixel;
@@ -334,8 +359,9 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_walk_kernel(
                 rng[i] = g;
                 if (connect)
                 {
-                        camera_size = bpt.camera_size;
-                        light_size = bpt.light_size;
+                        const int camera_size = bpt.camera_size;
+                        const int light_size = bpt.light_size;
+                        unsigned task_n = 0;
                         for (int t = 2; t <= camera_size; ++t)
                         {
                                 for (int sc = 0; sc <= light_size; ++sc)
@@ -343,34 +369,15 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_walk_kernel(
                                         task_n += (sc != 1 && t + sc - 2 <= max_depth) ? 1 : 0;
                                 }
                         }
-                }
-        }
-        // reserve this warp's task range with one atomic
-        const int lane = threadIdx.x & 31;
-        int offset = task_n;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1)
-        {
-                const int x = __shfl_up_sync(0xffffffffu, offset, o);
-                offset += lane >= o ? x : 0;
-        }
-        const int total = __shfl_sync(0xffffffffu, offset, 31);
-        unsigned base = 0;
-        if (lane == 31 && total > 0)
-        {
-                base = atomicAdd(task_count, static_cast<unsigned>(total));
-        }
-        base = __shfl_sync(0xffffffffu, base, 31);
-        if (task_n > 0)
-        {
-                unsigned k = base + static_cast<unsigned>(offset - task_n);
-                for (int t = 2; t <= camera_size; ++t)
-                {
-                        for (int sc = 0; sc <= light_size; ++sc)
+                        unsigned k = reserve_together(task_count, task_n);
+                        for (int t = 2; t <= camera_size; ++t)
                         {
-                                if (sc != 1 && t + sc - 2 <= max_depth)
+                                for (int sc = 0; sc <= light_size; ++sc)
                                 {
-                                        tasks[k++] = make_task(i, t, sc);
+                                        if (sc != 1 && t + sc - 2 <= max_depth)
+                                        {
+                                                tasks[k++] = make_task(i, t, sc);
+                                        }
                                 }
                         }
                 }

@@ -1520,6 +1520,7 @@ class PainterT final : public Painter
         DeviceArray<std::uint32_t> tape_;
         DeviceArray<std::uint32_t> tasks_;
         DeviceArray<unsigned> task_count_;
+        DeviceArray<unsigned> next_path_;
         DeviceArray<Arrival<N, T>> arrivals_;
         int connect_blocks_ = 0;
         long long launches_ = 0;
@@ -1611,6 +1612,7 @@ public:
                         rng_.allocate(paths);
                         tasks_.allocate(paths * tape_slot_count(max_depth_));
                         task_count_.allocate(1);
+                        next_path_.allocate(1);
                         arrivals_.allocate(paths * max_depth_);
                         int device = 0;
                         int sms = 0;
@@ -1679,10 +1681,12 @@ public:
                                         const long long e = std::min(pixels_, b + chunk_pixels_);
                                         const long long n = (e - b) * spp_;
                                         NBPT_CUDA(cudaMemsetAsync(task_count_.get(), 0, sizeof(unsigned), stream_));
-                                        paths_walk_kernel<N, T><<<blocks_for(n, 128), 128, 0, stream_>>>(
+                                        NBPT_CUDA(cudaMemsetAsync(next_path_.get(), 0, sizeof(unsigned), stream_));
+                                        paths_walk_kernel<N, T><<<std::min<long long>(connect_blocks_, blocks_for(n, 128)), 128, 0,
+                                                                  stream_>>>(
                                                 scene_1, b, e, spp_, max_depth_, seed_, pass, points_.get() + b * spp_ * (N - 1),
                                                 vertices_.get(), rng_.get(), tape_.get(), tape_words_, valid_.get() + b * spp_,
-                                                tasks_.get(), task_count_.get(), stats_.get());
+                                                tasks_.get(), task_count_.get(), next_path_.get(), stats_.get());
                                         NBPT_CUDA(cudaGetLastError());
                                         paths_light_kernel<N, T><<<blocks_for(n, 128), 128, 0, stream_>>>(
                                                 scene_1, n, max_depth_, vertices_.get(), rng_.get(), tape_.get(), tape_words_,
