@@ -274,6 +274,27 @@ NBPT_HD constexpr std::uint32_t make_task(const long long path, const int t, con
                static_cast<std::uint32_t>(s);
 }
 
+// Queued strategies, one queue per kind so that the warps of the connect
+// kernel run one kind of strategy at a time: s = 0 (emission at a camera
+// vertex), s = 1 (a resampled light) and s >= 2 (a vertex-vertex connection).
+// The queues are regions of one buffer with a counter each.
+struct TaskQueues final
+{
+        enum Kind : int
+        {
+                CONNECT = 0,
+                LIGHT = 1,
+                EMITTED = 2
+        };
+        std::uint32_t* base[3];
+        unsigned* count; // [3]
+
+        __device__ std::uint32_t& task(const int kind, const unsigned k) const
+        {
+                return base[kind][k];
+        }
+};
+
 // Reserves `n` consecutive slots of a counter for each calling thread with
 // one atomic per group of threads that call it together.
 __device__ inline unsigned reserve_together(unsigned* const counter, const unsigned n)
@@ -308,8 +329,7 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_walk_kernel(
         std::uint32_t* __restrict__ tape,
         const int words_per_path,
         unsigned char* __restrict__ valid,
-        std::uint32_t* __restrict__ tasks,
-        unsigned* __restrict__ task_count,
+        const TaskQueues queues,
         unsigned* __restrict__ next_path,
         PathStats* __restrict__ stats)
 {
@@ -361,22 +381,29 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_walk_kernel(
                 {
                         const int camera_size = bpt.camera_size;
                         const int light_size = bpt.light_size;
+                        // s = 0 strategies: one per t
+                        unsigned k = reserve_together(&queues.count[TaskQueues::EMITTED], camera_size - 1);
+                        for (int t = 2; t <= camera_size; ++t)
+                        {
+                                queues.task(TaskQueues::EMITTED, k++) = make_task(i, t, 0);
+                        }
+                        // s >= 2 strategies
                         unsigned task_n = 0;
                         for (int t = 2; t <= camera_size; ++t)
                         {
-                                for (int sc = 0; sc <= light_size; ++sc)
+                                for (int sc = 2; sc <= light_size; ++sc)
                                 {
-                                        task_n += (sc != 1 && t + sc - 2 <= max_depth) ? 1 : 0;
+                                        task_n += (t + sc - 2 <= max_depth) ? 1 : 0;
                                 }
                         }
-                        unsigned k = reserve_together(task_count, task_n);
+                        k = reserve_together(&queues.count[TaskQueues::CONNECT], task_n);
                         for (int t = 2; t <= camera_size; ++t)
                         {
-                                for (int sc = 0; sc <= light_size; ++sc)
+                                for (int sc = 2; sc <= light_size; ++sc)
                                 {
-                                        if (sc != 1 && t + sc - 2 <= max_depth)
+                                        if (t + sc - 2 <= max_depth)
                                         {
-                                                tasks[k++] = make_task(i, t, sc);
+                                                queues.task(TaskQueues::CONNECT, k++) = make_task(i, t, sc);
                                         }
                                 }
                         }
@@ -405,16 +432,18 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_connect_kern
         std::uint32_t* __restrict__ tape,
         const int words_per_path,
         const Arrival<N, T>* __restrict__ arrivals,
-        const std::uint32_t* __restrict__ tasks,
-        const unsigned* __restrict__ task_count,
+        const TaskQueues queues,
         PathStats* __restrict__ stats)
 {
         QueryCounters counters{0, 0, 0, 0};
-        const unsigned total = *task_count;
+        const unsigned n0 = queues.count[0];
+        const unsigned n1 = queues.count[1];
+        const unsigned total = n0 + n1 + queues.count[2];
         const unsigned stride = gridDim.x * blockDim.x;
         for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += stride)
         {
-                const std::uint32_t task = tasks[k];
+                const std::uint32_t task =
+                        k < n0 ? queues.base[0][k] : (k < n0 + n1 ? queues.base[1][k - n0] : queues.base[2][k - n0 - n1]);
                 const long long i = task >> TASK_PATH_SHIFT;
                 const int t = static_cast<int>((task >> 4) & 15u);
                 const int sc = static_cast<int>(task & 15u);
@@ -463,8 +492,7 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_light_kernel
         std::uint32_t* __restrict__ tape,
         const int words_per_path,
         Arrival<N, T>* __restrict__ arrivals,
-        std::uint32_t* __restrict__ tasks,
-        unsigned* __restrict__ task_count)
+        const TaskQueues queues)
 {
         const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
         unsigned queued = 0; // bit t - 2: strategy (1, t) queued
@@ -519,7 +547,7 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_light_kernel
         unsigned base = 0;
         if (lane == 31 && total > 0)
         {
-                base = atomicAdd(task_count, static_cast<unsigned>(total));
+                base = atomicAdd(&queues.count[TaskQueues::LIGHT], static_cast<unsigned>(total));
         }
         base = __shfl_sync(0xffffffffu, base, 31);
         unsigned k = base + static_cast<unsigned>(offset - task_n);
@@ -527,7 +555,7 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_light_kernel
         {
                 const int b = __ffs(queued) - 1;
                 queued &= queued - 1;
-                tasks[k++] = make_task(i, b + 2, 1);
+                queues.task(TaskQueues::LIGHT, k++) = make_task(i, b + 2, 1);
         }
 }
 

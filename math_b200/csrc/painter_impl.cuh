@@ -1611,7 +1611,7 @@ public:
                         vertices_.allocate(paths * 2 * (max_depth_ + 1));
                         rng_.allocate(paths);
                         tasks_.allocate(paths * tape_slot_count(max_depth_));
-                        task_count_.allocate(1);
+                        task_count_.allocate(3);
                         next_path_.allocate(1);
                         arrivals_.allocate(paths * max_depth_);
                         int device = 0;
@@ -1680,21 +1680,30 @@ public:
                                 {
                                         const long long e = std::min(pixels_, b + chunk_pixels_);
                                         const long long n = (e - b) * spp_;
-                                        NBPT_CUDA(cudaMemsetAsync(task_count_.get(), 0, sizeof(unsigned), stream_));
+                                        NBPT_CUDA(cudaMemsetAsync(task_count_.get(), 0, 3 * sizeof(unsigned), stream_));
+                                        // queue regions: s >= 2, then s = 1 and s = 0 (at most
+                                        // max_depth each per path)
+                                        TaskQueues queues;
+                                        queues.base[TaskQueues::CONNECT] = tasks_.get();
+                                        queues.base[TaskQueues::LIGHT] =
+                                                tasks_.get() + n * (tape_slot_count(max_depth_) - 2 * max_depth_);
+                                        queues.base[TaskQueues::EMITTED] =
+                                                tasks_.get() + n * (tape_slot_count(max_depth_) - max_depth_);
+                                        queues.count = task_count_.get();
                                         NBPT_CUDA(cudaMemsetAsync(next_path_.get(), 0, sizeof(unsigned), stream_));
                                         paths_walk_kernel<N, T><<<std::min<long long>(connect_blocks_, blocks_for(n, 128)), 128, 0,
                                                                   stream_>>>(
                                                 scene_1, b, e, spp_, max_depth_, seed_, pass, points_.get() + b * spp_ * (N - 1),
                                                 vertices_.get(), rng_.get(), tape_.get(), tape_words_, valid_.get() + b * spp_,
-                                                tasks_.get(), task_count_.get(), next_path_.get(), stats_.get());
+                                                queues, next_path_.get(), stats_.get());
                                         NBPT_CUDA(cudaGetLastError());
                                         paths_light_kernel<N, T><<<blocks_for(n, 128), 128, 0, stream_>>>(
                                                 scene_1, n, max_depth_, vertices_.get(), rng_.get(), tape_.get(), tape_words_,
-                                                arrivals_.get(), tasks_.get(), task_count_.get());
+                                                arrivals_.get(), queues);
                                         NBPT_CUDA(cudaGetLastError());
                                         paths_connect_kernel<N, T><<<connect_blocks_, 128, 0, stream_>>>(
                                                 scene_1, max_depth_, vertices_.get(), tape_.get(), tape_words_, arrivals_.get(),
-                                                tasks_.get(), task_count_.get(), stats_.get());
+                                                queues, stats_.get());
                                         NBPT_CUDA(cudaGetLastError());
                                         constexpr int LANES = C % 32 == 0 ? 32 : 1;
                                         paths_replay_kernel<N, T, C, LANES><<<blocks_for(n * LANES, 128), 128, 0, stream_>>>(
