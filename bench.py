@@ -235,6 +235,23 @@ def run_reference(args, rank: int):
     }))
 
 
+def slowest_rank(seconds: float, world: int, device: str) -> float:
+    """The largest of every rank's time (all ranks must call it)."""
+    if world <= 1:
+        return seconds
+    import torch
+
+    t = torch.tensor([seconds], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(units_per_rank: float, world: int, seconds: float) -> float:
+    """Whole-job throughput: every rank processed `units_per_rank` (weak
+    scaling), timed by the slowest rank."""
+    return world * units_per_rank / seconds
+
+
 def run_nbpt(args, rank: int, world: int, local: int):
     import torch
 
@@ -291,12 +308,8 @@ def run_nbpt(args, rank: int, world: int, local: int):
     clock_info = clocks.stop()
 
     paths_per_step = scene.pixels * painter.spp
-    ms = float(np.sum(step_ms))
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * paths_per_step * args.steps / (ms / 1000)
+    ms = slowest_rank(float(np.sum(step_ms)), world, "cuda")
+    value = job_throughput(paths_per_step * args.steps, world, ms / 1000)
 
     # end to end through the C ABI, every step a whole job: the scene built
     # from host arrays (host->device copies, BVH build, facet setup on the
@@ -316,12 +329,8 @@ def run_nbpt(args, rank: int, world: int, local: int):
         h2d = job_scene.upload_bytes()
         job.close()
         job_scene.close()
-    e2e_s = float(np.sum(e2e_times))
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = world * paths_per_step * args.steps / e2e_s
+    e2e_s = slowest_rank(float(np.sum(e2e_times)), world, "cuda")
+    e2e = job_throughput(paths_per_step * args.steps, world, e2e_s)
 
     # scene resident: one pass through the C ABI plus the image read back
     torch.cuda.synchronize()
