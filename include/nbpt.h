@@ -158,6 +158,14 @@ long long nbpt_scene_upload_bytes(const nbpt_scene* scene);
  * (seed, pass, pixel, sample) and accumulates the filtered, trimmed pixel
  * estimator.  max_depth is the reference's MAX_DEPTH (1..8). */
 nbpt_painter* nbpt_painter_create(nbpt_scene* scene, int samples_per_pixel, int max_depth, unsigned seed);
+/* painter::create_painter(Integrator, ...) (src/painter/painter.h:143-157):
+ * NBPT_INTEGRATOR_BPT as nbpt_painter_create; NBPT_INTEGRATOR_PT runs the
+ * path tracer with next-event estimation and Russian roulette
+ * (src/painter/integrators/pt/pt.cpp:138-170), which ignores max_depth */
+#define NBPT_INTEGRATOR_BPT 0
+#define NBPT_INTEGRATOR_PT 1
+nbpt_painter* nbpt_painter_create_integrator(
+        nbpt_scene* scene, int integrator, int samples_per_pixel, int max_depth, unsigned seed);
 void nbpt_painter_destroy(nbpt_painter* painter);
 /* enqueues `passes` passes on the painter's CUDA stream and returns */
 int nbpt_painter_enqueue(nbpt_painter* painter, int passes);

@@ -576,6 +576,30 @@ nbpt_painter* nbpt_painter_create(nbpt_scene* scene, const int samples_per_pixel
         return out;
 }
 
+nbpt_painter* nbpt_painter_create_integrator(
+        nbpt_scene* scene,
+        const int integrator,
+        const int samples_per_pixel,
+        const int max_depth,
+        const unsigned seed)
+{
+        nbpt_painter* out = nullptr;
+        guarded(
+                [&]
+                {
+                        if (integrator != NBPT_INTEGRATOR_BPT && integrator != NBPT_INTEGRATOR_PT)
+                        {
+                                throw std::runtime_error("Unknown integrator " + std::to_string(integrator));
+                        }
+                        auto p = std::make_unique<nbpt_painter>();
+                        p->impl = scene_of(scene).create_painter(samples_per_pixel, max_depth, seed,
+                                                                 static_cast<nbpt::Integrator>(integrator));
+                        out = p.release();
+                        return 0;
+                });
+        return out;
+}
+
 void nbpt_painter_destroy(nbpt_painter* painter)
 {
         delete painter;

@@ -22,6 +22,13 @@ struct Statistics final
         long long kernel_launches;     // kernels launched by the last pass
 };
 
+// painter::Integrator (src/painter/painter.h:143-147), same order
+enum class Integrator : int
+{
+        BPT = 0,
+        PT = 1
+};
+
 class Painter
 {
 public:
@@ -70,9 +77,13 @@ public:
         virtual long long device_bytes() const = 0;
         virtual long long upload_bytes() const = 0;
 
-        virtual std::unique_ptr<Painter> create_painter(int samples_per_pixel, int max_depth, std::uint32_t seed) = 0;
+        // max_depth bounds the BPT subpaths; the PT integrator ends its paths
+        // by Russian roulette and ignores it
+        virtual std::unique_ptr<Painter> create_painter(int samples_per_pixel, int max_depth, std::uint32_t seed,
+                                                        Integrator integrator = Integrator::BPT) = 0;
         // device bytes create_painter would allocate
-        virtual long long painter_bytes(int samples_per_pixel, int max_depth) const = 0;
+        virtual long long painter_bytes(int samples_per_pixel, int max_depth,
+                                        Integrator integrator = Integrator::BPT) const = 0;
 
         // verification: closest hit (any == 0) or any hit of rays [n][2N]
         virtual void trace(const double* rays, long long count, int any, int* kind, int* index, double* t,

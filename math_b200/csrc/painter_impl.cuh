@@ -17,6 +17,7 @@
 #include "host_math.h"
 #include "kernels.cuh"
 #include "painter_api.h"
+#include "pt.cuh"
 #include "tables.inc"
 
 #include <cuda_runtime.h>
@@ -852,6 +853,7 @@ public:
                 {
                         l.radiance.c[c] = rad[c];
                 }
+                l.shape = fi;
                 lights_.push_back(l);
                 flat_[fi].light = static_cast<int>(lights_.size()) - 1;
                 return static_cast<int>(lights_.size()) - 1;
@@ -880,6 +882,7 @@ public:
                 }
                 const T pdf_unit = static_cast<T>(1 / host::ball_volume(N - 1));
                 l.pdf = pdf_unit / power<N - 1>(r);
+                l.radius_squared = square(r);
                 const std::vector<float> rad = host::illuminant_color(C, rgb);
                 for (int c = 0; c < C; ++c)
                 {
@@ -1212,6 +1215,8 @@ public:
                                 o.radiance.c[0] = l.radiance.c[0];
                                 o.distribution_pdf = l.distribution_pdf;
                                 o.cumulative = l.cumulative;
+                                o.shape = l.shape;
+                                o.radius_squared = l.radius_squared;
                         }
                         d_materials_1_.upload(m1);
                         d_lights_1_.upload(l1);
@@ -1324,8 +1329,9 @@ public:
                 return d_cie_.get();
         }
 
-        std::unique_ptr<Painter> create_painter(int spp, int max_depth, std::uint32_t seed) override;
-        long long painter_bytes(int spp, int max_depth) const override;
+        std::unique_ptr<Painter> create_painter(int spp, int max_depth, std::uint32_t seed,
+                                                Integrator integrator) override;
+        long long painter_bytes(int spp, int max_depth, Integrator integrator) const override;
 
         void trace(const double* rays, long long count, int any, int* kind, int* index, double* t, double* point) override;
         void trace_device(const double* rays, long long count, int any, int* kind, int* index, double* t,
@@ -1493,6 +1499,7 @@ class PainterT final : public Painter
         int strata_;
         int max_depth_;
         std::uint32_t seed_;
+        Integrator integrator_;
         long long pixels_;
         long long pass_ = 0;
         long long passes_done_ = 0;
@@ -1538,8 +1545,17 @@ class PainterT final : public Painter
                        4LL * tape_slot_count(max_depth) + static_cast<long long>(max_depth) * sizeof(Arrival<N, T>);
         }
 
-        static long long chunk_pixels(const long long pixels, const int spp, const int max_depth)
+        // the PT kernel keeps nothing per path; its chunks only bound the
+        // 32-bit path counter
+        static constexpr long long PT_CHUNK_PATHS = 1LL << 30;
+
+        static long long chunk_pixels(const long long pixels, const int spp, const int max_depth,
+                                      const Integrator integrator)
         {
+                if (integrator == Integrator::PT)
+                {
+                        return std::max(1LL, std::min(pixels, PT_CHUNK_PATHS / spp));
+                }
                 const long long per_pixel = chunk_path_bytes(max_depth) * spp;
                 long long c = std::max(1LL, std::min(pixels, CHUNK_BUDGET / per_pixel));
                 return std::min(c, (TASK_MAX_PATHS - 1) / spp);
@@ -1547,26 +1563,37 @@ class PainterT final : public Painter
 
 public:
         // device bytes a painter of these parameters allocates
-        static long long estimate_bytes(const long long pixels, const int spp, const int max_depth, const int strata)
+        static long long estimate_bytes(const long long pixels, const int spp, const int max_depth, const int strata,
+                                        const Integrator integrator)
         {
                 const long long samples = pixels * spp;
                 const long long per_sample = (N - 1) * sizeof(T) + C * 4 + 4 + 1;
                 const long long per_pixel = sizeof(PixelState<C>) + 12 + 16;
+                const long long chunk = integrator == Integrator::PT
+                                                ? 4 // the path counter
+                                                : chunk_pixels(pixels, spp, max_depth, integrator) * spp *
+                                                          chunk_path_bytes(max_depth);
                 return (strata + 1) * sizeof(T) + samples * per_sample + pixels * per_pixel + sizeof(PathStats) +
-                       chunk_pixels(pixels, spp, max_depth) * spp * chunk_path_bytes(max_depth);
+                       chunk;
         }
 
-        PainterT(const SceneT<N, T, C>* scene, const int spp, const int max_depth, const std::uint32_t seed)
+        PainterT(const SceneT<N, T, C>* scene, const int spp, const int max_depth, const std::uint32_t seed,
+                 const Integrator integrator)
                 : scene_(scene),
                   spp_request_(spp),
                   max_depth_(max_depth),
-                  seed_(seed)
+                  seed_(seed),
+                  integrator_(integrator)
         {
                 if (spp < 1)
                 {
                         throw std::runtime_error("Painter samples per pixel must be greater than 0");
                 }
-                if (max_depth < 1 || max_depth > MAX_PATH_VERTICES - 1)
+                if (integrator != Integrator::BPT && integrator != Integrator::PT)
+                {
+                        throw std::runtime_error("Unknown integrator " + std::to_string(static_cast<int>(integrator)));
+                }
+                if (integrator == Integrator::BPT && (max_depth < 1 || max_depth > MAX_PATH_VERTICES - 1))
                 {
                         throw std::runtime_error("Painter maximum depth must be in [1, 8]");
                 }
@@ -1603,9 +1630,19 @@ public:
                 stats_.allocate(1);
                 rgb_.allocate(pixels_ * 3);
                 rgba_.allocate(pixels_ * 4);
+                int device = 0;
+                int sms = 0;
+                NBPT_CUDA(cudaGetDevice(&device));
+                NBPT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+                chunk_pixels_ = chunk_pixels(pixels_, spp_, max_depth_, integrator_);
+                if (integrator_ == Integrator::PT)
+                {
+                        next_path_.allocate(1);
+                        connect_blocks_ = sms * NBPT_PT_MIN_BLOCKS;
+                }
+                else
                 {
                         tape_words_ = tape_words(max_depth_);
-                        chunk_pixels_ = chunk_pixels(pixels_, spp_, max_depth_);
                         const long long paths = chunk_pixels_ * spp_;
                         tape_.allocate(paths * tape_words_);
                         vertices_.allocate(paths * 2 * (max_depth_ + 1));
@@ -1614,10 +1651,6 @@ public:
                         task_count_.allocate(3);
                         next_path_.allocate(1);
                         arrivals_.allocate(paths * max_depth_);
-                        int device = 0;
-                        int sms = 0;
-                        NBPT_CUDA(cudaGetDevice(&device));
-                        NBPT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
                         connect_blocks_ = sms * NBPT_PATHS_MIN_BLOCKS;
                 }
 
@@ -1650,7 +1683,8 @@ public:
                 const std::size_t own = offsets_.bytes() + points_.bytes() + colors_.bytes() + lum_.bytes() +
                                         valid_.bytes() + state_.bytes() + stats_.bytes() + rgb_.bytes() +
                                         rgba_.bytes() + vertices_.bytes() + rng_.bytes() + tape_.bytes() +
-                                        tasks_.bytes() + task_count_.bytes() + arrivals_.bytes();
+                                        tasks_.bytes() + task_count_.bytes() + arrivals_.bytes() +
+                                        next_path_.bytes();
                 return static_cast<long long>(own) + scene_->device_bytes();
         }
 
@@ -1672,6 +1706,25 @@ public:
                         NBPT_CUDA(cudaGetLastError());
                         NBPT_CUDA(cudaEventRecord(ev_paths_, stream_));
                         long long launches = 2;
+                        if (integrator_ == Integrator::PT)
+                        {
+                                // one launch per chunk: whole paths (pt.cuh)
+                                for (long long b = 0; b < pixels_; b += chunk_pixels_)
+                                {
+                                        const long long e = std::min(pixels_, b + chunk_pixels_);
+                                        const long long n = (e - b) * spp_;
+                                        NBPT_CUDA(cudaMemsetAsync(next_path_.get(), 0, sizeof(unsigned), stream_));
+                                        pt_paths_kernel<N, T, C>
+                                                <<<std::min<long long>(connect_blocks_, blocks_for(n, 128)), 128, 0, stream_>>>(
+                                                        scene, b, e, spp_, seed_, pass, points_.get() + b * spp_ * (N - 1),
+                                                        colors_.get() + b * spp_ * C, lum_.get() + b * spp_,
+                                                        valid_.get() + b * spp_, next_path_.get(), stats_.get(),
+                                                        scene_->cie() + 64);
+                                        NBPT_CUDA(cudaGetLastError());
+                                        launches += 1;
+                                }
+                        }
+                        else
                         {
                                 // per chunk of pixels: subpaths, strategies, the s = 1
                                 // strategies, then the colours (kernels.cuh)
@@ -1810,19 +1863,23 @@ public:
 };
 
 template <int N, typename T, int C>
-std::unique_ptr<Painter> SceneT<N, T, C>::create_painter(const int spp, const int max_depth, const std::uint32_t seed)
+std::unique_ptr<Painter> SceneT<N, T, C>::create_painter(
+        const int spp,
+        const int max_depth,
+        const std::uint32_t seed,
+        const Integrator integrator)
 {
-        return std::make_unique<PainterT<N, T, C>>(this, spp, max_depth, seed);
+        return std::make_unique<PainterT<N, T, C>>(this, spp, max_depth, seed, integrator);
 }
 
 template <int N, typename T, int C>
-long long SceneT<N, T, C>::painter_bytes(const int spp, const int max_depth) const
+long long SceneT<N, T, C>::painter_bytes(const int spp, const int max_depth, const Integrator integrator) const
 {
-        if (spp < 1 || max_depth < 1)
+        if (spp < 1 || (integrator == Integrator::BPT && max_depth < 1))
         {
                 throw std::runtime_error("painter samples per pixel and maximum depth must be positive");
         }
-        return PainterT<N, T, C>::estimate_bytes(pixel_count(), actual_spp(spp), max_depth, strata(spp));
+        return PainterT<N, T, C>::estimate_bytes(pixel_count(), actual_spp(spp), max_depth, strata(spp), integrator);
 }
 
 template <int N, typename T, int C>

@@ -108,6 +108,8 @@ struct Light final
         Color<C> radiance;
         T distribution_pdf; // probability of choosing this light
         double cumulative;  // discrete-distribution cumulative probability
+        int shape;          // parallelotope: the flat shape that carries it
+        T radius_squared;   // ball: square of the radius
 };
 
 enum class ProjectorType : int

@@ -87,6 +87,7 @@ SIGNATURES = [
     ("nbpt_scene_device_bytes", ctypes.c_longlong, [_P]),
     ("nbpt_scene_upload_bytes", ctypes.c_longlong, [_P]),
     ("nbpt_painter_create", _P, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_uint]),
+    ("nbpt_painter_create_integrator", _P, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint]),
     ("nbpt_painter_destroy", None, [_P]),
     ("nbpt_painter_enqueue", ctypes.c_int, [_P, ctypes.c_int]),
     ("nbpt_painter_wait", ctypes.c_int, [_P]),
@@ -268,8 +269,9 @@ class Scene:
     def upload_bytes(self) -> int:
         return _check(lib().nbpt_scene_upload_bytes(self.h))
 
-    def painter(self, samples_per_pixel: int, max_depth: int, seed: int = 1) -> "Painter":
-        return Painter(self, samples_per_pixel, max_depth, seed)
+    def painter(self, samples_per_pixel: int, max_depth: int, seed: int = 1,
+                integrator: str = "bpt") -> "Painter":
+        return Painter(self, samples_per_pixel, max_depth, seed, integrator)
 
     def trace(self, rays: np.ndarray, any_hit: bool = False):
         rays = _d(rays).reshape(-1, 2 * self.n)
@@ -326,13 +328,24 @@ class Scene:
         return out, rad
 
 
-class Painter:
-    """One render of a scene (the reference's create_painter with BPT)."""
+# painter::Integrator (src/painter/painter.h:143-147)
+INTEGRATORS = {"bpt": 0, "pt": 1}
 
-    def __init__(self, scene: Scene, samples_per_pixel: int, max_depth: int, seed: int = 1):
+
+class Painter:
+    """One render of a scene (the reference's create_painter): integrator
+    "bpt" (bidirectional, max_depth bounds the subpaths) or "pt" (path
+    tracing with next-event estimation; max_depth is not used)."""
+
+    def __init__(self, scene: Scene, samples_per_pixel: int, max_depth: int, seed: int = 1,
+                 integrator: str = "bpt"):
+        if integrator not in INTEGRATORS:
+            raise PainterError(f"Unknown integrator {integrator!r}")
         self.scene = scene
+        self.integrator = integrator
         self.spp = scene.actual_spp(samples_per_pixel)
-        self.h = lib().nbpt_painter_create(scene.h, samples_per_pixel, max_depth, seed)
+        self.h = lib().nbpt_painter_create_integrator(scene.h, INTEGRATORS[integrator], samples_per_pixel,
+                                                      max_depth, seed)
         if not self.h:
             raise PainterError(lib().nbpt_last_error().decode())
 

@@ -53,6 +53,7 @@
 #include <src/numerical/vector.h>
 #include <src/painter/integrators/bpt/bpt.h>
 #include <src/painter/integrators/bpt/light_distribution.h>
+#include <src/painter/integrators/pt/pt.h>
 #include <src/painter/lights/ball_light.h>
 #include <src/painter/lights/parallelotope_light.h>
 #include <src/painter/objects.h>
@@ -363,6 +364,7 @@ struct SceneBase
         virtual void finalize(const float*) = 0;
         virtual long long pixel_count() const = 0;
         virtual int actual_spp(int) const = 0;
+        virtual void set_integrator(int) = 0;
         virtual void render_samples(int, int, unsigned, unsigned, long long, long long, int, double*, float*, unsigned char*) = 0;
         virtual void render_image(int, int, unsigned, int, int, float*, float*) = 0;
         virtual void paint(int, int, int, int, double*, float*) = 0;
@@ -641,9 +643,20 @@ public:
                 return points.size();
         }
 
-        // One pass of per-path seeded BPT over pixels [begin, end).
+        int integrator_ = 0;
+
+        void set_integrator(const int integrator) override
+        {
+                if (integrator != 0 && integrator != 1)
+                {
+                        throw std::runtime_error("integrator must be 0 (BPT) or 1 (PT)");
+                }
+                integrator_ = integrator;
+        }
+
+        // One pass of per-path seeded BPT (or PT) over pixels [begin, end).
         // points: [pixel][sample][N-1] double; colors: [pixel][sample][C] float;
-        // valid: [pixel][sample] 1 if bpt() returned a colour, 0 for a
+        // valid: [pixel][sample] 1 if bpt() / pt() returned a colour, 0 for a
         // background sample (std::nullopt).
         void render_samples(
                 const int spp,
@@ -692,7 +705,10 @@ public:
                                                  static_cast<std::uint32_t>(i + 1)});
                                         const numerical::Ray<N, T> ray = sc.projector().ray(pixel_org + points[i]);
                                         const std::optional<Color> color =
-                                                painter::integrators::bpt::bpt<false>(sc, ray, *distribution, *engine);
+                                                integrator_ == 1
+                                                        ? painter::integrators::pt::pt<false>(sc, ray, *engine)
+                                                        : painter::integrators::bpt::bpt<false>(
+                                                                  sc, ray, *distribution, *engine);
                                         const long long s = k * count + i;
                                         for (std::size_t d = 0; d < N - 1; ++d)
                                         {
@@ -794,7 +810,8 @@ public:
                 CollectNotifier<N - 1> notifier;
                 const auto start = std::chrono::steady_clock::now();
                 std::unique_ptr<painter::Painter> p = painter::create_painter<N, T, Color>(
-                        painter::Integrator::BPT, &notifier, spp, passes, &sc, threads, false);
+                        integrator_ == 1 ? painter::Integrator::PT : painter::Integrator::BPT, &notifier, spp, passes,
+                        &sc, threads, false);
                 p->wait();
                 const double wall =
                         std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
@@ -1380,6 +1397,15 @@ int oracle_scene_actual_spp(void* const scene, const int spp)
                         res = as_scene(scene)->actual_spp(spp);
                 });
         return res;
+}
+
+int oracle_scene_set_integrator(void* const scene, const int integrator)
+{
+        return guarded(
+                [&]
+                {
+                        as_scene(scene)->set_integrator(integrator);
+                });
 }
 
 int oracle_render_samples(

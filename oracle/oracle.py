@@ -55,6 +55,7 @@ def lib():
             "oracle_scene_finalize": (ctypes.c_int, [_P, _F]),
             "oracle_scene_pixel_count": (ctypes.c_longlong, [_P]),
             "oracle_scene_actual_spp": (ctypes.c_int, [_P, ctypes.c_int]),
+            "oracle_scene_set_integrator": (ctypes.c_int, [_P, ctypes.c_int]),
             "oracle_render_samples": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.c_uint, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_int, _D, _F, _B]),
             "oracle_render_image": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.c_int, ctypes.c_int, _F, _F]),
             "oracle_paint": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _F]),
@@ -183,6 +184,12 @@ class Scene:
 
     def actual_spp(self, spp: int) -> int:
         return _check(lib().oracle_scene_actual_spp(self.h, spp))
+
+    def set_integrator(self, integrator: str):
+        """'bpt' (the default) or 'pt' for render_samples, render_image and paint."""
+        if integrator not in ("bpt", "pt"):
+            raise ValueError(f"Unknown integrator {integrator!r}")
+        _check(lib().oracle_scene_set_integrator(self.h, {"bpt": 0, "pt": 1}[integrator]))
 
     def render_samples(self, spp: int, max_depth: int, seed: int, pass_index: int = 0,
                        begin: int = 0, end: int | None = None, threads: int | None = None):

@@ -15,6 +15,13 @@ Fixtures (numpy .npz):
                double precision, 64-bin spectrum, 8 spp, depth 6
   cornell5d.npz  5-space box (4x4x4x4, hull of 200 points on S^4), double,
                RGB, 16 spp, depth 5
+  pt.npz       the PT integrator (src/painter/integrators/pt/pt.cpp) on the
+               three boxes above (keys <name>_colors, _valid, _rgb, _rgba;
+               same scenes, seeds and sample points) and on a 4-space sphere
+               lit by a ball light (8x8x8, hull of 2,000 points, RGB, 16 spp;
+               keys sphere4d_*, with its mesh arrays)
+
+    python tests/golden/make_golden.py pt    # pt.npz only
 """
 
 from __future__ import annotations
@@ -90,10 +97,39 @@ def small_scenes() -> dict:
     }
 
 
+def pt_sphere_scene() -> tuple:
+    return scenes.sphere_4d(size=(8, 8, 8), points=2000, buckets=4), False, 16
+
+
+def pt_fixture():
+    out = {}
+
+    def render(prefix: str, s: oracle.Scene, spp: int, depth: int):
+        s.set_integrator("pt")
+        _, colors, valid = s.render_samples(spp, depth, seed=1, pass_index=0)
+        rgb, rgba = s.render_image(spp, depth, seed=1, passes=1)
+        out.update({f"{prefix}_colors": colors, f"{prefix}_valid": valid, f"{prefix}_rgb": rgb,
+                    f"{prefix}_rgba": rgba})
+
+    for name, (desc, spectrum, spp, depth) in small_scenes().items():
+        render(name, oracle.Scene(desc, "double", spectrum), spp, depth)
+    desc, spectrum, spp = pt_sphere_scene()
+    s = oracle.Scene(desc, "double", spectrum)
+    out.update({f"sphere4d_mesh_{k}": v for k, v in mesh_arrays(s).items()
+                if k not in ("planes", "node_bounds", "node_info", "indices")})
+    out["sphere4d_spp"] = np.int32(spp)
+    render("sphere4d", s, spp, 1)
+    np.savez_compressed(OUT / "pt.npz", **out)
+
+
 def main():
+    if sys.argv[1:] == ["pt"]:
+        pt_fixture()
+        return
     rng_fixture()
     for name, (desc, spectrum, spp, depth) in small_scenes().items():
         scene_fixture(name, desc, spectrum, spp, depth, rays=4096)
+    pt_fixture()
 
 
 if __name__ == "__main__":

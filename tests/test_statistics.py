@@ -1,5 +1,6 @@
 """Statistical parity: the GPU painter in single precision against the
-reference painter in double precision, on independent random streams.
+reference painter in double precision, on independent random streams, for
+both integrators (BPT and PT).
 
 Each side renders K one-pass images with different seeds; per pixel the two
 means are compared with the z-score
@@ -24,8 +25,9 @@ from math_b200 import scenes
 K = 48
 
 CASES = {
-    "cornell3d": (lambda: scenes.cornell_3d(size=(32, 32), subdivisions=3), False, 16, 5),
-    "cornell4d": (lambda: scenes.cornell_4d(size=(10, 10, 10), points=600), True, 8, 6),
+    "cornell3d": (lambda: scenes.cornell_3d(size=(32, 32), subdivisions=3), False, 16, 5, "bpt"),
+    "cornell4d": (lambda: scenes.cornell_4d(size=(10, 10, 10), points=600), True, 8, 6, "bpt"),
+    "cornell3d_pt": (lambda: scenes.cornell_3d(size=(32, 32), subdivisions=3), False, 16, 5, "pt"),
 }
 
 
@@ -48,16 +50,17 @@ def z_scores(a: np.ndarray, b: np.ndarray) -> np.ndarray:
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", list(CASES))
 def test_float_gpu_matches_double_reference_statistically(painter, oracle_lib, name):
-    make, spectrum, spp, depth = CASES[name]
+    make, spectrum, spp, depth, integrator = CASES[name]
     desc = make()
     scene = P.Scene(desc, "float", spectrum)
     gpu = []
     for k in range(K):
-        p = scene.painter(spp, depth, seed=1000 + k)
+        p = scene.painter(spp, depth, seed=1000 + k, integrator=integrator)
         p.run(1)
         gpu.append(luminance(p.images()[0]))
         p.close()
     ref_scene = oracle_lib.Scene(desc, "double", spectrum)
+    ref_scene.set_integrator(integrator)
     ref = [luminance(ref_scene.render_image(spp, depth, seed=5000 + k)[0]) for k in range(K)]
     gpu = np.array(gpu)
     ref = np.array(ref)
