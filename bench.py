@@ -68,6 +68,8 @@ def parse():
                         "workloads; batch: the mixed-scene batch, FP32 through the "
                         "job server against plain FP64 one job at a time; serve: Poisson arrivals of renders "
                         "into the job server, with completion latencies")
+    p.add_argument("--integrator", default="bpt", choices=["bpt", "pt"],
+                   help="single-scene workloads: bidirectional (the headline) or path tracing")
     p.add_argument("--jobs", type=int, default=64, help="batch: scenes in the batch")
     p.add_argument("--points-scale", type=float, default=1.0, help="batch/serve: scale of the hull point counts")
     p.add_argument("--screen-scale", type=float, default=1.0, help="batch/serve: scale of the screen edges")
@@ -159,10 +161,9 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(small: bool, name: str = "cornell4d", precision: str = "float") -> dict:
-    """The reference's own painter (create_painter, BPT, float, spectrum),
-    unmodified, on the host cores: one pass over a bounded slab of the
-    workload's screen."""
+def cpu_baseline(small: bool, name: str = "cornell4d", precision: str = "float", integrator: str = "bpt") -> dict:
+    """The reference's own painter (create_painter with the integrator),
+    unmodified, on the host cores: one pass over the workload's screen."""
     from math_b200 import scenes
     from oracle import oracle
 
@@ -174,6 +175,7 @@ def cpu_baseline(small: bool, name: str = "cornell4d", precision: str = "float")
     desc = scene_desc(small, None, name)
     slab = desc["projector"]["size"]
     s = oracle.Scene(desc, precision, w["spectrum"])
+    s.set_integrator(integrator)
     cores = os.cpu_count() or 1
     stats, _ = s.paint(w["spp"], w["max_depth"], passes=1, threads=cores)
     value = stats["sample_count"] / stats["pass_duration"]
@@ -210,6 +212,7 @@ def run_reference(args, rank: int):
     desc = scene_desc(args.small, args.screen, args.workload if args.workload in WORKLOADS else "cornell4d")
     slab = desc["projector"]["size"]
     s = oracle.Scene(desc, args.precision, w["spectrum"])
+    s.set_integrator(args.integrator)
     cores = os.cpu_count() or 1
     for _ in range(args.warmup):
         s.paint(w["spp"], w["max_depth"], passes=1, threads=cores)
@@ -222,13 +225,13 @@ def run_reference(args, rank: int):
     value = samples / seconds
     sample = f"{args.steps} passes over the whole {'x'.join(map(str, slab))} screen"
     print(json.dumps({
-        "metric": "bpt_paths_per_second", "value": value, "unit": "paths/s", "impl": "reference",
+        "metric": f"{args.integrator}_paths_per_second", "value": value, "unit": "paths/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000 * seconds / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if args.precision == "double" else "f32",
         "data": "synthetic (seeded generators)",
         "config": {"workload": f"{args.workload} {w['label']}, {w['spp']} spp, depth {w['max_depth']}",
-                   "screen": slab, "precision": args.precision},
+                   "screen": slab, "precision": args.precision, "integrator": args.integrator},
         "cpu_baseline": {"value": value, "unit": "paths/s", "cores": cores, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": value, "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -270,7 +273,7 @@ def run_nbpt(args, rank: int, world: int, local: int):
     build_s = time.perf_counter() - t0
     # every rank renders its own pass sequence of the whole screen
     # (independent samples: weak scaling, no data-path collective)
-    painter = scene.painter(w["spp"], w["max_depth"], seed=1 + rank)
+    painter = scene.painter(w["spp"], w["max_depth"], seed=1 + rank, integrator=args.integrator)
     stream = torch.cuda.ExternalStream(painter_stream(painter))
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
 
@@ -322,7 +325,7 @@ def run_nbpt(args, rank: int, world: int, local: int):
     for _ in range(args.steps):
         e0 = time.perf_counter()
         job_scene = P.Scene(desc, args.precision, spectrum)
-        job = job_scene.painter(w["spp"], w["max_depth"], seed=1 + rank)
+        job = job_scene.painter(w["spp"], w["max_depth"], seed=1 + rank, integrator=args.integrator)
         job.run(1)
         P._check(P.lib().nbpt_painter_images(job.h, P._p(rgb, P._F), P._p(rgba, P._F)))
         e2e_times.append(time.perf_counter() - e0)
@@ -353,9 +356,10 @@ def run_nbpt(args, rank: int, world: int, local: int):
                 "frac": (achieved / peak) if achieved else None,
                 "traffic": (TRAFFIC_PER_PATH[args.precision] * paths_per_step
                             if args.precision in TRAFFIC_PER_PATH and args.workload == "cornell4d"
-                            and not args.small and args.screen is None else None),
+                            and args.integrator == "bpt" and not args.small and args.screen is None else None),
                 "traffic_source": "profiles/path_kernels_cornell4d_32.md (per path, scaled to one pass)",
-                "kernel": "path kernels (walk, connect, light, replay)",
+                "kernel": ("path kernels (walk, connect, light, replay)" if args.integrator == "bpt"
+                           else "pt_paths_kernel"),
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 "algorithmic_bytes_per_path": algorithmic / (paths_per_step * args.steps),
                 "node_visits_per_path": nodes / (paths_per_step * args.steps),
@@ -365,9 +369,9 @@ def run_nbpt(args, rank: int, world: int, local: int):
 
     if rank == 0:
         cpu = (None if (args.no_cpu_baseline or world > 1)
-               else cpu_baseline(args.small, args.workload, args.precision))
+               else cpu_baseline(args.small, args.workload, args.precision, args.integrator))
         line = {
-            "metric": "bpt_paths_per_second", "value": value, "unit": "paths/s", "n_gpus": world,
+            "metric": f"{args.integrator}_paths_per_second", "value": value, "unit": "paths/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if args.precision == "float" else "f64",
@@ -376,6 +380,7 @@ def run_nbpt(args, rank: int, world: int, local: int):
                                    f"({painter.spp} rendered), depth {w['max_depth']}",
                        "screen": desc["projector"]["size"],
                        "paths_per_step": paths_per_step, "precision": args.precision,
+                       "integrator": args.integrator,
                        "l2": "flushed (256 MiB write) between timed steps",
                        "scene_build_s": build_s},
             "e2e": {"value": e2e, "unit": "paths/s", "h2d_bytes_per_step": int(h2d),

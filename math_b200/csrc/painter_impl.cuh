@@ -1529,6 +1529,7 @@ class PainterT final : public Painter
         DeviceArray<unsigned> task_count_;
         DeviceArray<unsigned> next_path_;
         DeviceArray<Arrival<N, T>> arrivals_;
+        DeviceArray<PtEstimate> pt_estimates_;
         int connect_blocks_ = 0;
         long long launches_ = 0;
         Statistics statistics_{};
@@ -1570,7 +1571,7 @@ public:
                 const long long per_sample = (N - 1) * sizeof(T) + C * 4 + 4 + 1;
                 const long long per_pixel = sizeof(PixelState<C>) + 12 + 16;
                 const long long chunk = integrator == Integrator::PT
-                                                ? 4 // the path counter
+                                                ? 4 // the path counter; the direct-lighting records are small
                                                 : chunk_pixels(pixels, spp, max_depth, integrator) * spp *
                                                           chunk_path_bytes(max_depth);
                 return (strata + 1) * sizeof(T) + samples * per_sample + pixels * per_pixel + sizeof(PathStats) +
@@ -1639,6 +1640,9 @@ public:
                 {
                         next_path_.allocate(1);
                         connect_blocks_ = sms * NBPT_PT_MIN_BLOCKS;
+                        // direct-lighting records: 2 per light per thread
+                        pt_estimates_.allocate(std::max(1LL, static_cast<long long>(connect_blocks_) * 128 * 2 *
+                                                                     scene_->device().light_count));
                 }
                 else
                 {
@@ -1684,7 +1688,7 @@ public:
                                         valid_.bytes() + state_.bytes() + stats_.bytes() + rgb_.bytes() +
                                         rgba_.bytes() + vertices_.bytes() + rng_.bytes() + tape_.bytes() +
                                         tasks_.bytes() + task_count_.bytes() + arrivals_.bytes() +
-                                        next_path_.bytes();
+                                        next_path_.bytes() + pt_estimates_.bytes();
                 return static_cast<long long>(own) + scene_->device_bytes();
         }
 
@@ -1716,9 +1720,11 @@ public:
                                         NBPT_CUDA(cudaMemsetAsync(next_path_.get(), 0, sizeof(unsigned), stream_));
                                         pt_paths_kernel<N, T, C>
                                                 <<<std::min<long long>(connect_blocks_, blocks_for(n, 128)), 128, 0, stream_>>>(
-                                                        scene, b, e, spp_, seed_, pass, points_.get() + b * spp_ * (N - 1),
-                                                        colors_.get() + b * spp_ * C, lum_.get() + b * spp_,
-                                                        valid_.get() + b * spp_, next_path_.get(), stats_.get(),
+                                                        scene_->device_channel_0(), scene_->device_materials(),
+                                                        scene_->device_lights(), b, e, spp_, seed_, pass,
+                                                        points_.get() + b * spp_ * (N - 1), colors_.get() + b * spp_ * C,
+                                                        lum_.get() + b * spp_, valid_.get() + b * spp_,
+                                                        pt_estimates_.get(), next_path_.get(), stats_.get(),
                                                         scene_->cie() + 64);
                                         NBPT_CUDA(cudaGetLastError());
                                         launches += 1;

@@ -5,8 +5,8 @@
 // src/painter/integrators/com/surface_sample.cpp, with the parallelotope and
 // ball lights' arrive_info (src/painter/lights/parallelotope_light.cpp:92-115,
 // ball_light.cpp:90-113).  Russian roulette weighs the path by the
-// luminance of all its colour channels, so a path carries its full colour
-// (one thread per path; no channel-0 tape as for BPT).
+// luminance of all its colour channels, so each thread carries its path's
+// full throughput (beta) while it traces.
 #pragma once
 
 #include "bpt.cuh"
@@ -38,18 +38,42 @@ NBPT_HD T power_heuristic(const T f_pdf, const T g_pdf)
 // of the reference gets near it).
 inline constexpr int PT_MAX_BOUNCES = 100000;
 
-template <int N, typename T, int C>
+// One direct-lighting estimate of a bounce, colour-free: its channel c is
+// (brdf_c * radiance_c) * scale, brdf_c from the terms (0 when the BRDF's
+// own checks fail) and radiance_c the light's.
+struct PtEstimate final
+{
+        BrdfTerms terms;
+        float scale;
+        int light;
+        int zero;
+};
+
+// The sampled continuation of a bounce (com::surface_sample): beta_c is
+// multiplied by brdf_c * scale.
+template <int N, typename T>
+struct PtContinuation final
+{
+        BrdfTerms terms;
+        float scale;
+        Vec<N, T> l;
+};
+
+// Tracing and sampling run on the channel-0 view of the scene (the
+// reference's Color::is_black() and usable() look at channel 0 only, so
+// every decision is the same); the colour arithmetic runs per channel from
+// the recorded BRDF terms, in the reference's operation order.
+template <int N, typename T>
 struct Pt final
 {
-        const SceneQueries<N, T, C>& q;
-        const DeviceScene<N, T, C>& s;
+        const SceneQueries<N, T, 1>& q;
+        const DeviceScene<N, T, 1>& s;
         Pcg& g;
-        const float* cie_y;
-        Bpt<N, T, C> b; // light samples and visibility
+        Bpt<N, T, 1> b; // light samples and visibility
 
         // LightSource::arrive_info: the light seen from `point` in direction
         // `l`; false when not usable.
-        __device__ bool arrive_info(const Light<N, T, C>& light, const Vec<N, T>& point, const Vec<N, T>& l, T& pdf,
+        __device__ bool arrive_info(const Light<N, T, 1>& light, const Vec<N, T>& point, const Vec<N, T>& l, T& pdf,
                                     T& distance) const
         {
                 if (!(dot(light.normal, point - light.org) > 0))
@@ -91,11 +115,12 @@ struct Pt final
 
         // sample_light_with_mis (direct_lighting.cpp:59-99); the lights here
         // are area lights (is_delta() false)
-        NBPT_CALL bool light_with_mis(const Light<N, T, C>& light, const Hit<N, T>& surface, const Vec<N, T>& v,
-                                      const Normals<N, T>& normals, Color<C>& out) const
+        NBPT_CALL bool light_with_mis(const int k, const Hit<N, T>& surface, const Vec<N, T>& v,
+                                      const Normals<N, T>& normals, PtEstimate& out) const
         {
+                const Light<N, T, 1>& light = s.lights[k];
                 const Vec<N, T>& n = normals.shading;
-                const ArriveSample<N, T, C> sample = b.arrive_sample(light, surface.point);
+                const ArriveSample<N, T, 1> sample = b.arrive_sample(light, surface.point);
                 if (!sample.usable())
                 {
                         return false;
@@ -110,22 +135,30 @@ struct Pt final
                 {
                         return false;
                 }
-                const Material<T, C>& m = s.materials[q.material(surface)];
-                const Color<C> brdf = brdf_f(s.shading, m.roughness, m.f0, m.rho_ss, n, v, l);
+                const Material<T, 1>& m = s.materials[q.material(surface)];
+                // brdf::f's own checks (brdf.h:146-171), then its terms
+                out.zero = (dot(n, v) <= 0 || dot(n, l) <= 0) ? 1 : 0;
+                if (!out.zero)
+                {
+                        out.terms = brdf_terms<N>(s.shading, m.roughness, n, v, l);
+                }
                 const T pdf = brdf_pdf(s.shading, m.roughness, n, v, l);
                 const T weight = power_heuristic(sample.pdf, pdf);
-                out = brdf * sample.radiance * static_cast<float>(weight * n_l / sample.pdf);
+                out.scale = static_cast<float>(weight * n_l / sample.pdf);
+                out.light = k;
                 return true;
         }
 
         // sample_surface_with_mis (direct_lighting.cpp:101-147); no shape
         // here is specular
-        NBPT_CALL bool surface_with_mis(const Light<N, T, C>& light, const Hit<N, T>& surface, const Vec<N, T>& v,
-                                        const Normals<N, T>& normals, Color<C>& out) const
+        NBPT_CALL bool surface_with_mis(const int k, const Hit<N, T>& surface, const Vec<N, T>& v,
+                                        const Normals<N, T>& normals, PtEstimate& out) const
         {
+                const Light<N, T, 1>& light = s.lights[k];
                 const Vec<N, T>& n = normals.shading;
-                const Material<T, C>& m = s.materials[q.material(surface)];
-                const BrdfSample<N, C, T> sample = brdf_sample<N>(g, s.shading, m.roughness, m.f0, m.rho_ss, n, v);
+                const Material<T, 1>& m = s.materials[q.material(surface)];
+                const BrdfSample<N, 1, T> sample =
+                        brdf_sample<N>(g, s.shading, m.roughness, m.f0, m.rho_ss, n, v, &out.terms);
                 if (!(sample.pdf > 0 && !sample.brdf.is_black()))
                 {
                         return false;
@@ -147,81 +180,20 @@ struct Pt final
                         return false;
                 }
                 const T weight = power_heuristic(sample.pdf, light_pdf);
-                out = sample.brdf * light.radiance * static_cast<float>(weight * n_l / sample.pdf);
+                out.scale = static_cast<float>(weight * n_l / sample.pdf);
+                out.light = k;
+                out.zero = 0;
                 return true;
         }
 
-        // terminate (pt.cpp:43-66)
-        __device__ bool terminate(const int depth, Color<C>& beta) const
+        // com::surface_sample (surface_sample.cpp:31-70)
+        NBPT_CALL bool continuation(const Hit<N, T>& surface, const Vec<N, T>& v, const Normals<N, T>& normals,
+                                    PtContinuation<N, T>& out) const
         {
-                if (depth < 4)
-                {
-                        return false;
-                }
-                const float lum = luminance(beta, cie_y);
-                if (!(lum > 0))
-                {
-                        return true;
-                }
-                constexpr float MIN = 0.05f;
-                constexpr float MAX = 0.95f;
-                const float x = 1 - lum;
-                const float p = (x < MIN) ? MIN : ((MAX < x) ? MAX : x);
-                if (bernoulli(g, p))
-                {
-                        return true;
-                }
-                const float k = 1 - p;
-#pragma unroll 8
-                for (int i = 0; i < C; ++i)
-                {
-                        beta.c[i] /= k;
-                }
-                return false;
-        }
-
-        // one bounce (pt.cpp:68-111): false when the path ends
-        NBPT_CALL bool step(const int depth, Ray<N, T>& ray, Hit<N, T>& surface, Normals<N, T>& normals,
-                            Color<C>& color, Color<C>& beta) const
-        {
-                const Vec<N, T> v = -ray.dir;
-                if (dot(normals.shading, v) <= 0)
-                {
-                        return false;
-                }
-
-                // direct_lighting (direct_lighting.cpp:150-167): both
-                // estimates of every light, summed in that order
-                bool lit = false;
-                Color<C> direct;
-                for (int k = 0; k < s.light_count; ++k)
-                {
-                        const Light<N, T, C>& light = s.lights[k];
-                        Color<C> c;
-                        if (light_with_mis(light, surface, v, normals, c))
-                        {
-                                direct = lit ? direct + c : c;
-                                lit = true;
-                        }
-                        if (surface_with_mis(light, surface, v, normals, c))
-                        {
-                                direct = lit ? direct + c : c;
-                                lit = true;
-                        }
-                }
-                if (lit)
-                {
-#pragma unroll 8
-                        for (int i = 0; i < C; ++i)
-                        {
-                                color.c[i] += beta.c[i] * direct.c[i];
-                        }
-                }
-
-                // com::surface_sample (surface_sample.cpp:31-70)
                 const Vec<N, T>& n = normals.shading;
-                const Material<T, C>& m = s.materials[q.material(surface)];
-                const BrdfSample<N, C, T> sample = brdf_sample<N>(g, s.shading, m.roughness, m.f0, m.rho_ss, n, v);
+                const Material<T, 1>& m = s.materials[q.material(surface)];
+                const BrdfSample<N, 1, T> sample =
+                        brdf_sample<N>(g, s.shading, m.roughness, m.f0, m.rho_ss, n, v, &out.terms);
                 if (!(sample.pdf > 0 && !sample.brdf.is_black()))
                 {
                         return false;
@@ -235,65 +207,36 @@ struct Pt final
                 {
                         return false;
                 }
-                beta *= sample.brdf * static_cast<float>(n_l / sample.pdf);
-
-                if (terminate(depth, beta))
-                {
-                        return false;
-                }
-
-                ray = Ray<N, T>::make(surface.point, sample.l);
-                const Vec<N, T> gn = normals.geometric;
-                surface = q.scene_intersect(&gn, ray, normals);
-                return static_cast<bool>(surface);
-        }
-
-        // pt() (pt.cpp:138-170): false for a background sample (nullopt)
-        __device__ bool run(const Ray<N, T>& primary, Color<C>& out) const
-        {
-                Ray<N, T> ray = primary;
-                Normals<N, T> normals;
-                Hit<N, T> surface = q.scene_intersect(nullptr, ray, normals);
-                if (!surface)
-                {
-                        return false;
-                }
-                Color<C> color = Color<C>::filled(0);
-                const int li = q.light(surface);
-                if (li >= 0)
-                {
-                        // LightSource::leave_radiance(-dir)
-                        const Light<N, T, C>& light = s.lights[li];
-                        if (dot(-ray.dir, light.normal) > 0)
-                        {
-                                color = light.radiance;
-                        }
-                }
-                Color<C> beta = Color<C>::filled(1);
-                for (int depth = 0; depth < PT_MAX_BOUNCES; ++depth)
-                {
-                        if (!step(depth, ray, surface, normals, color, beta))
-                        {
-                                break;
-                        }
-                }
-                out = color;
+                out.scale = static_cast<float>(n_l / sample.pdf);
+                out.l = sample.l;
                 return true;
         }
 };
+
+template <typename T, int C>
+__device__ float pt_brdf_channel(const BrdfTerms& t, const int zero, const Material<T, C>& m, const int c,
+                                 const ShadingConstants<T>& sc)
+{
+        return zero ? 0.0f : brdf_channel(t, m.f0.c[c], m.rho_ss.c[c], sc.fresnel_a, sc.fresnel_b);
+}
 
 #ifndef NBPT_PT_MIN_BLOCKS
 #define NBPT_PT_MIN_BLOCKS 4
 #endif
 
-// One path of the PT integrator per thread, persistent: the threads take
-// paths from a shared counter.  The sample points, the path's ray and its
-// random stream are those of the BPT kernels (the same stratified points,
-// seed_seq{seed, pass, pixel, sample + 1}); the reference's painter draws
-// them the same way whichever integrator it runs (painting.cpp:225-257).
+// One path of the PT integrator per thread (pt.cpp:113-170), persistent: the
+// threads take paths from a shared counter.  The sample points, the path's
+// ray and its random stream are those of the BPT kernels (the same
+// stratified points, seed_seq{seed, pass, pixel, sample + 1}); the
+// reference's painter draws them the same way whichever integrator it runs
+// (painting.cpp:225-257).  beta stays in registers; the colour too for RGB,
+// while a spectrum accumulates in the output row.  `estimates` holds
+// 2 * light_count records per thread of the grid.
 template <int N, typename T, int C>
 __global__ void __launch_bounds__(128, NBPT_PT_MIN_BLOCKS) pt_paths_kernel(
-        const DeviceScene<N, T, C> scene,
+        const DeviceScene<N, T, 1> scene,
+        const Material<T, C>* __restrict__ materials,
+        const Light<N, T, C>* __restrict__ lights,
         const long long begin,
         const long long end,
         const int spp,
@@ -303,11 +246,16 @@ __global__ void __launch_bounds__(128, NBPT_PT_MIN_BLOCKS) pt_paths_kernel(
         float* __restrict__ colors,
         float* __restrict__ lum,
         unsigned char* __restrict__ valid,
+        PtEstimate* __restrict__ estimates,
         unsigned* __restrict__ next_path,
         PathStats* __restrict__ stats,
         const float* __restrict__ cie_y)
 {
+        constexpr bool IN_REGISTERS = C <= 4;
         const long long paths = (end - begin) * spp;
+        PtEstimate* const est =
+                estimates + (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) * 2 * scene.light_count;
+        const ShadingConstants<T>& sc = scene.shading;
         QueryCounters counters{0, 0, 0, 0};
         while (true)
         {
@@ -332,23 +280,157 @@ __global__ void __launch_bounds__(128, NBPT_PT_MIN_BLOCKS) pt_paths_kernel(
                                 rest = q;
                         }
                 }
-                const Ray<N, T> ray = scene.projector.ray(point);
+                Ray<N, T> ray = scene.projector.ray(point);
 
                 const std::uint32_t words[4] = {seed, pass, static_cast<std::uint32_t>(p),
                                                 static_cast<std::uint32_t>(sample + 1)};
                 Pcg g = seed_seq_pcg(words, 4);
-                const SceneQueries<N, T, C> q{scene, counters};
-                const Pt<N, T, C> pt{q, scene, g, cie_y, Bpt<N, T, C>{q, scene, g, 0, nullptr, nullptr}};
-                Color<C> color;
-                const bool has = pt.run(ray, color);
+                const SceneQueries<N, T, 1> q{scene, counters};
+                const Pt<N, T> pt{q, scene, g, Bpt<N, T, 1>{q, scene, g, 0, nullptr, nullptr}};
+
                 float* const out = colors + i * C;
-#pragma unroll 8
-                for (int k = 0; k < C; ++k)
+                Normals<N, T> normals;
+                Hit<N, T> surface = q.scene_intersect(nullptr, ray, normals);
+                if (!surface)
                 {
-                        out[k] = has ? color.c[k] : 0.0f;
+#pragma unroll 8
+                        for (int c = 0; c < C; ++c)
+                        {
+                                out[c] = 0.0f;
+                        }
+                        lum[i] = 0.0f;
+                        valid[i] = 0;
+                        continue;
                 }
-                lum[i] = has ? luminance(color, cie_y) : 0.0f;
-                valid[i] = has ? 1 : 0;
+
+                // the emitted radiance seen by the primary ray
+                // (LightSource::leave_radiance(-dir))
+                Color<IN_REGISTERS ? C : 1> reg;
+                {
+                        const int li = q.light(surface);
+                        const bool emits = li >= 0 && dot(-ray.dir, scene.lights[li].normal) > 0;
+#pragma unroll 8
+                        for (int c = 0; c < C; ++c)
+                        {
+                                const float e = emits ? lights[li].radiance.c[c] : 0.0f;
+                                if constexpr (IN_REGISTERS)
+                                {
+                                        reg.c[c] = e;
+                                }
+                                else
+                                {
+                                        out[c] = e;
+                                }
+                        }
+                }
+                Color<C> beta = Color<C>::filled(1);
+
+                for (int depth = 0; depth < PT_MAX_BOUNCES; ++depth)
+                {
+                        // one bounce (pt.cpp:68-111)
+                        const Vec<N, T> v = -ray.dir;
+                        if (dot(normals.shading, v) <= 0)
+                        {
+                                break;
+                        }
+
+                        // direct_lighting (direct_lighting.cpp:150-167): both
+                        // estimates of every light, summed in that order
+                        int count = 0;
+                        for (int k = 0; k < scene.light_count; ++k)
+                        {
+                                count += pt.light_with_mis(k, surface, v, normals, est[count]) ? 1 : 0;
+                                count += pt.surface_with_mis(k, surface, v, normals, est[count]) ? 1 : 0;
+                        }
+                        const Material<T, C>& m = materials[q.material(surface)];
+                        if (count > 0)
+                        {
+#pragma unroll 4
+                                for (int c = 0; c < C; ++c)
+                                {
+                                        float d = 0.0f;
+                                        for (int e = 0; e < count; ++e)
+                                        {
+                                                const PtEstimate& r = est[e];
+                                                const float brdf = pt_brdf_channel(r.terms, r.zero, m, c, sc);
+                                                const float x = (brdf * lights[r.light].radiance.c[c]) * r.scale;
+                                                d = e == 0 ? x : d + x;
+                                        }
+                                        if constexpr (IN_REGISTERS)
+                                        {
+                                                reg.c[c] += beta.c[c] * d;
+                                        }
+                                        else
+                                        {
+                                                out[c] += beta.c[c] * d;
+                                        }
+                                }
+                        }
+
+                        PtContinuation<N, T> next;
+                        if (!pt.continuation(surface, v, normals, next))
+                        {
+                                break;
+                        }
+#pragma unroll 8
+                        for (int c = 0; c < C; ++c)
+                        {
+                                beta.c[c] *= pt_brdf_channel(next.terms, 0, m, c, sc) * next.scale;
+                        }
+
+                        // terminate (pt.cpp:43-66)
+                        if (depth >= 4)
+                        {
+                                const float y = luminance(beta, cie_y);
+                                if (!(y > 0))
+                                {
+                                        break;
+                                }
+                                constexpr float MIN = 0.05f;
+                                constexpr float MAX = 0.95f;
+                                const float x = 1 - y;
+                                const float rr = (x < MIN) ? MIN : ((MAX < x) ? MAX : x);
+                                if (bernoulli(g, rr))
+                                {
+                                        break;
+                                }
+                                const float k = 1 - rr;
+#pragma unroll 8
+                                for (int c = 0; c < C; ++c)
+                                {
+                                        beta.c[c] /= k;
+                                }
+                        }
+
+                        ray = Ray<N, T>::make(surface.point, next.l);
+                        const Vec<N, T> gn = normals.geometric;
+                        surface = q.scene_intersect(&gn, ray, normals);
+                        if (!surface)
+                        {
+                                break;
+                        }
+                }
+
+                if constexpr (IN_REGISTERS)
+                {
+#pragma unroll
+                        for (int c = 0; c < C; ++c)
+                        {
+                                out[c] = reg.c[c];
+                        }
+                        lum[i] = luminance(reg, cie_y);
+                }
+                else
+                {
+                        Color<C> final_color;
+#pragma unroll 8
+                        for (int c = 0; c < C; ++c)
+                        {
+                                final_color.c[c] = out[c];
+                        }
+                        lum[i] = luminance(final_color, cie_y);
+                }
+                valid[i] = 1;
         }
         add_counters(counters, stats);
 }
