@@ -645,20 +645,46 @@ public:
                         throw std::runtime_error("No facets for facet object");
                 }
                 MeshObjectHost o;
-                o.points.assign(points, points + point_count * N);
-                o.facets.assign(facets, facets + facet_count * N);
-                for (const int i : o.facets)
+                // only the points the facets use, numbered in the order the
+                // facets first reach them (model/mesh/optimize.cpp:48-62,
+                // 168-205, which the reference applies to every mesh object)
+                std::vector<int> map(point_count, -1);
+                int used = 0;
+                o.facets.resize(facet_count * N);
+                for (long long k = 0; k < facet_count * N; ++k)
                 {
+                        const int i = facets[k];
                         if (i < 0 || i >= point_count)
                         {
                                 throw std::runtime_error("facet vertex index out of range");
                         }
+                        if (map[i] < 0)
+                        {
+                                map[i] = used++;
+                        }
+                        o.facets[k] = map[i];
                 }
-                std::copy(matrix, matrix + (N + 1) * (N + 1), o.matrix.begin());
+                o.points.resize(static_cast<std::size_t>(used) * N);
                 if (normals)
                 {
-                        o.normals.assign(normals, normals + point_count * N);
+                        o.normals.resize(static_cast<std::size_t>(used) * N);
                 }
+                for (long long i = 0; i < point_count; ++i)
+                {
+                        if (map[i] < 0)
+                        {
+                                continue;
+                        }
+                        for (int d = 0; d < N; ++d)
+                        {
+                                o.points[static_cast<std::size_t>(map[i]) * N + d] = points[i * N + d];
+                                if (normals)
+                                {
+                                        o.normals[static_cast<std::size_t>(map[i]) * N + d] = normals[i * N + d];
+                                }
+                        }
+                }
+                std::copy(matrix, matrix + (N + 1) * (N + 1), o.matrix.begin());
                 o.metalness = metalness;
                 o.roughness = roughness;
                 o.alpha = alpha;
@@ -691,19 +717,28 @@ public:
                                 o.normals = vertex_normals<N>(o.points, o.facets);
                         }
                         // vertices: M * (v, 1)  (numerical/transform.h:83-119)
-                        for (std::size_t v = 0; v < vcount; ++v)
-                        {
-                                for (int r = 0; r < N; ++r)
+                        const std::size_t vbase = mesh.vertices.size();
+                        mesh.vertices.resize(vbase + vcount * N);
+                        parallel_ranges(
+                                vcount,
+                                [&](const std::size_t begin, const std::size_t end)
                                 {
-                                        T x = static_cast<T>(o.matrix[r * (N + 1) + 0]) * static_cast<T>(o.points[v * N + 0]);
-                                        for (int c = 1; c < N; ++c)
+                                        for (std::size_t v = begin; v < end; ++v)
                                         {
-                                                x += static_cast<T>(o.matrix[r * (N + 1) + c]) * static_cast<T>(o.points[v * N + c]);
+                                                for (int r = 0; r < N; ++r)
+                                                {
+                                                        T x = static_cast<T>(o.matrix[r * (N + 1) + 0]) *
+                                                              static_cast<T>(o.points[v * N + 0]);
+                                                        for (int c = 1; c < N; ++c)
+                                                        {
+                                                                x += static_cast<T>(o.matrix[r * (N + 1) + c]) *
+                                                                     static_cast<T>(o.points[v * N + c]);
+                                                        }
+                                                        x += static_cast<T>(o.matrix[r * (N + 1) + N]);
+                                                        mesh.vertices[vbase + v * N + r] = x;
+                                                }
                                         }
-                                        x += static_cast<T>(o.matrix[r * (N + 1) + N]);
-                                        mesh.vertices.push_back(x);
-                                }
-                        }
+                                });
                         // normals: inverse transpose of the linear part
                         std::array<T, N * N> lin;
                         for (int r = 0; r < N; ++r)
@@ -714,19 +749,26 @@ public:
                                 }
                         }
                         const std::array<T, N * N> inv = inverse<N, T>(lin);
-                        for (std::size_t v = 0; v < vcount; ++v)
-                        {
-                                for (int r = 0; r < N; ++r)
+                        const std::size_t nbase = mesh.normals.size();
+                        mesh.normals.resize(nbase + vcount * N);
+                        parallel_ranges(
+                                vcount,
+                                [&](const std::size_t begin, const std::size_t end)
                                 {
-                                        // row r of the transpose = column r of the inverse
-                                        T x = inv[0 * N + r] * static_cast<T>(o.normals[v * N + 0]);
-                                        for (int c = 1; c < N; ++c)
+                                        for (std::size_t v = begin; v < end; ++v)
                                         {
-                                                x += inv[c * N + r] * static_cast<T>(o.normals[v * N + c]);
+                                                for (int r = 0; r < N; ++r)
+                                                {
+                                                        // row r of the transpose = column r of the inverse
+                                                        T x = inv[0 * N + r] * static_cast<T>(o.normals[v * N + 0]);
+                                                        for (int c = 1; c < N; ++c)
+                                                        {
+                                                                x += inv[c * N + r] * static_cast<T>(o.normals[v * N + c]);
+                                                        }
+                                                        mesh.normals[nbase + v * N + r] = x;
+                                                }
                                         }
-                                        mesh.normals.push_back(x);
-                                }
-                        }
+                                });
                         const int material = add_material(
                                 [&]
                                 {
