@@ -322,6 +322,7 @@ def run_nbpt(args, rank: int, world: int, local: int):
     torch.cuda.synchronize()
     e2e_times = []
     h2d = 0
+    build = {}
     for _ in range(args.steps):
         e0 = time.perf_counter()
         job_scene = P.Scene(desc, args.precision, spectrum)
@@ -330,6 +331,7 @@ def run_nbpt(args, rank: int, world: int, local: int):
         P._check(P.lib().nbpt_painter_images(job.h, P._p(rgb, P._F), P._p(rgba, P._F)))
         e2e_times.append(time.perf_counter() - e0)
         h2d = job_scene.upload_bytes()
+        build = job_scene.build_seconds()
         job.close()
         job_scene.close()
     e2e_s = slowest_rank(float(np.sum(e2e_times)), world, "cuda")
@@ -386,6 +388,7 @@ def run_nbpt(args, rank: int, world: int, local: int):
             "e2e": {"value": e2e, "unit": "paths/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(rgb.nbytes + rgba.nbytes),
                     "seconds_per_step": e2e_s / args.steps,
+                    "scene_build_seconds": build,
                     "note": "every step a whole job through the C ABI: scene from host arrays (copies, BVH "
                             "build, facet setup), one pass, RGB and RGBA images read back to host memory"},
             "resident": {"value": paths_per_step * args.steps / resident_s, "unit": "paths/s",

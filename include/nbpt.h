@@ -150,6 +150,11 @@ int nbpt_scene_actual_spp(const nbpt_scene* scene, int samples_per_pixel);
 long long nbpt_scene_device_bytes(const nbpt_scene* scene);
 /* bytes finalize copied from host to device (shapes, BVH, vertices, facets) */
 long long nbpt_scene_upload_bytes(const nbpt_scene* scene);
+/* host seconds of the scene build, as the reference logs its mesh and BVH
+ * build times (src/painter/shapes/mesh.cpp:190-209): seconds[0] mesh
+ * ingestion, [1] BVH builds, [2] the rest of nbpt_scene_finalize (device
+ * uploads, facet setup on the GPU), [3] the total */
+int nbpt_scene_build_seconds(const nbpt_scene* scene, double* seconds);
 
 /* ---- painter (painter::create_painter with Integrator::BPT) ---- */
 

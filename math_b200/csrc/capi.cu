@@ -562,6 +562,20 @@ long long nbpt_scene_upload_bytes(const nbpt_scene* scene)
         return r;
 }
 
+int nbpt_scene_build_seconds(const nbpt_scene* scene, double* seconds)
+{
+        return guarded(
+                [&]
+                {
+                        if (!seconds)
+                        {
+                                throw std::runtime_error("null output");
+                        }
+                        scene_of(const_cast<nbpt_scene*>(scene)).build_seconds(seconds);
+                        return 0;
+                });
+}
+
 nbpt_painter* nbpt_painter_create(nbpt_scene* scene, const int samples_per_pixel, const int max_depth, const unsigned seed)
 {
         nbpt_painter* out = nullptr;

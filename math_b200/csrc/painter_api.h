@@ -76,6 +76,9 @@ public:
         virtual int actual_spp(int samples_per_pixel) const = 0;
         virtual long long device_bytes() const = 0;
         virtual long long upload_bytes() const = 0;
+        // host seconds of the build: [mesh ingestion, BVH builds, the rest of
+        // finalize (device uploads, facet setup), total]
+        virtual void build_seconds(double* out) const = 0;
 
         // max_depth bounds the BPT subpaths; the PT integrator ends its paths
         // by Russian roulette and ignores it

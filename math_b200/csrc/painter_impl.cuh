@@ -24,6 +24,7 @@
 
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -249,6 +250,28 @@ void parallel_ranges(const std::size_t count, const F& f)
         }
 }
 
+// Adds the seconds from its construction to its destruction to `total`.
+class Stopwatch final
+{
+        double& total_;
+        std::chrono::steady_clock::time_point start_;
+
+public:
+        explicit Stopwatch(double& total)
+                : total_(total),
+                  start_(std::chrono::steady_clock::now())
+        {
+        }
+
+        ~Stopwatch()
+        {
+                total_ += std::chrono::duration<double>(std::chrono::steady_clock::now() - start_).count();
+        }
+
+        Stopwatch(const Stopwatch&) = delete;
+        Stopwatch& operator=(const Stopwatch&) = delete;
+};
+
 // Vertex normals of a simplex mesh: per vertex, the facet normals around it
 // weighted by the facet's solid angle at the vertex (n = 3, 4) or 1
 // (n >= 5), oriented consistently and averaged
@@ -437,6 +460,11 @@ class SceneT final : public Scene
         std::vector<MeshShape<N, T>> mesh_records_;
         long long facet_total_ = 0;
         long long upload_bytes_ = 0;
+        // host seconds of the scene build: mesh ingestion (add_mesh,
+        // add_mesh_data), BVH builds, the rest of finalize
+        double ingest_seconds_ = 0;
+        double bvh_seconds_ = 0;
+        double finalize_seconds_ = 0;
         long long node_total_ = 0;
 
         DeviceScene<N, T, C> device_{};
@@ -698,6 +726,7 @@ public:
         int add_mesh() override
         {
                 check_open();
+                const Stopwatch watch(ingest_seconds_);
                 if (pending_.empty())
                 {
                         throw std::runtime_error("No objects to paint");
@@ -813,6 +842,7 @@ public:
                 const float* material_colors) override
         {
                 check_open();
+                const Stopwatch watch(ingest_seconds_);
                 if (facet_count <= 0)
                 {
                         throw std::runtime_error("No facets found in meshes");
@@ -1018,6 +1048,7 @@ public:
         void finalize() override
         {
                 check_open();
+                const Stopwatch watch(finalize_seconds_);
                 if (!has_projector_)
                 {
                         throw std::runtime_error("no projector");
@@ -1057,7 +1088,10 @@ public:
                 }
                 for (MeshHost& m : meshes_)
                 {
-                        m.bvh = host::build_facet_bvh<N, T>(m.vertices, m.facets);
+                        {
+                                const Stopwatch bvh_watch(bvh_seconds_);
+                                m.bvh = host::build_facet_bvh<N, T>(m.vertices, m.facets);
+                        }
                         m.facet_offset = static_cast<int>(all_facets.size() / N);
                         m.node_offset = static_cast<int>(nodes.size());
                         m.index_offset = static_cast<int>(indices.size());
@@ -1343,6 +1377,14 @@ public:
                         r *= k;
                 }
                 return r;
+        }
+
+        void build_seconds(double* out) const override
+        {
+                out[0] = ingest_seconds_;
+                out[1] = bvh_seconds_;
+                out[2] = finalize_seconds_ - bvh_seconds_;
+                out[3] = ingest_seconds_ + finalize_seconds_;
         }
 
         long long upload_bytes() const override

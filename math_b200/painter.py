@@ -86,6 +86,7 @@ SIGNATURES = [
     ("nbpt_scene_actual_spp", ctypes.c_int, [_P, ctypes.c_int]),
     ("nbpt_scene_device_bytes", ctypes.c_longlong, [_P]),
     ("nbpt_scene_upload_bytes", ctypes.c_longlong, [_P]),
+    ("nbpt_scene_build_seconds", ctypes.c_int, [_P, _D]),
     ("nbpt_painter_create", _P, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_uint]),
     ("nbpt_painter_create_integrator", _P, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint]),
     ("nbpt_painter_destroy", None, [_P]),
@@ -268,6 +269,13 @@ class Scene:
 
     def upload_bytes(self) -> int:
         return _check(lib().nbpt_scene_upload_bytes(self.h))
+
+    def build_seconds(self) -> dict:
+        """Host seconds of the build: mesh ingestion, BVH builds, the rest of
+        finalize (device uploads, facet setup) and the total."""
+        out = np.zeros(4)
+        _check(lib().nbpt_scene_build_seconds(self.h, _p(out, _D)))
+        return dict(zip(("ingest", "bvh", "upload", "total"), (float(x) for x in out)))
 
     def painter(self, samples_per_pixel: int, max_depth: int, seed: int = 1,
                 integrator: str = "bpt") -> "Painter":

@@ -268,3 +268,15 @@ def test_errors(painter):
     bad["lights"] = []
     with pytest.raises(painter.PainterError, match="No light sources"):
         painter.Scene(bad, "double", False)
+
+
+def test_build_seconds(painter):
+    """The scene reports where its build time went (mesh ingestion, BVH,
+    the rest of finalize); the parts add up to the total."""
+    desc = scenes.cornell_3d(size=(8, 8), subdivisions=2)
+    s = painter.Scene(desc, "float", False)
+    b = s.build_seconds()
+    assert set(b) == {"ingest", "bvh", "upload", "total"}
+    assert all(v >= 0 for v in b.values())
+    assert b["bvh"] > 0 and b["total"] > 0
+    assert abs(b["ingest"] + b["bvh"] + b["upload"] - b["total"]) < 1e-9
