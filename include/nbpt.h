@@ -140,6 +140,13 @@ int nbpt_scene_set_parallel_projector(
 /* background colour (only black is supported) */
 int nbpt_scene_set_background(nbpt_scene* scene, const float* rgb);
 
+/* Where nbpt_scene_finalize builds the mesh BVHs (geometry::accelerators::Bvh,
+ * src/geometry/accelerators/bvh.cpp:35-86): NBPT_BVH_DEVICE (the default) on
+ * the GPU, NBPT_BVH_HOST on the host threads; both give the reference's tree */
+#define NBPT_BVH_DEVICE 0
+#define NBPT_BVH_HOST 1
+int nbpt_scene_set_bvh_builder(nbpt_scene* scene, int builder);
+
 /* Builds the acceleration structures and uploads the scene to the GPU. */
 int nbpt_scene_finalize(nbpt_scene* scene);
 

@@ -562,6 +562,16 @@ long long nbpt_scene_upload_bytes(const nbpt_scene* scene)
         return r;
 }
 
+int nbpt_scene_set_bvh_builder(nbpt_scene* scene, const int builder)
+{
+        return guarded(
+                [&]
+                {
+                        scene_of(scene).set_bvh_builder(builder);
+                        return 0;
+                });
+}
+
 int nbpt_scene_build_seconds(const nbpt_scene* scene, double* seconds)
 {
         return guarded(

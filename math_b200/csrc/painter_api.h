@@ -70,6 +70,8 @@ public:
         virtual void set_parallel_projector(const double* org, const double* dir, const double* axes,
                                             double units_per_pixel, const int* size) = 0;
         virtual void set_background(const float* rgb) = 0;
+        // 0: mesh BVHs built on the GPU (the default), 1: on the host
+        virtual void set_bvh_builder(int builder) = 0;
         virtual void finalize() = 0;
 
         virtual long long pixel_count() const = 0;

@@ -12,6 +12,7 @@
 #pragma once
 
 #include "bvh_build.h"
+#include "bvh_device.cuh"
 #include "device_pool.h"
 #include "estimator.cuh"
 #include "host_math.h"
@@ -381,6 +382,147 @@ std::vector<float> vertex_normals(const std::vector<float>& points, const std::v
 
 // ---------------------------------------------------------------------------
 
+// Builds the BVH of `count` facets (global vertex indices `facets`, N per
+// facet, into `vertices`) on the GPU (bvh_device.cuh); returns the node
+// count.  nodes: depth-first records, interior offsets and leaf index slots
+// local to the mesh; indices: the facet of every leaf slot.
+template <int N, typename T>
+int build_device_bvh(
+        const double* vertices,
+        const int* facets,
+        const int count,
+        const double* uniform_sums,
+        const T interior_cost,
+        DeviceArray<BvhNode<N, T>>& nodes,
+        DeviceArray<std::uint32_t>& indices)
+{
+        using K = typename BvhKey<T>::K;
+        if (count <= 0)
+        {
+                throw std::runtime_error("No objects to build BVH");
+        }
+        const int task_capacity = count / (BVH_SMALL + 1) + 1;
+        const int chunk_capacity = count / BVH_CHUNK + task_capacity + 1;
+        DeviceArray<BvhObject<N, T>> objects;
+        objects.allocate(count);
+        DeviceArray<unsigned char> buckets;
+        buckets.allocate(count);
+        DeviceArray<int> first;
+        first.allocate(count);
+        DeviceArray<int> second;
+        second.allocate(count);
+        DeviceArray<BvhBuildNode<N, T>> leaves;
+        leaves.allocate(count);
+        DeviceArray<BvhBuildNode<N, T>> inner;
+        inner.allocate(count);
+        DeviceArray<int> leaf_list;
+        leaf_list.allocate(count);
+        DeviceArray<int> inner_list;
+        inner_list.allocate(count);
+        DeviceArray<BvhTask<N, T>> tasks[2];
+        DeviceArray<BvhChunk> chunks[2];
+        for (int i = 0; i < 2; ++i)
+        {
+                tasks[i].allocate(task_capacity);
+                chunks[i].allocate(chunk_capacity);
+        }
+        DeviceArray<int2> chunk_counts;
+        chunk_counts.allocate(chunk_capacity);
+        DeviceArray<int2> chunk_offsets;
+        chunk_offsets.allocate(chunk_capacity);
+        DeviceArray<BvhSmallTask<N, T>> small;
+        small.allocate(count);
+        DeviceArray<BvhCounters> counters;
+        counters.allocate(1);
+        DeviceArray<K> root_keys;
+        root_keys.allocate(2 * N);
+
+        NBPT_CUDA(cudaMemset(counters.get(), 0, sizeof(BvhCounters)));
+        NBPT_CUDA(cudaMemset(root_keys.get(), 0xff, N * sizeof(K)));
+        NBPT_CUDA(cudaMemset(root_keys.get() + N, 0, N * sizeof(K)));
+        bvh_objects_kernel<N, T><<<blocks_for(count, 256), 256>>>(vertices, facets, count, objects.get(), root_keys.get());
+        NBPT_CUDA(cudaGetLastError());
+        bvh_root_kernel<N, T><<<1, 1>>>(count, root_keys.get(), tasks[0].get(), chunks[0].get(), small.get(),
+                                          counters.get());
+        NBPT_CUDA(cudaGetLastError());
+        BvhCounters h{};
+        NBPT_CUDA(cudaMemcpy(&h, counters.get(), sizeof(h), cudaMemcpyDeviceToHost));
+        int cur = 0;
+        while (h.tasks > 0)
+        {
+                const int task_count = h.tasks;
+                const int chunk_count = h.chunks;
+                if (task_count > task_capacity || chunk_count > chunk_capacity)
+                {
+                        throw std::runtime_error("BVH build: level larger than its buffers");
+                }
+                BvhTask<N, T>* const t = tasks[cur].get();
+                const BvhChunk* const c = chunks[cur].get();
+                bvh_center_kernel<N, T><<<chunk_count, BVH_THREADS>>>(t, c, objects.get());
+                bvh_bin_kernel<N, T><<<chunk_count, BVH_THREADS>>>(t, c, objects.get(), buckets.get());
+                NBPT_CUDA(cudaMemset(counters.get(), 0, 2 * sizeof(int))); // next level: tasks, chunks
+                bvh_split_kernel<N, T><<<blocks_for(task_count, 128), 128>>>(
+                        t, task_count, uniform_sums, interior_cost, tasks[1 - cur].get(), chunks[1 - cur].get(),
+                        small.get(), leaves.get(), inner.get(), leaf_list.get(), inner_list.get(), counters.get());
+                bvh_misplaced_kernel<N, T><<<chunk_count, BVH_THREADS>>>(
+                        t, c, buckets.get(), chunk_counts.get(), nullptr, first.get(), second.get());
+                bvh_offsets_kernel<N, T><<<blocks_for(task_count, 128), 128>>>(
+                        t, task_count, chunk_counts.get(), chunk_offsets.get(), counters.get());
+                bvh_misplaced_kernel<N, T><<<chunk_count, BVH_THREADS>>>(
+                        t, c, buckets.get(), chunk_counts.get(), chunk_offsets.get(), first.get(), second.get());
+                bvh_swap_kernel<N, T><<<chunk_count, BVH_THREADS>>>(t, c, first.get(), second.get(), objects.get());
+                NBPT_CUDA(cudaGetLastError());
+                NBPT_CUDA(cudaMemcpy(&h, counters.get(), sizeof(h), cudaMemcpyDeviceToHost));
+                if (h.error)
+                {
+                        break;
+                }
+                cur = 1 - cur;
+        }
+        if (h.small > 0 && !h.error)
+        {
+                bvh_small_kernel<N, T><<<(h.small + 3) / 4, 128>>>(
+                        small.get(), h.small, uniform_sums, interior_cost, objects.get(), leaves.get(), inner.get(),
+                        leaf_list.get(), inner_list.get(), counters.get());
+                NBPT_CUDA(cudaGetLastError());
+                NBPT_CUDA(cudaMemcpy(&h, counters.get(), sizeof(h), cudaMemcpyDeviceToHost));
+        }
+        if (h.error == 2)
+        {
+                throw std::runtime_error("BVH leaf too large");
+        }
+        if (h.error)
+        {
+                throw std::runtime_error("BVH split produced an empty side");
+        }
+        bvh_sizes_kernel<N, T><<<blocks_for(h.leaves, 128), 128>>>(leaf_list.get(), h.leaves, leaves.get(), inner.get(),
+                                                                    counters.get());
+        NBPT_CUDA(cudaGetLastError());
+        NBPT_CUDA(cudaMemcpy(&h, counters.get(), sizeof(h), cudaMemcpyDeviceToHost));
+        if (h.root_size != h.leaves + h.inner)
+        {
+                throw std::runtime_error("BVH build: the tree does not reach every node");
+        }
+        bvh_preorder_kernel<N, T><<<blocks_for(h.leaves + h.inner, 128), 128>>>(
+                leaf_list.get(), h.leaves, inner_list.get(), h.inner, leaves.get(), inner.get());
+        NBPT_CUDA(cudaGetLastError());
+        const int node_count = h.leaves + h.inner;
+        nodes.allocate(node_count);
+        bvh_write_kernel<N, T><<<blocks_for(node_count, 128), 128>>>(
+                leaf_list.get(), h.leaves, inner_list.get(), h.inner, leaves.get(), inner.get(), nodes.get(),
+                counters.get());
+        NBPT_CUDA(cudaGetLastError());
+        indices.allocate(count);
+        bvh_indices_kernel<N, T><<<blocks_for(count, 256), 256>>>(objects.get(), count, indices.get());
+        NBPT_CUDA(cudaGetLastError());
+        NBPT_CUDA(cudaMemcpy(&h, counters.get(), sizeof(h), cudaMemcpyDeviceToHost));
+        if (h.error)
+        {
+                throw std::runtime_error("BVH build: a node outside the depth-first order");
+        }
+        return node_count;
+}
+
 template <int N, typename T, int C>
 class PainterT;
 
@@ -426,7 +568,7 @@ class SceneT final : public Scene
                 std::vector<T> normals;  // [V][N] or empty
                 std::vector<int> facets;
                 std::vector<int> facet_materials;
-                host::BuiltBvh<N, T> bvh;
+                int node_count = 0;
                 int facet_offset = 0;
                 int node_offset = 0;
                 int index_offset = 0;
@@ -444,6 +586,7 @@ class SceneT final : public Scene
         Projector<N, T> projector_{};
         bool has_projector_ = false;
         bool finalized_ = false;
+        int bvh_builder_ = 0; // 0: on the GPU, 1: on the host
 
         DeviceArray<FlatShape<N, T>> d_flat_;
         DeviceArray<SolidShape<N, T>> d_solid_;
@@ -1045,6 +1188,16 @@ public:
                 }
         }
 
+        void set_bvh_builder(const int builder) override
+        {
+                check_open();
+                if (builder != 0 && builder != 1)
+                {
+                        throw std::runtime_error("BVH builder must be 0 (GPU) or 1 (host)");
+                }
+                bvh_builder_ = builder;
+        }
+
         void finalize() override
         {
                 check_open();
@@ -1074,113 +1227,201 @@ public:
                         }
                 }
 
-                // meshes: BVH on the host, facet records on the GPU
-                std::vector<BvhNode<N, T>> nodes;
-                std::vector<std::uint32_t> indices;
+                // meshes: vertices, normals and facets of all meshes in one
+                // set of arrays; BVHs built on the GPU (or the host); facet
+                // records set up on the GPU
                 std::vector<double> all_vertices;
                 std::vector<T> all_normals;
                 std::vector<int> all_facets;
                 std::vector<int> all_materials;
                 bool any_normals = false;
+                std::size_t max_facets = 0;
                 for (const MeshHost& m : meshes_)
                 {
                         any_normals = any_normals || !m.normals.empty();
+                        max_facets = std::max(max_facets, m.facets.size() / N);
                 }
-                for (MeshHost& m : meshes_)
                 {
+                        std::size_t vertex_total = 0;
+                        std::size_t facet_total = 0;
+                        for (MeshHost& m : meshes_)
                         {
-                                const Stopwatch bvh_watch(bvh_seconds_);
-                                m.bvh = host::build_facet_bvh<N, T>(m.vertices, m.facets);
+                                m.facet_offset = static_cast<int>(facet_total);
+                                m.index_offset = static_cast<int>(facet_total);
+                                m.vertex_offset = static_cast<int>(vertex_total);
+                                vertex_total += m.vertices.size() / N;
+                                facet_total += m.facets.size() / N;
                         }
-                        m.facet_offset = static_cast<int>(all_facets.size() / N);
-                        m.node_offset = static_cast<int>(nodes.size());
-                        m.index_offset = static_cast<int>(indices.size());
-                        m.vertex_offset = static_cast<int>(all_vertices.size() / N);
-                        const std::size_t node_count = m.bvh.count.size();
-                        for (std::size_t i = 0; i < node_count; ++i)
-                        {
-                                BvhNode<N, T> b;
-                                for (int d = 0; d < N; ++d)
-                                {
-                                        b.lo[d] = m.bvh.lo[i * N + d];
-                                        b.hi[d] = m.bvh.hi[i * N + d];
-                                }
-                                b.offset = m.bvh.offset[i];
-                                b.count = static_cast<std::uint16_t>(m.bvh.count[i]);
-                                b.axis = static_cast<std::uint16_t>(m.bvh.axis[i]);
-                                if (m.bvh.count[i] > 0xffff)
-                                {
-                                        throw std::runtime_error("BVH leaf too large");
-                                }
-                                nodes.push_back(b);
-                        }
-                        indices.insert(indices.end(), m.bvh.indices.begin(), m.bvh.indices.end());
-                        for (const T v : m.vertices)
-                        {
-                                all_vertices.push_back(static_cast<double>(v));
-                        }
-                        const std::size_t vcount = m.vertices.size() / N;
+                        all_vertices.resize(vertex_total * N);
+                        all_facets.resize(facet_total * N);
+                        all_materials.resize(facet_total);
                         if (any_normals)
                         {
-                                if (m.normals.empty())
+                                all_normals.assign(vertex_total * N, T(0));
+                        }
+                        for (const MeshHost& m : meshes_)
+                        {
+                                const std::size_t vo = static_cast<std::size_t>(m.vertex_offset) * N;
+                                const std::size_t fo = static_cast<std::size_t>(m.facet_offset) * N;
+                                parallel_ranges(
+                                        m.vertices.size(),
+                                        [&](const std::size_t b, const std::size_t e)
+                                        {
+                                                for (std::size_t i = b; i < e; ++i)
+                                                {
+                                                        all_vertices[vo + i] = static_cast<double>(m.vertices[i]);
+                                                }
+                                        });
+                                if (!m.normals.empty())
                                 {
-                                        all_normals.insert(all_normals.end(), vcount * N, T(0));
+                                        std::copy(m.normals.begin(), m.normals.end(), all_normals.begin() + vo);
+                                }
+                                parallel_ranges(
+                                        m.facets.size(),
+                                        [&](const std::size_t b, const std::size_t e)
+                                        {
+                                                for (std::size_t i = b; i < e; ++i)
+                                                {
+                                                        all_facets[fo + i] = m.facets[i] + m.vertex_offset;
+                                                }
+                                        });
+                                std::copy(m.facet_materials.begin(), m.facet_materials.end(),
+                                          all_materials.begin() + m.facet_offset);
+                        }
+                }
+                facet_total_ = static_cast<long long>(all_facets.size() / N);
+
+                DeviceArray<double> dv;
+                DeviceArray<int> df;
+                if (facet_total_ > 0)
+                {
+                        dv.upload(all_vertices);
+                        df.upload(all_facets);
+                }
+
+                // BVHs: per mesh, nodes and leaf index slots local to the mesh
+                std::vector<std::unique_ptr<DeviceArray<BvhNode<N, T>>>> mesh_nodes;
+                std::vector<std::unique_ptr<DeviceArray<std::uint32_t>>> mesh_indices;
+                {
+                        const Stopwatch bvh_watch(bvh_seconds_);
+                        const T facet_cost = static_cast<T>(static_cast<double>(N) / host::SIMPLEX_RATE);
+                        const T box_r_cost = static_cast<T>(static_cast<double>(N) / host::BOX_R_RATE);
+                        const T interior_cost = static_cast<T>(2 * box_r_cost);
+                        DeviceArray<double> uniform_sums;
+                        if (bvh_builder_ == 0 && max_facets > 0)
+                        {
+                                // the running sums of the one facet cost (bvh_build.cpp)
+                                std::vector<double> sums(max_facets + 1);
+                                sums[0] = 0;
+                                sums[1] = facet_cost;
+                                for (std::size_t k = 2; k <= max_facets; ++k)
+                                {
+                                        sums[k] = sums[k - 1] + facet_cost;
+                                }
+                                uniform_sums.upload(sums);
+                        }
+                        for (MeshHost& m : meshes_)
+                        {
+                                const int count = static_cast<int>(m.facets.size() / N);
+                                auto nodes = std::make_unique<DeviceArray<BvhNode<N, T>>>();
+                                auto indices = std::make_unique<DeviceArray<std::uint32_t>>();
+                                if (bvh_builder_ == 0)
+                                {
+                                        m.node_count = build_device_bvh<N, T>(
+                                                dv.get(), df.get() + static_cast<std::size_t>(m.facet_offset) * N, count,
+                                                uniform_sums.get(), interior_cost, *nodes, *indices);
                                 }
                                 else
                                 {
-                                        all_normals.insert(all_normals.end(), m.normals.begin(), m.normals.end());
+                                        const host::BuiltBvh<N, T> bvh = host::build_facet_bvh<N, T>(m.vertices, m.facets);
+                                        const std::size_t node_count = bvh.count.size();
+                                        std::vector<BvhNode<N, T>> host_nodes(node_count);
+                                        for (std::size_t i = 0; i < node_count; ++i)
+                                        {
+                                                BvhNode<N, T>& b = host_nodes[i];
+                                                for (int d = 0; d < N; ++d)
+                                                {
+                                                        b.lo[d] = bvh.lo[i * N + d];
+                                                        b.hi[d] = bvh.hi[i * N + d];
+                                                }
+                                                b.offset = bvh.offset[i];
+                                                b.count = static_cast<std::uint16_t>(bvh.count[i]);
+                                                b.axis = static_cast<std::uint16_t>(bvh.axis[i]);
+                                                if (bvh.count[i] > 0xffff)
+                                                {
+                                                        throw std::runtime_error("BVH leaf too large");
+                                                }
+                                        }
+                                        nodes->upload(host_nodes);
+                                        indices->upload(bvh.indices);
+                                        m.node_count = static_cast<int>(node_count);
                                 }
+                                mesh_nodes.push_back(std::move(nodes));
+                                mesh_indices.push_back(std::move(indices));
                         }
-                        const int vo = m.vertex_offset;
-                        for (const int f : m.facets)
-                        {
-                                all_facets.push_back(f + vo);
-                        }
-                        all_materials.insert(all_materials.end(), m.facet_materials.begin(), m.facet_materials.end());
+                }
+                long long node_total = 0;
+                for (MeshHost& m : meshes_)
+                {
+                        m.node_offset = static_cast<int>(node_total);
+                        node_total += m.node_count;
+                }
+                node_total_ = node_total;
+                d_nodes_.allocate(node_total);
+                d_indices_.allocate(facet_total_);
+                mesh_records_.clear();
+                for (std::size_t k = 0; k < meshes_.size(); ++k)
+                {
+                        const MeshHost& m = meshes_[k];
+                        const std::size_t count = m.facets.size() / N;
+                        NBPT_CUDA(cudaMemcpy(d_nodes_.get() + m.node_offset, mesh_nodes[k]->get(),
+                                             static_cast<std::size_t>(m.node_count) * sizeof(BvhNode<N, T>),
+                                             cudaMemcpyDeviceToDevice));
+                        NBPT_CUDA(cudaMemcpy(d_indices_.get() + m.index_offset, mesh_indices[k]->get(),
+                                             count * sizeof(std::uint32_t), cudaMemcpyDeviceToDevice));
+                        BvhNode<N, T> root;
+                        NBPT_CUDA(cudaMemcpy(&root, mesh_nodes[k]->get(), sizeof(root), cudaMemcpyDeviceToHost));
                         MeshShape<N, T> rec;
                         for (int d = 0; d < N; ++d)
                         {
-                                rec.lo[d] = m.bvh.lo[d];
-                                rec.hi[d] = m.bvh.hi[d];
+                                rec.lo[d] = root.lo[d];
+                                rec.hi[d] = root.hi[d];
                         }
                         rec.node_offset = m.node_offset;
                         rec.index_offset = m.index_offset;
                         rec.facet_offset = m.facet_offset;
                         mesh_records_.push_back(rec);
                 }
-                facet_total_ = static_cast<long long>(all_facets.size() / N);
-                node_total_ = static_cast<long long>(nodes.size());
+                mesh_nodes.clear();
+                mesh_indices.clear();
 
                 d_flat_.upload(flat_);
                 d_solid_.upload(solid_);
                 d_meshes_.upload(mesh_records_);
-                d_nodes_.upload(nodes);
-                d_indices_.upload(indices);
                 d_materials_.upload(materials_);
                 d_lights_.upload(lights_);
                 upload_bytes_ = static_cast<long long>(d_flat_.bytes() + d_solid_.bytes() + d_meshes_.bytes() +
-                                                       d_nodes_.bytes() + d_indices_.bytes() + d_materials_.bytes() +
-                                                       d_lights_.bytes());
+                                                       d_materials_.bytes() + d_lights_.bytes() + dv.bytes() +
+                                                       df.bytes());
+                if (bvh_builder_ != 0)
+                {
+                        upload_bytes_ += static_cast<long long>(d_nodes_.bytes() + d_indices_.bytes());
+                }
 
                 if (facet_total_ > 0)
                 {
-                        DeviceArray<double> dv;
-                        dv.upload(all_vertices);
                         DeviceArray<double> dn;
-                        std::vector<double> normals_double(all_normals.begin(), all_normals.end());
                         if (any_normals)
                         {
+                                std::vector<double> normals_double(all_normals.begin(), all_normals.end());
                                 dn.upload(normals_double);
                         }
-                        DeviceArray<int> df;
-                        df.upload(all_facets);
                         DeviceArray<int> dm;
                         dm.upload(all_materials);
                         DeviceArray<int> derr;
                         std::vector<int> zero(1, 0);
                         derr.upload(zero);
-                        upload_bytes_ += static_cast<long long>(dv.bytes() + dn.bytes() + df.bytes() + dm.bytes() +
-                                                                derr.bytes());
+                        upload_bytes_ += static_cast<long long>(dn.bytes() + dm.bytes() + derr.bytes());
                         d_facets_.allocate(facet_total_);
                         facet_setup_kernel<N, T><<<blocks_for(facet_total_, 128), 128>>>(
                                 dv.get(), any_normals ? dn.get() : nullptr, df.get(), dm.get(), facet_total_,
@@ -2041,10 +2282,10 @@ void SceneT<N, T, C>::mesh_export(
         }
         const MeshHost& m = meshes_[mesh];
         const long long facets = static_cast<long long>(m.facets.size() / N);
-        const long long nodes = static_cast<long long>(m.bvh.count.size());
+        const long long nodes = m.node_count;
         counts[0] = facets;
         counts[1] = nodes;
-        counts[2] = static_cast<long long>(m.bvh.indices.size());
+        counts[2] = facets;
         if (!planes)
         {
                 return;
@@ -2071,18 +2312,22 @@ void SceneT<N, T, C>::mesh_export(
                 normal_info[i * 2] = f[i].normal_type;
                 normal_info[i * 2 + 1] = static_cast<int>(f[i].reverse_mask);
         }
+        std::vector<BvhNode<N, T>> b(nodes);
+        NBPT_CUDA(cudaMemcpy(b.data(), d_nodes_.get() + m.node_offset, nodes * sizeof(BvhNode<N, T>),
+                             cudaMemcpyDeviceToHost));
         for (long long i = 0; i < nodes; ++i)
         {
                 for (int d = 0; d < N; ++d)
                 {
-                        node_lo[i * N + d] = static_cast<double>(m.bvh.lo[i * N + d]);
-                        node_hi[i * N + d] = static_cast<double>(m.bvh.hi[i * N + d]);
+                        node_lo[i * N + d] = static_cast<double>(b[i].lo[d]);
+                        node_hi[i * N + d] = static_cast<double>(b[i].hi[d]);
                 }
-                node_info[i * 3] = m.bvh.offset[i];
-                node_info[i * 3 + 1] = m.bvh.count[i];
-                node_info[i * 3 + 2] = m.bvh.axis[i];
+                node_info[i * 3] = b[i].offset;
+                node_info[i * 3 + 1] = b[i].count;
+                node_info[i * 3 + 2] = b[i].axis;
         }
-        std::copy(m.bvh.indices.begin(), m.bvh.indices.end(), indices);
+        NBPT_CUDA(cudaMemcpy(indices, d_indices_.get() + m.index_offset, facets * sizeof(std::uint32_t),
+                             cudaMemcpyDeviceToHost));
 }
 
 template <int N, typename T, int C>

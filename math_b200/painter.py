@@ -87,6 +87,7 @@ SIGNATURES = [
     ("nbpt_scene_device_bytes", ctypes.c_longlong, [_P]),
     ("nbpt_scene_upload_bytes", ctypes.c_longlong, [_P]),
     ("nbpt_scene_build_seconds", ctypes.c_int, [_P, _D]),
+    ("nbpt_scene_set_bvh_builder", ctypes.c_int, [_P, ctypes.c_int]),
     ("nbpt_painter_create", _P, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_uint]),
     ("nbpt_painter_create_integrator", _P, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint]),
     ("nbpt_painter_destroy", None, [_P]),
@@ -178,7 +179,7 @@ class Scene:
     """
 
     def __init__(self, desc: dict, precision: str = "float", spectrum: bool = False,
-                 mesh_data: list | None = None):
+                 mesh_data: list | None = None, bvh_builder: str = "device"):
         L = lib()
         self.n = int(desc["n"])
         self.spectrum = bool(spectrum)
@@ -248,6 +249,7 @@ class Scene:
                 self.h, _p(_d(p["org"]), _D), _p(_d(p["dir"]), _D),
                 _p(_d(p["axes"]).reshape(-1), _D), p["units_per_pixel"], _p(size, _I)))
         _check(L.nbpt_scene_set_background(self.h, _p(_f(desc["background"]), _F)))
+        _check(L.nbpt_scene_set_bvh_builder(self.h, {"device": 0, "host": 1}[bvh_builder]))
         _check(L.nbpt_scene_finalize(self.h))
         self.size = [int(x) for x in p["size"]]
         self.pixels = int(np.prod(self.size))
