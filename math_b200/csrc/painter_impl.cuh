@@ -33,6 +33,9 @@
 #include <string>
 #include <type_traits>
 #include <thread>
+#include <atomic>
+#include <exception>
+#include <mutex>
 #include <vector>
 
 namespace nbpt
@@ -251,6 +254,59 @@ void parallel_ranges(const std::size_t count, const F& f)
         }
 }
 
+// f(begin, end) over [0, count): in parts on the host threads, or at once
+template <typename F>
+void ranges(const bool parallel, const std::size_t count, const F& f)
+{
+        if (parallel)
+        {
+                parallel_ranges(count, f);
+        }
+        else
+        {
+                f(std::size_t{0}, count);
+        }
+}
+
+// f(i) for i in [0, count), the indices shared out among the host threads
+template <typename F>
+void parallel_items(const std::size_t count, const F& f)
+{
+        const unsigned threads = std::min<std::size_t>(std::max(1u, std::thread::hardware_concurrency()), count);
+        std::atomic<std::size_t> next{0};
+        std::vector<std::thread> pool;
+        std::exception_ptr error;
+        std::mutex error_mutex;
+        const auto work = [&]
+        {
+                try
+                {
+                        for (std::size_t i = next++; i < count; i = next++)
+                        {
+                                f(i);
+                        }
+                }
+                catch (...)
+                {
+                        const std::lock_guard lock(error_mutex);
+                        error = std::current_exception();
+                }
+        };
+        for (unsigned t = 1; t < threads; ++t)
+        {
+                pool.emplace_back(work);
+        }
+        work();
+        for (std::thread& t : pool)
+        {
+                t.join();
+        }
+        if (error)
+        {
+                std::rethrow_exception(error);
+        }
+}
+
 // Adds the seconds from its construction to its destruction to `total`.
 class Stopwatch final
 {
@@ -279,14 +335,15 @@ public:
 // (after src/model/mesh/normals.cpp:46-195).  Facet normals and angles are
 // computed in parallel; the sums run over the facets in order.
 template <int N>
-std::vector<float> vertex_normals(const std::vector<float>& points, const std::vector<int>& facets)
+std::vector<float> vertex_normals(const std::vector<float>& points, const std::vector<int>& facets,
+                                  const bool parallel = true)
 {
         const std::size_t vcount = points.size() / N;
         const std::size_t fcount = facets.size() / N;
         std::vector<Vec<N, double>> fn(fcount);
         std::vector<double> weight(fcount * N, 1.0);
-        parallel_ranges(
-                fcount,
+        ranges(
+                parallel, fcount,
                 [&](const std::size_t begin, const std::size_t end)
                 {
                         for (std::size_t f = begin; f < end; ++f)
@@ -874,7 +931,17 @@ public:
                 {
                         throw std::runtime_error("No objects to paint");
                 }
+                // objects in order: offsets and materials; then every object's
+                // normals and transforms, the objects shared out among the host
+                // threads when there are many, each object's work shared out
+                // when there are few
                 MeshHost mesh;
+                std::vector<MeshObjectHost*> objects;
+                std::vector<std::size_t> vertex_base;
+                std::vector<std::size_t> facet_base;
+                std::vector<int> materials;
+                std::size_t vertex_total = 0;
+                std::size_t facet_total = 0;
                 for (MeshObjectHost& o : pending_)
                 {
                         const T alpha = clamp_t(static_cast<T>(o.alpha));
@@ -882,17 +949,42 @@ public:
                         {
                                 continue;
                         }
-                        const int vertex_offset = static_cast<int>(mesh.vertices.size() / N);
+                        objects.push_back(&o);
+                        vertex_base.push_back(vertex_total);
+                        facet_base.push_back(facet_total);
+                        vertex_total += o.points.size() / N;
+                        facet_total += o.facets.size() / N;
+                        materials.push_back(add_material(
+                                [&]
+                                {
+                                        std::vector<float> c = host::surface_color(C, o.rgb);
+                                        for (float& x : c)
+                                        {
+                                                x = host::clamp01(x);
+                                        }
+                                        return c;
+                                }(),
+                                static_cast<float>(clamp_t(static_cast<T>(o.metalness))),
+                                clamp_t(static_cast<T>(o.roughness))));
+                }
+                mesh.vertices.resize(vertex_total * N);
+                mesh.normals.resize(vertex_total * N);
+                mesh.facets.resize(facet_total * N);
+                mesh.facet_materials.resize(facet_total);
+                const bool per_object = objects.size() >= 4;
+                const auto ingest = [&](const std::size_t k)
+                {
+                        MeshObjectHost& o = *objects[k];
+                        const bool inner_parallel = !per_object;
                         const std::size_t vcount = o.points.size() / N;
                         if (o.normals.empty())
                         {
-                                o.normals = vertex_normals<N>(o.points, o.facets);
+                                o.normals = vertex_normals<N>(o.points, o.facets, inner_parallel);
                         }
                         // vertices: M * (v, 1)  (numerical/transform.h:83-119)
-                        const std::size_t vbase = mesh.vertices.size();
-                        mesh.vertices.resize(vbase + vcount * N);
-                        parallel_ranges(
-                                vcount,
+                        const std::size_t vbase = vertex_base[k] * N;
+                        ranges(
+                                inner_parallel, vcount,
                                 [&](const std::size_t begin, const std::size_t end)
                                 {
                                         for (std::size_t v = begin; v < end; ++v)
@@ -921,10 +1013,8 @@ public:
                                 }
                         }
                         const std::array<T, N * N> inv = inverse<N, T>(lin);
-                        const std::size_t nbase = mesh.normals.size();
-                        mesh.normals.resize(nbase + vcount * N);
-                        parallel_ranges(
-                                vcount,
+                        ranges(
+                                inner_parallel, vcount,
                                 [&](const std::size_t begin, const std::size_t end)
                                 {
                                         for (std::size_t v = begin; v < end; ++v)
@@ -937,27 +1027,29 @@ public:
                                                         {
                                                                 x += inv[c * N + r] * static_cast<T>(o.normals[v * N + c]);
                                                         }
-                                                        mesh.normals[nbase + v * N + r] = x;
+                                                        mesh.normals[vbase + v * N + r] = x;
                                                 }
                                         }
                                 });
-                        const int material = add_material(
-                                [&]
-                                {
-                                        std::vector<float> c = host::surface_color(C, o.rgb);
-                                        for (float& x : c)
-                                        {
-                                                x = host::clamp01(x);
-                                        }
-                                        return c;
-                                }(),
-                                static_cast<float>(clamp_t(static_cast<T>(o.metalness))),
-                                clamp_t(static_cast<T>(o.roughness)));
-                        for (const int i : o.facets)
+                        const std::size_t fbase = facet_base[k];
+                        const int vertex_offset = static_cast<int>(vertex_base[k]);
+                        for (std::size_t i = 0; i < o.facets.size(); ++i)
                         {
-                                mesh.facets.push_back(i + vertex_offset);
+                                mesh.facets[fbase * N + i] = o.facets[i] + vertex_offset;
                         }
-                        mesh.facet_materials.insert(mesh.facet_materials.end(), o.facets.size() / N, material);
+                        std::fill(mesh.facet_materials.begin() + fbase,
+                                  mesh.facet_materials.begin() + fbase + o.facets.size() / N, materials[k]);
+                };
+                if (per_object)
+                {
+                        parallel_items(objects.size(), ingest);
+                }
+                else
+                {
+                        for (std::size_t k = 0; k < objects.size(); ++k)
+                        {
+                                ingest(k);
+                        }
                 }
                 pending_.clear();
                 if (mesh.facets.empty())
