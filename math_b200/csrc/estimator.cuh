@@ -22,170 +22,15 @@
 #pragma once
 
 #include "core.cuh"
+#include "group_order.h"
 
 #include <cstdint>
 
 namespace nbpt
 {
-inline constexpr int HELD_OUT = 4; // the reference's FILTER_SAMPLE_COUNT (pixels.h:42)
 
 // largest number of samples per pixel a pass can gather in one group
 inline constexpr int MAX_GROUP = 256;
-
-// ---------------------------------------------------------------------------
-// ordering of a group: the steps of an insertion sort (for up to eight
-// entries) and of a binary-heap partial selection (more entries), with the
-// "hole" moves of the classic sift-down / sift-up, on an index array ordered
-// by `less(a, b)`.
-
-template <typename Less>
-NBPT_HD void insertion_sort(int* a, const int n, const Less& less)
-{
-        for (int i = 1; i < n; ++i)
-        {
-                const int v = a[i];
-                if (less(v, a[0]))
-                {
-                        for (int k = i; k > 0; --k)
-                        {
-                                a[k] = a[k - 1];
-                        }
-                        a[0] = v;
-                }
-                else
-                {
-                        int k = i;
-                        while (less(v, a[k - 1]))
-                        {
-                                a[k] = a[k - 1];
-                                --k;
-                        }
-                        a[k] = v;
-                }
-        }
-}
-
-// Accessors that view either a plain range or its reverse.
-struct Forward final
-{
-        int* base;
-        NBPT_HD int& at(const int i) const
-        {
-                return base[i];
-        }
-};
-
-struct Reverse final
-{
-        int* last; // element 0 of the view is *last, element i is last[-i]
-        NBPT_HD int& at(const int i) const
-        {
-                return last[-i];
-        }
-};
-
-template <typename View, typename Less>
-NBPT_HD void heap_push(const View& v, int hole, const int top, const int value, const Less& less)
-{
-        int parent = (hole - 1) / 2;
-        while (hole > top && less(v.at(parent), value))
-        {
-                v.at(hole) = v.at(parent);
-                hole = parent;
-                parent = (hole - 1) / 2;
-        }
-        v.at(hole) = value;
-}
-
-template <typename View, typename Less>
-NBPT_HD void heap_adjust(const View& v, int hole, const int len, const int value, const Less& less)
-{
-        const int top = hole;
-        int second = hole;
-        while (second < (len - 1) / 2)
-        {
-                second = 2 * (second + 1);
-                if (less(v.at(second), v.at(second - 1)))
-                {
-                        --second;
-                }
-                v.at(hole) = v.at(second);
-                hole = second;
-        }
-        if ((len & 1) == 0 && second == (len - 2) / 2)
-        {
-                second = 2 * (second + 1);
-                v.at(hole) = v.at(second - 1);
-                hole = second - 1;
-        }
-        heap_push(v, hole, top, value, less);
-}
-
-template <typename View, typename Less>
-NBPT_HD void heap_make(const View& v, const int len, const Less& less)
-{
-        if (len < 2)
-        {
-                return;
-        }
-        int parent = (len - 2) / 2;
-        while (true)
-        {
-                const int value = v.at(parent);
-                heap_adjust(v, parent, len, value, less);
-                if (parent == 0)
-                {
-                        return;
-                }
-                --parent;
-        }
-}
-
-// pop the top of the heap [0, len) into position `result`
-template <typename View, typename Less>
-NBPT_HD void heap_pop(const View& v, const int len, const int result, const Less& less)
-{
-        const int value = v.at(result);
-        v.at(result) = v.at(0);
-        heap_adjust(v, 0, len, value, less);
-}
-
-// the `middle` smallest of [0, last) sorted into [0, middle)
-template <typename View, typename Less>
-NBPT_HD void partial_sort(const View& v, const int middle, const int last, const Less& less)
-{
-        heap_make(v, middle, less);
-        for (int i = middle; i < last; ++i)
-        {
-                if (less(v.at(i), v.at(0)))
-                {
-                        heap_pop(v, middle, i, less);
-                }
-        }
-        for (int len = middle; len > 1;)
-        {
-                --len;
-                heap_pop(v, len, len, less);
-        }
-}
-
-// src/painter/pixels/samples/com/sort.h:26-46
-template <typename Less, typename Greater>
-NBPT_HD void order_group(int* a, const int n, const Less& less, const Greater& greater)
-{
-        if (n <= 1)
-        {
-                return;
-        }
-        if (n <= HELD_OUT * 2)
-        {
-                insertion_sort(a, n, less);
-                return;
-        }
-        partial_sort(Forward{a}, HELD_OUT / 2, n, less);
-        // the highest of [HELD_OUT / 2, n), viewed from the end
-        partial_sort(Reverse{a + n - 1}, HELD_OUT / 2, n - HELD_OUT / 2, greater);
-}
 
 // ---------------------------------------------------------------------------
 // sample sets (samples/color.h, samples/background.h)
@@ -829,15 +674,7 @@ NBPT_HD void accumulate_pixel(
 
                 if (nc > 0)
                 {
-                        const auto less = [&](const int a, const int b)
-                        {
-                                return contribution[a] < contribution[b];
-                        };
-                        const auto greater = [&](const int a, const int b)
-                        {
-                                return contribution[a] > contribution[b];
-                        };
-                        order_group(color_order, nc, less, greater);
+                        order_group(color_order, nc, [&](const int i) { return contribution[i]; });
                         const ColorGroup<C> g{colors + p * spp * C, w, contribution, color_order, nc, C, 1, 0};
                         float g_sum[C];
                         float g_wsum = 0;
@@ -870,15 +707,7 @@ NBPT_HD void accumulate_pixel(
                         {
                                 order[k] = k;
                         }
-                        const auto less = [&](const int a, const int b)
-                        {
-                                return background[a] < background[b];
-                        };
-                        const auto greater = [&](const int a, const int b)
-                        {
-                                return background[a] > background[b];
-                        };
-                        order_group(order, nbg, less, greater);
+                        order_group(order, nbg, [&](const int i) { return background[i]; });
                         float sorted[MAX_GROUP];
                         for (int k = 0; k < nbg; ++k)
                         {
@@ -1066,15 +895,7 @@ __global__ void __launch_bounds__(128) accumulate_warp_kernel(
                                         background[nbg++] = w[j];
                                 }
                         }
-                        const auto less = [&](const int a, const int b)
-                        {
-                                return contribution[a] < contribution[b];
-                        };
-                        const auto greater = [&](const int a, const int b)
-                        {
-                                return contribution[a] > contribution[b];
-                        };
-                        order_group(order, nc, less, greater);
+                        order_group(order, nc, [&](const int i) { return contribution[i]; });
                         if (nbg > 1)
                         {
                                 // background samples are ordered by value; reuse
@@ -1084,15 +905,7 @@ __global__ void __launch_bounds__(128) accumulate_warp_kernel(
                                 {
                                         index[j] = j;
                                 }
-                                const auto bless = [&](const int a, const int b)
-                                {
-                                        return background[a] < background[b];
-                                };
-                                const auto bgreater = [&](const int a, const int b)
-                                {
-                                        return background[a] > background[b];
-                                };
-                                order_group(index, nbg, bless, bgreater);
+                                order_group(index, nbg, [&](const int i) { return background[i]; });
                                 for (int j = 0; j < nbg; ++j)
                                 {
                                         sorted[j] = background[index[j]];
