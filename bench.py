@@ -345,6 +345,16 @@ def run_nbpt(args, rank: int, world: int, local: int):
         P._check(P.lib().nbpt_painter_images(painter.h, P._p(rgb, P._F), P._p(rgba, P._F)))
     resident_s = time.perf_counter() - r0
 
+    # scene resident, passes on the painter's worker thread, every pass's
+    # images delivered to a callback while the next pass renders
+    delivered = []
+    noop = P.PASS_CALLBACK(lambda user, k, rgb, rgba, pixels: delivered.append(k))
+    torch.cuda.synchronize()
+    s0 = time.perf_counter()
+    P._check(P.lib().nbpt_painter_start(painter.h, args.steps, P.ctypes.cast(noop, P.ctypes.c_void_p), None, None))
+    P._check(P.lib().nbpt_painter_join(painter.h))
+    streamed_s = time.perf_counter() - s0
+
     sizes = record_bytes(desc["n"], args.precision)
     algorithmic = nodes * sizes["node"] + facets * sizes["facet"] + shapes * sizes["shape"]
     achieved = algorithmic / paths_s / 1e9 if paths_s > 0 else None
@@ -393,6 +403,10 @@ def run_nbpt(args, rank: int, world: int, local: int):
                             "build, facet setup), one pass, RGB and RGBA images read back to host memory"},
             "resident": {"value": paths_per_step * args.steps / resident_s, "unit": "paths/s",
                          "note": "scene resident; one pass through the C ABI plus the image read back"},
+            "streamed": {"value": paths_per_step * len(delivered) / streamed_s, "unit": "paths/s",
+                         "note": "scene resident; passes on the painter's worker thread (nbpt_painter_start), "
+                                 "each pass's RGB and RGBA images copied to pinned host memory and handed to a "
+                                 "callback while the next pass renders"},
             "gpu_launches": launches,
             "roofline": roofline,
             "clocks": clock_info,

@@ -179,6 +179,29 @@ nbpt_painter* nbpt_painter_create(nbpt_scene* scene, int samples_per_pixel, int 
 nbpt_painter* nbpt_painter_create_integrator(
         nbpt_scene* scene, int integrator, int samples_per_pixel, int max_depth, unsigned seed);
 void nbpt_painter_destroy(nbpt_painter* painter);
+
+/* ---- passes on a worker thread (the reference painter's thread and its
+ * Notifier: src/painter/painter.cpp:77-134, painter.h:36-78) ---- */
+
+/* called on the painter's worker thread after each pass with that pass's
+ * images (as nbpt_painter_images), valid until the callback returns; `pass`
+ * counts from 1 (Notifier::pass_done, Notifier::images) */
+typedef void (*nbpt_pass_callback)(void* user, long long pass, const float* rgb, const float* rgba,
+                                   long long pixel_count);
+/* called on the worker thread when a pass fails (Notifier::error_message);
+ * the worker then ends */
+typedef void (*nbpt_error_callback)(void* user, const char* message);
+/* starts max_pass_count passes (0: until nbpt_painter_stop) on a worker
+ * thread and returns; while pass k + 1 renders, the images of pass k go to
+ * on_pass.  Until the worker ends, the painter's other calls fail. */
+int nbpt_painter_start(nbpt_painter* painter, int max_pass_count, nbpt_pass_callback on_pass,
+                       nbpt_error_callback on_error, void* user);
+/* asks the worker to stop after the pass in flight and waits for it */
+int nbpt_painter_stop(nbpt_painter* painter);
+/* waits for the worker to end (Painter::wait) */
+int nbpt_painter_join(nbpt_painter* painter);
+/* 1 while the worker runs, else 0 */
+int nbpt_painter_is_running(const nbpt_painter* painter);
 /* enqueues `passes` passes on the painter's CUDA stream and returns */
 int nbpt_painter_enqueue(nbpt_painter* painter, int passes);
 /* waits for the enqueued passes and updates the statistics */

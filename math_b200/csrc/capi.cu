@@ -5,6 +5,7 @@
 #include "core.cuh"
 #include "device_pool.h"
 #include "painter_api.h"
+#include "pass_stream.h"
 #include "server.h"
 
 #include <cuda_runtime.h>
@@ -25,6 +26,8 @@ struct nbpt_scene
 struct nbpt_painter
 {
         std::unique_ptr<nbpt::Painter> impl;
+        // passes on a worker thread (nbpt_painter_start); destroyed first
+        std::unique_ptr<nbpt::PassStream> stream;
 };
 
 struct nbpt_server
@@ -84,6 +87,10 @@ nbpt::Painter& painter_of(nbpt_painter* p)
         if (!p || !p->impl)
         {
                 throw std::runtime_error("null painter");
+        }
+        if (p->stream && p->stream->running())
+        {
+                throw std::runtime_error("the painter is running passes on its worker thread");
         }
         return *p->impl;
 }
@@ -622,6 +629,76 @@ nbpt_painter* nbpt_painter_create_integrator(
                         return 0;
                 });
         return out;
+}
+
+int nbpt_painter_start(
+        nbpt_painter* painter,
+        const int max_pass_count,
+        const nbpt_pass_callback on_pass,
+        const nbpt_error_callback on_error,
+        void* const user)
+{
+        return guarded(
+                [&]
+                {
+                        nbpt::Painter& p = painter_of(painter);
+                        if (!on_pass)
+                        {
+                                throw std::runtime_error("null pass callback");
+                        }
+                        if (max_pass_count < 0)
+                        {
+                                throw std::runtime_error("pass count must not be negative");
+                        }
+                        painter->stream.reset();
+                        painter->stream = std::make_unique<nbpt::PassStream>(
+                                &p, p.statistics().pixel_count, max_pass_count, on_pass, on_error, user);
+                        return 0;
+                });
+}
+
+int nbpt_painter_stop(nbpt_painter* painter)
+{
+        return guarded(
+                [&]
+                {
+                        if (!painter)
+                        {
+                                throw std::runtime_error("null painter");
+                        }
+                        if (painter->stream)
+                        {
+                                painter->stream->stop();
+                        }
+                        return 0;
+                });
+}
+
+int nbpt_painter_join(nbpt_painter* painter)
+{
+        return guarded(
+                [&]
+                {
+                        if (!painter)
+                        {
+                                throw std::runtime_error("null painter");
+                        }
+                        if (painter->stream)
+                        {
+                                painter->stream->join();
+                        }
+                        return 0;
+                });
+}
+
+int nbpt_painter_is_running(const nbpt_painter* painter)
+{
+        if (!painter)
+        {
+                g_error = "null painter";
+                return NBPT_ERROR;
+        }
+        return painter->stream && painter->stream->running() ? 1 : 0;
 }
 
 void nbpt_painter_destroy(nbpt_painter* painter)

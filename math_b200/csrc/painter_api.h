@@ -36,6 +36,11 @@ public:
         virtual void enqueue_passes(int passes) = 0;
         virtual void wait() = 0;
         virtual void images(float* rgb, float* rgba) = 0;
+        // resolves the images of the passes so far and copies them to host
+        // memory on the painter's stream, without waiting (the copy overlaps
+        // later work when the host memory is pinned)
+        virtual void enqueue_images(float* rgb, float* rgba) = 0;
+        virtual int device() const = 0;
         virtual void samples(double* points, float* colors, unsigned char* valid) = 0;
         virtual Statistics statistics() = 0;
         virtual void* stream() = 0;

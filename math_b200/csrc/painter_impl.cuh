@@ -1917,6 +1917,7 @@ class PainterT final : public Painter
         int max_depth_;
         std::uint32_t seed_;
         Integrator integrator_;
+        int device_ = 0;
         long long pixels_;
         long long pass_ = 0;
         long long passes_done_ = 0;
@@ -2051,6 +2052,7 @@ public:
                 int device = 0;
                 int sms = 0;
                 NBPT_CUDA(cudaGetDevice(&device));
+                device_ = device;
                 NBPT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
                 chunk_pixels_ = chunk_pixels(pixels_, spp_, max_depth_, integrator_);
                 if (integrator_ == Integrator::PT)
@@ -2254,6 +2256,28 @@ public:
                 {
                         rgba_.download_on(rgba, pixels_ * 4, stream_);
                 }
+        }
+
+        void enqueue_images(float* rgb, float* rgba) override
+        {
+                resolve_kernel<C><<<blocks_for(pixels_, 128), 128, 0, stream_>>>(
+                        pixels_, state_.get(), scene_->cie(), rgb_.get(), rgba_.get());
+                NBPT_CUDA(cudaGetLastError());
+                if (rgb)
+                {
+                        NBPT_CUDA(cudaMemcpyAsync(rgb, rgb_.get(), pixels_ * 3 * sizeof(float), cudaMemcpyDeviceToHost,
+                                                  stream_));
+                }
+                if (rgba)
+                {
+                        NBPT_CUDA(cudaMemcpyAsync(rgba, rgba_.get(), pixels_ * 4 * sizeof(float),
+                                                  cudaMemcpyDeviceToHost, stream_));
+                }
+        }
+
+        int device() const override
+        {
+                return device_;
         }
 
         void samples(double* points, float* colors, unsigned char* valid) override

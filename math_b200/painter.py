@@ -91,6 +91,10 @@ SIGNATURES = [
     ("nbpt_painter_create", _P, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_uint]),
     ("nbpt_painter_create_integrator", _P, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint]),
     ("nbpt_painter_destroy", None, [_P]),
+    ("nbpt_painter_start", ctypes.c_int, [_P, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, _P]),
+    ("nbpt_painter_stop", ctypes.c_int, [_P]),
+    ("nbpt_painter_join", ctypes.c_int, [_P]),
+    ("nbpt_painter_is_running", ctypes.c_int, [_P]),
     ("nbpt_painter_enqueue", ctypes.c_int, [_P, ctypes.c_int]),
     ("nbpt_painter_wait", ctypes.c_int, [_P]),
     ("nbpt_painter_images", ctypes.c_int, [_P, _F, _F]),
@@ -341,6 +345,10 @@ class Scene:
 # painter::Integrator (src/painter/painter.h:143-147)
 INTEGRATORS = {"bpt": 0, "pt": 1}
 
+PASS_CALLBACK = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_float),
+                                 ctypes.POINTER(ctypes.c_float), ctypes.c_longlong)
+ERROR_CALLBACK = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_char_p)
+
 
 class Painter:
     """One render of a scene (the reference's create_painter): integrator
@@ -364,6 +372,36 @@ class Painter:
         if h and _lib is not None:
             _lib.nbpt_painter_destroy(h)
         self.h = None
+        self._callbacks = None
+
+    def start(self, max_passes: int, on_pass, on_error=None):
+        """Runs `max_passes` passes (0: until stop()) on the painter's worker
+        thread; on_pass(pass, rgb [P, 3], rgba [P, 4]) gets each pass's images
+        (copies) while the next pass renders; on_error(message) a failure."""
+
+        def pass_cb(user, pass_number, rgb, rgba, pixels):
+            a = np.ctypeslib.as_array(rgb, shape=(pixels, 3)).copy()
+            b = np.ctypeslib.as_array(rgba, shape=(pixels, 4)).copy()
+            on_pass(int(pass_number), a, b)
+
+        def error_cb(user, message):
+            if on_error is not None:
+                on_error(message.decode())
+
+        c_pass = PASS_CALLBACK(pass_cb)
+        c_error = ERROR_CALLBACK(error_cb)
+        self._callbacks = (c_pass, c_error)  # kept alive while the worker runs
+        _check(lib().nbpt_painter_start(self.h, max_passes, ctypes.cast(c_pass, ctypes.c_void_p),
+                                        ctypes.cast(c_error, ctypes.c_void_p), None))
+
+    def stop(self):
+        _check(lib().nbpt_painter_stop(self.h))
+
+    def join(self):
+        _check(lib().nbpt_painter_join(self.h))
+
+    def is_running(self) -> bool:
+        return _check(lib().nbpt_painter_is_running(self.h)) == 1
 
     def __del__(self):
         self.close()
