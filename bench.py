@@ -349,6 +349,10 @@ def run_nbpt(args, rank: int, world: int, local: int):
     # images delivered to a callback while the next pass renders
     delivered = []
     noop = P.PASS_CALLBACK(lambda user, k, rgb, rgba, pixels: delivered.append(k))
+    # one untimed pass pins the painter's host image buffers
+    P._check(P.lib().nbpt_painter_start(painter.h, 1, P.ctypes.cast(noop, P.ctypes.c_void_p), None, None))
+    P._check(P.lib().nbpt_painter_join(painter.h))
+    delivered.clear()
     torch.cuda.synchronize()
     s0 = time.perf_counter()
     P._check(P.lib().nbpt_painter_start(painter.h, args.steps, P.ctypes.cast(noop, P.ctypes.c_void_p), None, None))

@@ -26,6 +26,8 @@ struct nbpt_scene
 struct nbpt_painter
 {
         std::unique_ptr<nbpt::Painter> impl;
+        // pinned images of the pass worker, kept from one start to the next
+        std::unique_ptr<nbpt::PassBuffers> buffers;
         // passes on a worker thread (nbpt_painter_start); destroyed first
         std::unique_ptr<nbpt::PassStream> stream;
 };
@@ -651,8 +653,12 @@ int nbpt_painter_start(
                                 throw std::runtime_error("pass count must not be negative");
                         }
                         painter->stream.reset();
+                        if (!painter->buffers)
+                        {
+                                painter->buffers = std::make_unique<nbpt::PassBuffers>(p.statistics().pixel_count);
+                        }
                         painter->stream = std::make_unique<nbpt::PassStream>(
-                                &p, p.statistics().pixel_count, max_pass_count, on_pass, on_error, user);
+                                &p, painter->buffers.get(), max_pass_count, on_pass, on_error, user);
                         return 0;
                 });
 }

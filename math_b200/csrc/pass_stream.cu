@@ -18,14 +18,12 @@ void check(const cudaError_t e, const char* what)
         }
 }
 
-// two pinned image buffers and an event for each
-struct Slots final
-{
-        float* rgb[2] = {nullptr, nullptr};
-        float* rgba[2] = {nullptr, nullptr};
-        cudaEvent_t done[2] = {nullptr, nullptr};
+} // namespace
 
-        explicit Slots(const long long pixels)
+PassBuffers::PassBuffers(const long long pixels)
+        : pixel_count(pixels)
+{
+        try
         {
                 for (int i = 0; i < 2; ++i)
                 {
@@ -35,46 +33,63 @@ struct Slots final
                         check(cudaHostAlloc(reinterpret_cast<void**>(&rgba[i]), pixels * 4 * sizeof(float),
                                             cudaHostAllocDefault),
                               "cudaHostAlloc");
-                        check(cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming), "cudaEventCreate");
+                        cudaEvent_t e = nullptr;
+                        check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+                        done[i] = e;
                 }
         }
-
-        ~Slots()
+        catch (...)
         {
-                for (int i = 0; i < 2; ++i)
+                release();
+                throw;
+        }
+}
+
+PassBuffers::~PassBuffers()
+{
+        release();
+}
+
+void PassBuffers::release()
+{
+        for (int i = 0; i < 2; ++i)
+        {
+                if (done[i])
                 {
-                        if (done[i])
-                        {
-                                cudaEventSynchronize(done[i]);
-                                cudaEventDestroy(done[i]);
-                        }
+                        cudaEventSynchronize(static_cast<cudaEvent_t>(done[i]));
+                        cudaEventDestroy(static_cast<cudaEvent_t>(done[i]));
+                        done[i] = nullptr;
+                }
+                if (rgb[i])
+                {
                         cudaFreeHost(rgb[i]);
+                        rgb[i] = nullptr;
+                }
+                if (rgba[i])
+                {
                         cudaFreeHost(rgba[i]);
+                        rgba[i] = nullptr;
                 }
         }
-
-        Slots(const Slots&) = delete;
-        Slots& operator=(const Slots&) = delete;
-};
-} // namespace
+}
 
 PassStream::PassStream(
         Painter* const painter,
-        const long long pixel_count,
+        PassBuffers* const buffers,
         const int max_passes,
         const PassCallback on_pass,
         const ErrorCallback on_error,
         void* const user)
         : painter_(painter),
-          pixel_count_(pixel_count),
+          buffers_(buffers),
           max_passes_(max_passes),
           on_pass_(on_pass),
           on_error_(on_error),
           user_(user)
 {
-        if (!painter || !on_pass)
+        if (!painter || !buffers || !on_pass)
         {
-                throw std::runtime_error("a pass stream needs a painter and a pass callback");
+                throw std::runtime_error("a pass stream needs a painter, its buffers and a pass callback");
         }
         if (max_passes < 0)
         {
@@ -118,13 +133,13 @@ void PassStream::run()
         try
         {
                 check(cudaSetDevice(painter_->device()), "cudaSetDevice");
-                const Slots slots(pixel_count_);
+                PassBuffers& b = *buffers_;
                 const auto stream = static_cast<cudaStream_t>(painter_->stream());
                 const auto launch = [&](const int slot)
                 {
                         painter_->enqueue_passes(1);
-                        painter_->enqueue_images(slots.rgb[slot], slots.rgba[slot]);
-                        check(cudaEventRecord(slots.done[slot], stream), "cudaEventRecord");
+                        painter_->enqueue_images(b.rgb[slot], b.rgba[slot]);
+                        check(cudaEventRecord(static_cast<cudaEvent_t>(b.done[slot]), stream), "cudaEventRecord");
                 };
                 launch(0);
                 for (long long k = 0;; ++k)
@@ -135,9 +150,9 @@ void PassStream::run()
                         {
                                 launch(1 - slot);
                         }
-                        check(cudaEventSynchronize(slots.done[slot]), "pass");
+                        check(cudaEventSynchronize(static_cast<cudaEvent_t>(b.done[slot])), "pass");
                         passes_ = k + 1;
-                        on_pass_(user_, k + 1, slots.rgb[slot], slots.rgba[slot], pixel_count_);
+                        on_pass_(user_, k + 1, b.rgb[slot], b.rgba[slot], b.pixel_count);
                         if (!more)
                         {
                                 break;

@@ -12,6 +12,26 @@
 
 namespace nbpt
 {
+// Two pinned host image buffers and an event for each: pinning host memory
+// is slow, so a painter keeps its buffers from one start to the next.
+class PassBuffers final
+{
+public:
+        explicit PassBuffers(long long pixel_count);
+        ~PassBuffers();
+
+        PassBuffers(const PassBuffers&) = delete;
+        PassBuffers& operator=(const PassBuffers&) = delete;
+
+        long long pixel_count;
+        float* rgb[2] = {nullptr, nullptr};
+        float* rgba[2] = {nullptr, nullptr};
+        void* done[2] = {nullptr, nullptr}; // cudaEvent_t
+
+private:
+        void release();
+};
+
 class PassStream final
 {
 public:
@@ -21,7 +41,7 @@ public:
 
         // Runs `max_passes` passes (0: until stop()).  While pass k + 1 renders,
         // the images of pass k go to `on_pass` on the worker thread.
-        PassStream(Painter* painter, long long pixel_count, int max_passes, PassCallback on_pass,
+        PassStream(Painter* painter, PassBuffers* buffers, int max_passes, PassCallback on_pass,
                    ErrorCallback on_error, void* user);
         ~PassStream();
 
@@ -39,7 +59,7 @@ private:
         void run();
 
         Painter* painter_;
-        long long pixel_count_;
+        PassBuffers* buffers_;
         int max_passes_;
         PassCallback on_pass_;
         ErrorCallback on_error_;

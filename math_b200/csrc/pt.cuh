@@ -221,7 +221,7 @@ __device__ float pt_brdf_channel(const BrdfTerms& t, const int zero, const Mater
 }
 
 #ifndef NBPT_PT_MIN_BLOCKS
-#define NBPT_PT_MIN_BLOCKS 4
+#define NBPT_PT_MIN_BLOCKS 16
 #endif
 
 // One path of the PT integrator per thread (pt.cpp:113-170), persistent: the
