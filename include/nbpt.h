@@ -105,6 +105,18 @@ int nbpt_scene_add_mesh_object(
         nbpt_scene* scene, const float* points, long long point_count, const int* facets, long long facet_count,
         const double* matrix, const float* normals, float metalness, float roughness, const float* rgb, float alpha);
 
+/* A mesh object read from an n-dimensional OBJ (v, vn, f, usemtl, mtllib
+ * with Kd) or STL (ASCII or binary) file, as model::mesh::load reads it
+ * (src/model/mesh/file.cpp:86-104, file/load_obj.cpp, file/load_stl.cpp):
+ * .obj / .stl are 3-space files, .objN / .stlN N-space ones.  Facets with
+ * normals in the file keep them; facets without are flat.  Facets that name a
+ * material take its Kd colour, the others the object's colour. */
+int nbpt_scene_add_mesh_file(
+        nbpt_scene* scene, const char* path, const double* matrix, float metalness, float roughness, const float* rgb,
+        float alpha);
+/* the dimension of an OBJ or STL file from its name (file_type.cpp) */
+int nbpt_mesh_file_dimension(const char* path);
+
 /* shapes::create_mesh(mesh_objects, no clip plane, ...): one mesh shape from
  * the accumulated objects; returns the shape index. */
 int nbpt_scene_add_mesh(nbpt_scene* scene);

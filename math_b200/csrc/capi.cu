@@ -4,6 +4,7 @@
 
 #include "core.cuh"
 #include "device_pool.h"
+#include "mesh_files.h"
 #include "painter_api.h"
 #include "pass_stream.h"
 #include "server.h"
@@ -398,6 +399,40 @@ int nbpt_scene_add_mesh_object(
                         return scene_of(scene).add_mesh_object(
                                 points, point_count, facets, facet_count, matrix, normals, metalness, roughness, rgb,
                                 alpha);
+                });
+}
+
+int nbpt_scene_add_mesh_file(
+        nbpt_scene* scene,
+        const char* path,
+        const double* matrix,
+        const float metalness,
+        const float roughness,
+        const float* rgb,
+        const float alpha)
+{
+        return guarded(
+                [&]
+                {
+                        require(path, "path");
+                        require(matrix, "matrix");
+                        require(rgb, "color");
+                        return scene_of(scene).add_mesh_file(path, matrix, metalness, roughness, rgb, alpha);
+                });
+}
+
+int nbpt_mesh_file_dimension(const char* path)
+{
+        return guarded(
+                [&]
+                {
+                        require(path, "path");
+                        const int n = nbpt::host::mesh_file_dimension(path);
+                        if (n == 0)
+                        {
+                                throw std::runtime_error(std::string("Not an OBJ or STL file name: ") + path);
+                        }
+                        return n;
                 });
 }
 

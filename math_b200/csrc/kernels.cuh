@@ -26,6 +26,7 @@ template <int N, typename T>
 __global__ void facet_setup_kernel(
         const double* __restrict__ vertices,
         const double* __restrict__ normals, // nullptr: no vertex normals
+        const unsigned char* __restrict__ flat, // nullptr, or 1 for a facet without vertex normals
         const int* __restrict__ facet_vertices,
         const int* __restrict__ facet_materials,
         const long long count,
@@ -57,7 +58,7 @@ __global__ void facet_setup_kernel(
         }
         int normal_type = static_cast<int>(NormalType::NONE);
         unsigned reverse_mask = 0;
-        if (normals)
+        if (normals && !(flat && flat[f]))
         {
                 double dots[N];
                 bool unidirectional = true;

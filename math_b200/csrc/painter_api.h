@@ -64,6 +64,8 @@ public:
         virtual int add_mesh_object(const float* points, long long point_count, const int* facets,
                                     long long facet_count, const double* matrix, const float* normals,
                                     float metalness, float roughness, const float* rgb, float alpha) = 0;
+        virtual int add_mesh_file(const char* path, const double* matrix, float metalness, float roughness,
+                                  const float* rgb, float alpha) = 0;
         virtual int add_mesh() = 0;
         virtual int add_mesh_data(long long vertex_count, const double* vertices, const double* normals,
                                   long long facet_count, const int* facets, const int* facet_materials,

@@ -13,6 +13,7 @@
 
 #include "bvh_build.h"
 #include "bvh_device.cuh"
+#include "mesh_files.h"
 #include "device_pool.h"
 #include "estimator.cuh"
 #include "host_math.h"
@@ -32,6 +33,7 @@
 #include <stdexcept>
 #include <string>
 #include <type_traits>
+#include <unordered_map>
 #include <thread>
 #include <atomic>
 #include <exception>
@@ -617,6 +619,12 @@ class SceneT final : public Scene
                 float roughness;
                 float alpha;
                 float rgb[3];
+                // mesh files: the normals are the file's (none: a flat facet),
+                // and facets may name materials of their own
+                bool file = false;
+                std::vector<unsigned char> flat;               // [F]
+                std::vector<int> facet_material;               // [F], -1: the object's colour
+                std::vector<std::array<float, 3>> colors;      // the file's materials
         };
 
         struct MeshHost final
@@ -625,6 +633,7 @@ class SceneT final : public Scene
                 std::vector<T> normals;  // [V][N] or empty
                 std::vector<int> facets;
                 std::vector<int> facet_materials;
+                std::vector<unsigned char> flat; // [F]: no vertex normals
                 int node_count = 0;
                 int facet_offset = 0;
                 int node_offset = 0;
@@ -921,6 +930,61 @@ public:
                 return static_cast<int>(pending_.size()) - 1;
         }
 
+        // A mesh object read from an OBJ or STL file (model/mesh/file.cpp:86-104):
+        // every distinct (vertex, normal) corner of its facets becomes a point,
+        // numbered by first use; facets without normals are flat.
+        int add_mesh_file(
+                const char* path,
+                const double* matrix,
+                const float metalness,
+                const float roughness,
+                const float* rgb,
+                const float alpha) override
+        {
+                check_open();
+                const host::MeshFile file = host::load_mesh_file(path, N);
+                MeshObjectHost o;
+                o.file = true;
+                const std::size_t facet_count = file.has_normal.size();
+                const long long normal_slots = static_cast<long long>(file.normals.size() / N) + 1;
+                std::unordered_map<long long, int> corner;
+                o.facets.resize(facet_count * N);
+                for (std::size_t f = 0; f < facet_count; ++f)
+                {
+                        for (int k = 0; k < N; ++k)
+                        {
+                                const int v = file.facet_vertices[f * N + k];
+                                const int nm = file.has_normal[f] ? file.facet_normals[f * N + k] : -1;
+                                const long long key = static_cast<long long>(v) * normal_slots + (nm + 1);
+                                auto [it, inserted] = corner.emplace(key, static_cast<int>(o.points.size() / N));
+                                if (inserted)
+                                {
+                                        for (int d = 0; d < N; ++d)
+                                        {
+                                                o.points.push_back(file.vertices[static_cast<std::size_t>(v) * N + d]);
+                                                o.normals.push_back(
+                                                        nm < 0 ? 0.0f : file.normals[static_cast<std::size_t>(nm) * N + d]);
+                                        }
+                                }
+                                o.facets[f * N + k] = it->second;
+                        }
+                }
+                o.flat.resize(facet_count);
+                for (std::size_t f = 0; f < facet_count; ++f)
+                {
+                        o.flat[f] = file.has_normal[f] ? 0 : 1;
+                }
+                o.facet_material = file.facet_material;
+                o.colors = file.material_colors;
+                std::copy(matrix, matrix + (N + 1) * (N + 1), o.matrix.begin());
+                o.metalness = metalness;
+                o.roughness = roughness;
+                o.alpha = alpha;
+                std::copy(rgb, rgb + 3, o.rgb);
+                pending_.push_back(std::move(o));
+                return static_cast<int>(pending_.size()) - 1;
+        }
+
         // shapes/mesh/data.cpp:88-310: transform the objects' vertices and
         // normals, one material per object
         int add_mesh() override
@@ -939,7 +1003,8 @@ public:
                 std::vector<MeshObjectHost*> objects;
                 std::vector<std::size_t> vertex_base;
                 std::vector<std::size_t> facet_base;
-                std::vector<int> materials;
+                std::vector<int> materials;            // the object's colour
+                std::vector<std::vector<int>> file_materials; // the file's materials
                 std::size_t vertex_total = 0;
                 std::size_t facet_total = 0;
                 for (MeshObjectHost& o : pending_)
@@ -954,30 +1019,39 @@ public:
                         facet_base.push_back(facet_total);
                         vertex_total += o.points.size() / N;
                         facet_total += o.facets.size() / N;
-                        materials.push_back(add_material(
-                                [&]
+                        const auto color_of = [&](const float* rgb)
+                        {
+                                std::vector<float> c = host::surface_color(C, rgb);
+                                for (float& x : c)
                                 {
-                                        std::vector<float> c = host::surface_color(C, o.rgb);
-                                        for (float& x : c)
-                                        {
-                                                x = host::clamp01(x);
-                                        }
-                                        return c;
-                                }(),
-                                static_cast<float>(clamp_t(static_cast<T>(o.metalness))),
-                                clamp_t(static_cast<T>(o.roughness))));
+                                        x = host::clamp01(x);
+                                }
+                                return c;
+                        };
+                        const float metalness = static_cast<float>(clamp_t(static_cast<T>(o.metalness)));
+                        const T roughness = clamp_t(static_cast<T>(o.roughness));
+                        // the file's materials, then the object's colour
+                        // (shapes/mesh/data.cpp:113-161)
+                        std::vector<int> own;
+                        for (const std::array<float, 3>& c : o.colors)
+                        {
+                                own.push_back(add_material(color_of(c.data()), metalness, roughness));
+                        }
+                        file_materials.push_back(std::move(own));
+                        materials.push_back(add_material(color_of(o.rgb), metalness, roughness));
                 }
                 mesh.vertices.resize(vertex_total * N);
                 mesh.normals.resize(vertex_total * N);
                 mesh.facets.resize(facet_total * N);
                 mesh.facet_materials.resize(facet_total);
+                mesh.flat.assign(facet_total, 0);
                 const bool per_object = objects.size() >= 4;
                 const auto ingest = [&](const std::size_t k)
                 {
                         MeshObjectHost& o = *objects[k];
                         const bool inner_parallel = !per_object;
                         const std::size_t vcount = o.points.size() / N;
-                        if (o.normals.empty())
+                        if (o.normals.empty() && !o.file)
                         {
                                 o.normals = vertex_normals<N>(o.points, o.facets, inner_parallel);
                         }
@@ -1037,8 +1111,13 @@ public:
                         {
                                 mesh.facets[fbase * N + i] = o.facets[i] + vertex_offset;
                         }
-                        std::fill(mesh.facet_materials.begin() + fbase,
-                                  mesh.facet_materials.begin() + fbase + o.facets.size() / N, materials[k]);
+                        const std::size_t fcount = o.facets.size() / N;
+                        for (std::size_t f = 0; f < fcount; ++f)
+                        {
+                                const int own = o.facet_material.empty() ? -1 : o.facet_material[f];
+                                mesh.facet_materials[fbase + f] = own < 0 ? materials[k] : file_materials[k][own];
+                                mesh.flat[fbase + f] = o.flat.empty() ? 0 : o.flat[f];
+                        }
                 };
                 if (per_object)
                 {
@@ -1326,11 +1405,14 @@ public:
                 std::vector<T> all_normals;
                 std::vector<int> all_facets;
                 std::vector<int> all_materials;
+                std::vector<unsigned char> all_flat;
                 bool any_normals = false;
+                bool any_flat = false;
                 std::size_t max_facets = 0;
                 for (const MeshHost& m : meshes_)
                 {
                         any_normals = any_normals || !m.normals.empty();
+                        any_flat = any_flat || std::find(m.flat.begin(), m.flat.end(), 1) != m.flat.end();
                         max_facets = std::max(max_facets, m.facets.size() / N);
                 }
                 {
@@ -1347,6 +1429,10 @@ public:
                         all_vertices.resize(vertex_total * N);
                         all_facets.resize(facet_total * N);
                         all_materials.resize(facet_total);
+                        if (any_flat)
+                        {
+                                all_flat.assign(facet_total, 0);
+                        }
                         if (any_normals)
                         {
                                 all_normals.assign(vertex_total * N, T(0));
@@ -1379,6 +1465,10 @@ public:
                                         });
                                 std::copy(m.facet_materials.begin(), m.facet_materials.end(),
                                           all_materials.begin() + m.facet_offset);
+                                if (any_flat && !m.flat.empty())
+                                {
+                                        std::copy(m.flat.begin(), m.flat.end(), all_flat.begin() + m.facet_offset);
+                                }
                         }
                 }
                 facet_total_ = static_cast<long long>(all_facets.size() / N);
@@ -1510,14 +1600,19 @@ public:
                         }
                         DeviceArray<int> dm;
                         dm.upload(all_materials);
+                        DeviceArray<unsigned char> dflat;
+                        if (any_flat)
+                        {
+                                dflat.upload(all_flat);
+                        }
                         DeviceArray<int> derr;
                         std::vector<int> zero(1, 0);
                         derr.upload(zero);
-                        upload_bytes_ += static_cast<long long>(dn.bytes() + dm.bytes() + derr.bytes());
+                        upload_bytes_ += static_cast<long long>(dn.bytes() + dm.bytes() + derr.bytes() + dflat.bytes());
                         d_facets_.allocate(facet_total_);
                         facet_setup_kernel<N, T><<<blocks_for(facet_total_, 128), 128>>>(
-                                dv.get(), any_normals ? dn.get() : nullptr, df.get(), dm.get(), facet_total_,
-                                d_facets_.get(), derr.get());
+                                dv.get(), any_normals ? dn.get() : nullptr, any_flat ? dflat.get() : nullptr, df.get(),
+                                dm.get(), facet_total_, d_facets_.get(), derr.get());
                         NBPT_CUDA(cudaGetLastError());
                         NBPT_CUDA(cudaDeviceSynchronize());
                         int err = 0;

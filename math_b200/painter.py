@@ -87,6 +87,9 @@ SIGNATURES = [
     ("nbpt_scene_device_bytes", ctypes.c_longlong, [_P]),
     ("nbpt_scene_upload_bytes", ctypes.c_longlong, [_P]),
     ("nbpt_scene_build_seconds", ctypes.c_int, [_P, _D]),
+    ("nbpt_scene_add_mesh_file", ctypes.c_int,
+     [_P, ctypes.c_char_p, _D, ctypes.c_float, ctypes.c_float, _F, ctypes.c_float]),
+    ("nbpt_mesh_file_dimension", ctypes.c_int, [ctypes.c_char_p]),
     ("nbpt_scene_set_bvh_builder", ctypes.c_int, [_P, ctypes.c_int]),
     ("nbpt_painter_create", _P, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_uint]),
     ("nbpt_painter_create_integrator", _P, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint]),
@@ -219,6 +222,11 @@ class Scene:
                         _p(fc, _I), _p(fm, _I), len(mp), _p(mp, _D), _p(mc, _F)))
                 else:
                     for o in s["objects"]:
+                        if "file" in o:
+                            _check(L.nbpt_scene_add_mesh_file(
+                                self.h, str(o["file"]).encode(), _p(_d(o["matrix"]).reshape(-1), _D),
+                                o["metalness"], o["roughness"], _p(_f(o["color"]), _F), o["alpha"]))
+                            continue
                         pts = _f(o["points"]).reshape(-1, n)
                         fac = _i(o["facets"]).reshape(-1, n)
                         nrm = o.get("normals")

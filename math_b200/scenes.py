@@ -14,6 +14,8 @@ through their own constructors, so that both render exactly the same geometry:
             {"points": float32 [V, n], "facets": int32 [F, n],
              "matrix": [(n+1)][(n+1)], "metalness", "roughness",
              "color": [r, g, b], "alpha"}, ...]},
+            (or {"file": an OBJ / STL path, "matrix", "metalness", ...} in
+             place of "points" and "facets")
       ],
       "lights": [                          in creation order
         {"type": "parallelotope", "shape": index of a hyperplane_parallelotope,

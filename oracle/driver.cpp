@@ -47,6 +47,8 @@
 #include <src/image/image.h>
 #include <src/model/mesh.h>
 #include <src/model/mesh/create_facets.h>
+#include <src/model/mesh/file/load_obj.h>
+#include <src/model/mesh/file/load_stl.h>
 #include <src/model/mesh_object.h>
 #include <src/numerical/matrix.h>
 #include <src/numerical/ray.h>
@@ -79,6 +81,7 @@
 #include <cstdint>
 #include <cstring>
 #include <exception>
+#include <filesystem>
 #include <memory>
 #include <optional>
 #include <random>
@@ -356,6 +359,7 @@ struct SceneBase
         virtual int add_hyperplane_parallelotope(double, double, const float*, double, const double*, const double*) = 0;
         virtual int add_parallelotope(double, double, const float*, double, const double*, const double*) = 0;
         virtual int add_mesh_object(const float*, long, const int*, long, const double*, double, double, const float*, double) = 0;
+        virtual int add_mesh_file(const char*, const double*, double, double, const float*, double) = 0;
         virtual int add_mesh() = 0;
         virtual int add_parallelotope_light(int, const double*, const float*) = 0;
         virtual int add_ball_light(const double*, const double*, double, const float*) = 0;
@@ -508,6 +512,56 @@ public:
                 }
                 auto object = std::make_unique<ns::model::mesh::MeshObject<N>>(
                         ns::model::mesh::create_mesh_for_facets(p, f, /*write_log=*/false), m, "oracle");
+                {
+                        ns::model::mesh::Writing<N> writing(object.get());
+                        writing.set_metalness(metalness);
+                        writing.set_roughness(roughness);
+                        writing.set_alpha(alpha);
+                        writing.set_color(ns::color::Color(rgb[0], rgb[1], rgb[2]));
+                }
+                mesh_objects_.push_back(std::move(object));
+                return mesh_objects_.size() - 1;
+        }
+
+        // model::mesh::load (src/model/mesh/file.cpp:86-104) of an OBJ or STL file
+        // of this dimension, as one mesh object
+        int add_mesh_file(
+                const char* const path,
+                const double* const matrix,
+                const double metalness,
+                const double roughness,
+                const float* const rgb,
+                const double alpha) override
+        {
+                const std::filesystem::path file(path);
+                std::string ext = file.extension().string();
+                for (char& c : ext)
+                {
+                        c = static_cast<char>(std::tolower(static_cast<unsigned char>(c)));
+                }
+                const std::string n_text = N == 3 ? "" : std::to_string(N);
+                std::unique_ptr<ns::model::mesh::Mesh<N>> mesh;
+                if (ext == ".obj" + n_text || (N == 3 && ext == ".obj3"))
+                {
+                        mesh = ns::model::mesh::file::load_from_obj_file<N>(file, &progress_);
+                }
+                else if (ext == ".stl" + n_text || (N == 3 && ext == ".stl3"))
+                {
+                        mesh = ns::model::mesh::file::load_from_stl_file<N>(file, &progress_, false);
+                }
+                else
+                {
+                        throw std::runtime_error("not an OBJ or STL file of this dimension: " + file.string());
+                }
+                numerical::Matrix<N + 1, N + 1, double> m;
+                for (std::size_t r = 0; r < N + 1; ++r)
+                {
+                        for (std::size_t c = 0; c < N + 1; ++c)
+                        {
+                                m.row(r)[c] = matrix[r * (N + 1) + c];
+                        }
+                }
+                auto object = std::make_unique<ns::model::mesh::MeshObject<N>>(std::move(mesh), m, "oracle");
                 {
                         ns::model::mesh::Writing<N> writing(object.get());
                         writing.set_metalness(metalness);
@@ -1292,6 +1346,24 @@ int oracle_scene_add_mesh_object(
                 {
                         index = as_scene(scene)->add_mesh_object(
                                 points, n_points, facets, n_facets, matrix, metalness, roughness, rgb, alpha);
+                });
+        return r < 0 ? r : index;
+}
+
+int oracle_scene_add_mesh_file(
+        void* const scene,
+        const char* const path,
+        const double* const matrix,
+        const double metalness,
+        const double roughness,
+        const float* const rgb,
+        const double alpha)
+{
+        int index = -1;
+        const int r = guarded(
+                [&]
+                {
+                        index = as_scene(scene)->add_mesh_file(path, matrix, metalness, roughness, rgb, alpha);
                 });
         return r < 0 ? r : index;
 }

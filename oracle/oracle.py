@@ -48,6 +48,7 @@ def lib():
             "oracle_scene_add_parallelotope": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, _F, ctypes.c_double, _D, _D]),
             "oracle_scene_add_mesh_object": (ctypes.c_int, [_P, _F, ctypes.c_long, _I, ctypes.c_long, _D, ctypes.c_double, ctypes.c_double, _F, ctypes.c_double]),
             "oracle_scene_add_mesh": (ctypes.c_int, [_P]),
+            "oracle_scene_add_mesh_file": (ctypes.c_int, [_P, ctypes.c_char_p, _D, ctypes.c_double, ctypes.c_double, _F, ctypes.c_double]),
             "oracle_scene_add_parallelotope_light": (ctypes.c_int, [_P, ctypes.c_int, _D, _F]),
             "oracle_scene_add_ball_light": (ctypes.c_int, [_P, _D, _D, ctypes.c_double, _F]),
             "oracle_scene_set_perspective": (ctypes.c_int, [_P, _D, _D, _D, ctypes.c_double, _I]),
@@ -143,6 +144,11 @@ class Scene:
                     ptr(_d(s["org"]), _D), ptr(_d(s["vectors"]).reshape(-1), _D)))
             elif kind == "mesh":
                 for o in s["objects"]:
+                    if "file" in o:
+                        _check(L.oracle_scene_add_mesh_file(
+                            self.h, str(o["file"]).encode(), ptr(_d(o["matrix"]).reshape(-1), _D),
+                            o["metalness"], o["roughness"], ptr(_f(o["color"]), _F), o["alpha"]))
+                        continue
                     pts = _f(o["points"]).reshape(-1, n)
                     fac = _i(o["facets"]).reshape(-1, n)
                     _check(L.oracle_scene_add_mesh_object(
