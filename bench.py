@@ -63,7 +63,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--screen", type=int, default=None,
                    help="edge of the voxel screen (default: the workload's 64), for smaller profiling runs")
-    p.add_argument("--workload", default="cornell4d", choices=["cornell4d", "cornell3d", "sphere4d", "batch", "serve"],
+    p.add_argument("--workload", default="cornell4d", choices=["cornell4d", "cornell3d", "sphere4d", "batch", "serve", "meshfile"],
                    help="cornell4d: the headline benchmark; cornell3d, sphere4d: the other single-scene "
                         "workloads; batch: the mixed-scene batch, FP32 through the "
                         "job server against plain FP64 one job at a time; serve: Poisson arrivals of renders "
@@ -614,6 +614,62 @@ def run_arrivals(args, server, pool, built, arrivals, note):
     print(json.dumps(line), flush=True)
 
 
+def run_meshfile(args):
+    """Reading mesh files: a 4-space OBJ (with normals) and a binary STL of
+    the convex hull of 50,000 points on S^3 (about 340,000 facets), parsed by
+    nbpt_scene_add_mesh_file and by the reference's loaders (oracle), in
+    file MB per second.  The library's figure includes turning the file's
+    corners into the scene's points."""
+    import tempfile
+
+    sys.path.insert(0, str(ROOT / "tests"))
+    from mesh_file_writers import write_obj, write_stl_binary
+    from math_b200 import painter as P
+    from math_b200 import scenes
+    from oracle import oracle
+
+    p, f = scenes.convex_hull_mesh(scenes.sphere_points(4, 50000 if not args.small else 2000, 8))
+    p = np.asarray(p, np.float32)
+    results = {}
+    with tempfile.TemporaryDirectory() as d:
+        files = {"obj4": Path(d) / "m.obj4", "stl4": Path(d) / "m.stl4"}
+        write_obj(files["obj4"], p, f, normals=p / np.linalg.norm(p, axis=1, keepdims=True))
+        write_stl_binary(files["stl4"], p, f)
+        L = P.lib()
+        m = np.eye(5).reshape(-1)
+        rgb = np.array([0.5, 0.5, 0.5], np.float32)
+        for name, path in files.items():
+            size_mb = path.stat().st_size / 1e6
+            ours = []
+            ref = []
+            for _ in range(args.warmup + args.steps):
+                h = L.nbpt_scene_create(4, 0, 0)
+                t0 = time.perf_counter()
+                P._check(L.nbpt_scene_add_mesh_file(h, str(path).encode(), P._p(m, P._D), 0.0, 0.3,
+                                                    P._p(rgb, P._F), 1.0))
+                ours.append(time.perf_counter() - t0)
+                L.nbpt_scene_destroy(h)
+                if oracle.available():
+                    t0 = time.perf_counter()
+                    oracle.load_mesh_file(path, 4)
+                    ref.append(time.perf_counter() - t0)
+            ours = ours[args.warmup:]
+            ref = ref[args.warmup:]
+            results[name] = {"file_mb": size_mb, "facets": int(len(f)),
+                             "nbpt_mb_per_s": size_mb / float(np.median(ours)),
+                             "reference_mb_per_s": size_mb / float(np.median(ref)) if ref else None}
+    first = results["obj4"]
+    print(json.dumps({
+        "metric": "mesh_file_mb_per_second", "value": first["nbpt_mb_per_s"], "unit": "MB/s",
+        "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
+        "config": {"workload": "4-space OBJ with normals (value) and binary STL of a hull of 50,000 points on S^3",
+                   "files": results},
+        "cpu_baseline": {"value": first["reference_mb_per_s"], "unit": "MB/s", "cores": os.cpu_count(),
+                         "kind": "reference", "sample": "the reference's load_from_obj_file on the same file"},
+    }), flush=True)
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -627,6 +683,10 @@ def main():
     if args.workload == "serve":
         if rank == 0:
             run_serve(args)
+        return
+    if args.workload == "meshfile":
+        if rank == 0:
+            run_meshfile(args)
         return
     run_nbpt(args, rank, world, local)
 

@@ -16,6 +16,7 @@
 #include <string>
 #include <string_view>
 #include <unordered_map>
+#include <thread>
 #include <vector>
 
 namespace nbpt::host
@@ -56,12 +57,39 @@ bool is_print(const char c)
         return c >= '\x20' && c <= '\x7e';
 }
 
-// strtof with the reference's checks (src/com/read.h): a number must be
-// read, and it must be finite
+// What strtof reads (leading white space, an optional sign, decimal,
+// hexadecimal, infinity or NaN forms), with the reference's checks
+// (src/com/read.h): a number must be read, and it must be finite.  Decimal
+// numbers go through std::from_chars, which rounds as strtof does.
 bool read_float(const char*& s, float& out)
 {
-        char* end = nullptr;
-        const float v = std::strtof(s, &end);
+        const char* p = s;
+        while (*p && is_space(*p))
+        {
+                ++p;
+        }
+        const char* q = (*p == '+' && p[1] != '+' && p[1] != '-') ? p + 1 : p;
+        // the characters a number can be made of; the text ends with a zero
+        const char* line_end = q;
+        while (std::isalnum(static_cast<unsigned char>(*line_end)) || *line_end == '.' || *line_end == '+' ||
+               *line_end == '-' || *line_end == '(' || *line_end == ')' || *line_end == '_')
+        {
+                ++line_end;
+        }
+        float v = 0;
+        const auto [ptr, ec] = std::from_chars(q, line_end, v);
+        const bool hex = ptr < line_end && (*ptr == 'x' || *ptr == 'X');
+        const char* end = ptr;
+        if (hex || ec == std::errc::result_out_of_range || (ec != std::errc{} && ptr != q))
+        {
+                char* e = nullptr;
+                v = std::strtof(s, &e);
+                end = e;
+        }
+        else if (ec != std::errc{})
+        {
+                end = s;
+        }
         if (end <= s)
         {
                 return false;
@@ -286,47 +314,60 @@ void read_color(const char* s, std::array<float, 3>& rgb)
         }
 }
 
-void read_obj(const std::filesystem::path& path, const int n, MeshFile& m)
+enum class LineKind : unsigned char
 {
-        const int max_corners = (n == 3 ? 5 : 1) + n - 1;
-        std::vector<int> texcoord_index; // per facet corner, -1 without
-        int texcoord_count = 0;
-        int normal_count = 0;
-        int material = -1;
-        std::map<std::string, int, std::less<>> material_index; // materials still to find in the libraries
-        std::vector<std::string> material_names;
-        std::vector<std::filesystem::path> libraries;
-        std::set<std::filesystem::path> unique_libraries;
+        NONE,
+        V,
+        VT,
+        VN,
+        F,
+        USEMTL,
+        MTLLIB
+};
 
-        const Lines lines(read_bytes(path));
+// The lines of one part of an OBJ file, parsed: what does not depend on the
+// lines before (numbers, normalised normals, facet corners) is read here, in
+// parallel with the other parts.
+struct ObjPart final
+{
+        std::vector<LineKind> kind;
+        std::vector<float> values;               // v and vn payloads, n each
+        std::vector<unsigned char> corner_count; // per f line
+        std::vector<Corner> corners;
+        std::size_t error_line = static_cast<std::size_t>(-1);
+        std::string error;
+};
+
+void parse_obj_lines(const Lines& lines, const std::size_t begin, const std::size_t end, const int n,
+                     const int max_corners, ObjPart& part)
+{
         std::vector<Corner> corners(max_corners);
-        for (std::size_t i = 0; i < lines.size(); ++i)
+        std::vector<float> v(n);
+        for (std::size_t i = begin; i < end; ++i)
         {
                 const Split s = split(lines.line(i));
                 try
                 {
                         if (s.first == "v")
                         {
-                                const std::size_t base = m.vertices.size();
-                                m.vertices.resize(base + n);
                                 const char* p = s.rest_b;
-                                read_floats(p, &m.vertices[base], n);
+                                read_floats(p, v.data(), n);
+                                part.values.insert(part.values.end(), v.begin(), v.end());
+                                part.kind.push_back(LineKind::V);
                         }
                         else if (s.first == "vt")
                         {
-                                std::vector<float> t(n - 1);
                                 const char* p = s.rest_b;
-                                read_floats(p, t.data(), n - 1);
+                                read_floats(p, v.data(), n - 1);
                                 float w = 0;
                                 if (read_float(p, w) && !(w == 0))
                                 {
                                         fail(std::to_string(n) + "-dimensional textures are not supported");
                                 }
-                                ++texcoord_count;
+                                part.kind.push_back(LineKind::VT);
                         }
                         else if (s.first == "vn")
                         {
-                                std::vector<float> v(n);
                                 const char* p = s.rest_b;
                                 read_floats(p, v.data(), n);
                                 float sq = v[0] * v[0];
@@ -345,8 +386,8 @@ void read_obj(const std::filesystem::path& path, const int n, MeshFile& m)
                                 {
                                         std::fill(v.begin(), v.end(), 0.0f);
                                 }
-                                m.normals.insert(m.normals.end(), v.begin(), v.end());
-                                ++normal_count;
+                                part.values.insert(part.values.end(), v.begin(), v.end());
+                                part.kind.push_back(LineKind::VN);
                         }
                         else if (s.first == "f")
                         {
@@ -390,14 +431,112 @@ void read_obj(const std::filesystem::path& path, const int n, MeshFile& m)
                                 {
                                         fail("Inconsistent facet normal indices");
                                 }
+                                part.corner_count.push_back(static_cast<unsigned char>(count));
+                                part.corners.insert(part.corners.end(), corners.begin(), corners.begin() + count);
+                                part.kind.push_back(LineKind::F);
+                        }
+                        else if (s.first == "usemtl")
+                        {
+                                read_name("material", s.rest_b, s.rest_e);
+                                part.kind.push_back(LineKind::USEMTL);
+                        }
+                        else if (s.first == "mtllib")
+                        {
+                                part.kind.push_back(LineKind::MTLLIB);
+                        }
+                        else
+                        {
+                                part.kind.push_back(LineKind::NONE);
+                        }
+                }
+                catch (const std::exception& e)
+                {
+                        part.error_line = i;
+                        part.error = "Line " + std::to_string(i) + ": " + std::string(s.first) + " " +
+                                     std::string(s.rest_b, s.rest_e) + "\n" + e.what();
+                        return;
+                }
+        }
+}
+
+void read_obj(const std::filesystem::path& path, const int n, MeshFile& m)
+{
+        const int max_corners = (n == 3 ? 5 : 1) + n - 1;
+        std::vector<int> texcoord_index; // per facet corner, -1 without
+        int texcoord_count = 0;
+        int normal_count = 0;
+        int material = -1;
+        std::map<std::string, int, std::less<>> material_index; // materials still to find in the libraries
+        std::vector<std::string> material_names;
+        std::vector<std::filesystem::path> libraries;
+        std::set<std::filesystem::path> unique_libraries;
+
+        const Lines lines(read_bytes(path));
+
+        // parse the lines in parts on the host threads, then apply them in order
+        const std::size_t line_count = lines.size();
+        const unsigned threads = static_cast<unsigned>(std::max<std::size_t>(
+                1, std::min<std::size_t>(std::max(1u, std::thread::hardware_concurrency()), line_count / 4096)));
+        std::vector<ObjPart> parts(threads);
+        {
+                std::vector<std::thread> pool;
+                const std::size_t step = (line_count + threads - 1) / threads;
+                for (unsigned t = 1; t < threads; ++t)
+                {
+                        pool.emplace_back(
+                                [&, t]
+                                {
+                                        parse_obj_lines(lines, std::min(line_count, t * step),
+                                                        std::min(line_count, (t + 1) * step), n, max_corners, parts[t]);
+                                });
+                }
+                parse_obj_lines(lines, 0, std::min(line_count, step), n, max_corners, parts[0]);
+                for (std::thread& th : pool)
+                {
+                        th.join();
+                }
+        }
+
+        std::size_t i = 0;
+        for (const ObjPart& part : parts)
+        {
+                std::size_t value = 0;
+                std::size_t facet_line = 0;
+                std::size_t corner = 0;
+                for (const LineKind kind : part.kind)
+                {
+                        const std::size_t line = i++;
+                        switch (kind)
+                        {
+                        case LineKind::NONE:
+                                break;
+                        case LineKind::V:
+                                m.vertices.insert(m.vertices.end(), part.values.begin() + value,
+                                                  part.values.begin() + value + n);
+                                value += n;
+                                break;
+                        case LineKind::VT:
+                                ++texcoord_count;
+                                break;
+                        case LineKind::VN:
+                                m.normals.insert(m.normals.end(), part.values.begin() + value,
+                                                 part.values.begin() + value + n);
+                                value += n;
+                                ++normal_count;
+                                break;
+                        case LineKind::F:
+                        {
+                                const int count = part.corner_count[facet_line++];
+                                const Corner* const c0 = &part.corners[corner];
+                                corner += count;
                                 const int vertex_count = static_cast<int>(m.vertices.size() / n);
-                                const bool normals = with_n > 0;
+                                const bool normals = c0[0].normal != 0;
                                 // a fan around the first corner
                                 for (int f = 0; f + n - 1 < count; ++f)
                                 {
                                         for (int k = 0; k < n; ++k)
                                         {
-                                                const Corner& c = corners[k == 0 ? 0 : f + k];
+                                                const Corner& c = c0[k == 0 ? 0 : f + k];
                                                 const int v = c.vertex > 0 ? c.vertex - 1 : vertex_count + c.vertex;
                                                 m.facet_vertices.push_back(v);
                                                 m.facet_normals.push_back(absolute_index(c.normal, normal_count));
@@ -406,9 +545,11 @@ void read_obj(const std::filesystem::path& path, const int n, MeshFile& m)
                                         m.has_normal.push_back(normals ? 1 : 0);
                                         m.facet_material.push_back(material);
                                 }
+                                break;
                         }
-                        else if (s.first == "usemtl")
+                        case LineKind::USEMTL:
                         {
+                                const Split s = split(lines.line(line));
                                 const std::string name{read_name("material", s.rest_b, s.rest_e)};
                                 const auto it = std::find(material_names.begin(), material_names.end(), name);
                                 if (it != material_names.end())
@@ -422,9 +563,11 @@ void read_obj(const std::filesystem::path& path, const int n, MeshFile& m)
                                         material = static_cast<int>(material_names.size()) - 1;
                                         material_index.emplace(name, material);
                                 }
+                                break;
                         }
-                        else if (s.first == "mtllib")
+                        case LineKind::MTLLIB:
                         {
+                                const Split s = split(lines.line(line));
                                 const char* b = s.rest_b;
                                 bool found = false;
                                 while (true)
@@ -452,14 +595,16 @@ void read_obj(const std::filesystem::path& path, const int n, MeshFile& m)
                                 }
                                 if (!found)
                                 {
-                                        fail("Library name not found");
+                                        fail("Line " + std::to_string(line) + ": mtllib " + std::string(s.rest_b, s.rest_e) +
+                                             "\nLibrary name not found");
                                 }
+                                break;
+                        }
                         }
                 }
-                catch (const std::exception& e)
+                if (!part.error.empty())
                 {
-                        fail("Line " + std::to_string(i) + ": " + std::string(s.first) + " " +
-                             std::string(s.rest_b, s.rest_e) + "\n" + e.what());
+                        fail(part.error);
                 }
         }
         if (m.has_normal.empty())

@@ -947,26 +947,53 @@ public:
                 o.file = true;
                 const std::size_t facet_count = file.has_normal.size();
                 const long long normal_slots = static_cast<long long>(file.normals.size() / N) + 1;
-                std::unordered_map<long long, int> corner;
+                // the first corner of each vertex in a table, the others in a map
+                const std::size_t vertex_count = file.vertices.size() / N;
+                std::vector<int> first_normal(vertex_count, -2);
+                std::vector<int> first_id(vertex_count, -1);
+                std::unordered_map<long long, int> other;
                 o.facets.resize(facet_count * N);
+                const auto new_point = [&](const int v, const int nm)
+                {
+                        const int id = static_cast<int>(o.points.size() / N);
+                        for (int d = 0; d < N; ++d)
+                        {
+                                o.points.push_back(file.vertices[static_cast<std::size_t>(v) * N + d]);
+                                o.normals.push_back(nm < 0 ? 0.0f : file.normals[static_cast<std::size_t>(nm) * N + d]);
+                        }
+                        return id;
+                };
                 for (std::size_t f = 0; f < facet_count; ++f)
                 {
                         for (int k = 0; k < N; ++k)
                         {
                                 const int v = file.facet_vertices[f * N + k];
                                 const int nm = file.has_normal[f] ? file.facet_normals[f * N + k] : -1;
-                                const long long key = static_cast<long long>(v) * normal_slots + (nm + 1);
-                                auto [it, inserted] = corner.emplace(key, static_cast<int>(o.points.size() / N));
-                                if (inserted)
+                                int id;
+                                if (first_normal[v] == -2)
                                 {
-                                        for (int d = 0; d < N; ++d)
+                                        first_normal[v] = nm;
+                                        id = first_id[v] = new_point(v, nm);
+                                }
+                                else if (first_normal[v] == nm)
+                                {
+                                        id = first_id[v];
+                                }
+                                else
+                                {
+                                        const long long key = static_cast<long long>(v) * normal_slots + (nm + 1);
+                                        const auto it = other.find(key);
+                                        if (it != other.end())
                                         {
-                                                o.points.push_back(file.vertices[static_cast<std::size_t>(v) * N + d]);
-                                                o.normals.push_back(
-                                                        nm < 0 ? 0.0f : file.normals[static_cast<std::size_t>(nm) * N + d]);
+                                                id = it->second;
+                                        }
+                                        else
+                                        {
+                                                id = new_point(v, nm);
+                                                other.emplace(key, id);
                                         }
                                 }
-                                o.facets[f * N + k] = it->second;
+                                o.facets[f * N + k] = id;
                         }
                 }
                 o.flat.resize(facet_count);

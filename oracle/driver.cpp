@@ -1368,6 +1368,43 @@ int oracle_scene_add_mesh_file(
         return r < 0 ? r : index;
 }
 
+// model::mesh::file::load_from_obj_file / load_from_stl_file alone:
+// counts[0] vertices, [1] normals, [2] facets
+int oracle_load_mesh_file(const char* const path, const int n, const int stl, long long* const counts)
+{
+        return guarded(
+                [&]
+                {
+                        ns::progress::Ratio progress(nullptr);
+                        const std::filesystem::path file(path);
+                        const auto fill = [&](const auto& mesh)
+                        {
+                                counts[0] = mesh->vertices.size();
+                                counts[1] = mesh->normals.size();
+                                counts[2] = mesh->facets.size();
+                        };
+                        if (n == 3)
+                        {
+                                stl ? fill(ns::model::mesh::file::load_from_stl_file<3>(file, &progress, false))
+                                    : fill(ns::model::mesh::file::load_from_obj_file<3>(file, &progress));
+                        }
+                        else if (n == 4)
+                        {
+                                stl ? fill(ns::model::mesh::file::load_from_stl_file<4>(file, &progress, false))
+                                    : fill(ns::model::mesh::file::load_from_obj_file<4>(file, &progress));
+                        }
+                        else if (n == 5)
+                        {
+                                stl ? fill(ns::model::mesh::file::load_from_stl_file<5>(file, &progress, false))
+                                    : fill(ns::model::mesh::file::load_from_obj_file<5>(file, &progress));
+                        }
+                        else
+                        {
+                                throw std::runtime_error("dimension must be 3, 4 or 5");
+                        }
+                });
+}
+
 int oracle_scene_add_mesh(void* const scene)
 {
         int index = -1;

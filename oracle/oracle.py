@@ -49,6 +49,7 @@ def lib():
             "oracle_scene_add_mesh_object": (ctypes.c_int, [_P, _F, ctypes.c_long, _I, ctypes.c_long, _D, ctypes.c_double, ctypes.c_double, _F, ctypes.c_double]),
             "oracle_scene_add_mesh": (ctypes.c_int, [_P]),
             "oracle_scene_add_mesh_file": (ctypes.c_int, [_P, ctypes.c_char_p, _D, ctypes.c_double, ctypes.c_double, _F, ctypes.c_double]),
+            "oracle_load_mesh_file": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _L]),
             "oracle_scene_add_parallelotope_light": (ctypes.c_int, [_P, ctypes.c_int, _D, _F]),
             "oracle_scene_add_ball_light": (ctypes.c_int, [_P, _D, _D, ctypes.c_double, _F]),
             "oracle_scene_set_perspective": (ctypes.c_int, [_P, _D, _D, _D, ctypes.c_double, _I]),
@@ -352,3 +353,12 @@ def constants(n: int, double: bool) -> np.ndarray:
     out = np.zeros(8)
     _check(lib().oracle_constants(n, 1 if double else 0, ptr(out, _D)))
     return out
+
+
+def load_mesh_file(path, n: int) -> dict:
+    """The reference's own OBJ / STL loader on `path`: counts of the mesh it
+    reads (vertices, normals, facets)."""
+    counts = np.zeros(3, np.int64)
+    stl = 1 if ".stl" in str(path).lower() else 0
+    _check(lib().oracle_load_mesh_file(str(path).encode(), n, stl, ptr(counts, _L)))
+    return {"vertices": int(counts[0]), "normals": int(counts[1]), "facets": int(counts[2])}
