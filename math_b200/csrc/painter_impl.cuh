@@ -399,43 +399,59 @@ std::vector<float> vertex_normals(const std::vector<float>& points, const std::v
                                 }
                         }
                 });
-        std::vector<Vec<N, double>> sum(vcount, Vec<N, double>::filled(0));
-        std::vector<Vec<N, double>> reference(vcount, Vec<N, double>::filled(0));
-        std::vector<char> has_reference(vcount, 0);
-        for (std::size_t f = 0; f < fcount; ++f)
+        // the corners of every vertex in facet order, then each vertex's sum in
+        // that order (the vertices in parallel)
+        std::vector<std::size_t> first(vcount + 1, 0);
+        for (std::size_t c = 0; c < fcount * N; ++c)
         {
-                for (int k = 0; k < N; ++k)
+                ++first[facets[c] + 1];
+        }
+        for (std::size_t v = 0; v < vcount; ++v)
+        {
+                first[v + 1] += first[v];
+        }
+        std::vector<std::size_t> corners(fcount * N);
+        {
+                std::vector<std::size_t> fill(first.begin(), first.end() - 1);
+                for (std::size_t c = 0; c < fcount * N; ++c)
                 {
-                        const int v = facets[f * N + k];
-                        if (!has_reference[v])
-                        {
-                                reference[v] = fn[f];
-                                has_reference[v] = 1;
-                        }
-                        const Vec<N, double> wn = fn[f] * weight[f * N + k];
-                        if (dot(fn[f], reference[v]) >= 0)
-                        {
-                                sum[v] = sum[v] + wn;
-                        }
-                        else
-                        {
-                                sum[v] = sum[v] - wn;
-                        }
+                        corners[fill[facets[c]]++] = c;
                 }
         }
         std::vector<float> out(vcount * N, 0.0f);
-        for (std::size_t v = 0; v < vcount; ++v)
-        {
-                if (!has_reference[v])
+        ranges(
+                parallel, vcount,
+                [&](const std::size_t begin, const std::size_t end)
                 {
-                        continue;
-                }
-                const Vec<N, double> n = sum[v].normalized();
-                for (int d = 0; d < N; ++d)
-                {
-                        out[v * N + d] = static_cast<float>(n[d]);
-                }
-        }
+                        for (std::size_t v = begin; v < end; ++v)
+                        {
+                                if (first[v] == first[v + 1])
+                                {
+                                        continue;
+                                }
+                                const Vec<N, double> reference = fn[corners[first[v]] / N];
+                                Vec<N, double> sum = Vec<N, double>::filled(0);
+                                for (std::size_t i = first[v]; i < first[v + 1]; ++i)
+                                {
+                                        const std::size_t c = corners[i];
+                                        const Vec<N, double>& n = fn[c / N];
+                                        const Vec<N, double> wn = n * weight[c];
+                                        if (dot(n, reference) >= 0)
+                                        {
+                                                sum = sum + wn;
+                                        }
+                                        else
+                                        {
+                                                sum = sum - wn;
+                                        }
+                                }
+                                const Vec<N, double> n = sum.normalized();
+                                for (int d = 0; d < N; ++d)
+                                {
+                                        out[v * N + d] = static_cast<float>(n[d]);
+                                }
+                        }
+                });
         return out;
 }
 
