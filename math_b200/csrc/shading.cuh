@@ -60,6 +60,23 @@ NBPT_HD void uniform_in_ball(Pcg& g, Vec<M, T>& v, T& length_square)
         }
 }
 
+// Cosine-weighted direction about `normal` from a point `v` drawn uniformly
+// in the unit (N-1)-ball, given the orthonormal complement of `normal`
+// (sphere_cosine.h:41-80).
+template <int N, typename T>
+NBPT_HD Vec<N, T> cosine_from_ball(const Vec<N, T>& normal, const Vec<N, T>* basis, const Vec<N - 1, T>& v,
+                                   const T length_square)
+{
+        const T h = sqrt_value(1 - length_square);
+        Vec<N, T> r = normal * h;
+#pragma unroll
+        for (int i = 0; i < N - 1; ++i)
+        {
+                r.multiply_add(basis[i], v[i]);
+        }
+        return r;
+}
+
 // Cosine-weighted direction about `normal` (sphere_cosine.h:41-80).
 template <int N, typename T>
 NBPT_HD Vec<N, T> cosine_on_hemisphere(Pcg& g, const Vec<N, T>& normal)
@@ -252,9 +269,11 @@ NBPT_HD void ggx_basis(const Vec<N, T>& vh, Vec<N, T>* res)
         }
 }
 
-// Visible-normal sample in the local frame (ggx.h:173-233).
+// Visible-normal sample in the local frame (ggx.h:173-233), from the point
+// `t` drawn uniformly in the unit (N-1)-ball (the sample's only random draw)
+// and its squared length.
 template <int N, typename T>
-NBPT_HD Vec<N, T> ggx_vn(Pcg& g, const Vec<N, T>& ve, const T alpha)
+NBPT_HD Vec<N, T> ggx_vn_from_ball(const Vec<N, T>& ve, const T alpha, Vec<N - 1, T> t, const T length_square)
 {
         Vec<N, T> t0;
 #pragma unroll
@@ -268,9 +287,7 @@ NBPT_HD Vec<N, T> ggx_vn(Pcg& g, const Vec<N, T>& ve, const T alpha)
         Vec<N, T> basis[N - 1];
         ggx_basis(vh, basis);
 
-        Vec<N - 1, T> t;
-        T length_square;
-        uniform_in_ball<N - 1>(g, t, length_square);
+        static_cast<void>(length_square);
         const T s = T(0.5) * (1 + vh[N - 1]);
         T sum = 0;
 #pragma unroll
@@ -298,11 +315,12 @@ NBPT_HD Vec<N, T> ggx_vn(Pcg& g, const Vec<N, T>& ve, const T alpha)
         return ne.normalized();
 }
 
+// the visible-normal half vector about `normal` (ggx.h:235-260), given the
+// orthonormal complement of `normal` and the ball point of ggx_vn_from_ball
 template <int N, typename T>
-NBPT_HD Vec<N, T> ggx_visible_normals_h(Pcg& g, const Vec<N, T>& normal, const Vec<N, T>& v, const T alpha)
+NBPT_HD Vec<N, T> ggx_visible_normals_h(const Vec<N, T>& normal, const Vec<N, T>* basis, const Vec<N, T>& v,
+                                        const T alpha, const Vec<N - 1, T>& ball, const T ball_length_square)
 {
-        Vec<N, T> basis[N - 1];
-        orthogonal_complement_of_unit_vector(normal, basis);
         Vec<N, T> ve;
 #pragma unroll
         for (int i = 0; i < N - 1; ++i)
@@ -310,7 +328,7 @@ NBPT_HD Vec<N, T> ggx_visible_normals_h(Pcg& g, const Vec<N, T>& normal, const V
                 ve[i] = dot(v, basis[i]);
         }
         ve[N - 1] = dot(v, normal);
-        const Vec<N, T> ne = ggx_vn(g, ve, alpha);
+        const Vec<N, T> ne = ggx_vn_from_ball(ve, alpha, ball, ball_length_square);
         Vec<N, T> r = normal * ne[N - 1];
 #pragma unroll
         for (int i = 0; i < N - 1; ++i)
@@ -560,14 +578,24 @@ NBPT_HD_CALL BrdfSample<N, C, T> brdf_sample(
         const T alpha = square(roughness);
         Vec<N, T> l;
         Vec<N, T> h;
-        if (bernoulli_half(g))
+        // Both ways draw one point in the unit (N-1)-ball after the choice
+        // and work in the complement of n (ggx.h:235-260,
+        // sphere_cosine.h:41-80), so the complement and the draw are shared
+        // and only the arithmetic between them diverges.
+        const bool ggx = bernoulli_half(g);
+        Vec<N, T> basis[N - 1];
+        orthogonal_complement_of_unit_vector(n, basis);
+        Vec<N - 1, T> ball;
+        T ball_length_square;
+        uniform_in_ball<N - 1>(g, ball, ball_length_square);
+        if (ggx)
         {
-                h = ggx_visible_normals_h(g, n, v, alpha);
+                h = ggx_visible_normals_h(n, basis, v, alpha, ball, ball_length_square);
                 l = reflect_vn(v, h);
         }
         else
         {
-                l = cosine_on_hemisphere(g, n);
+                l = cosine_from_ball(n, basis, ball, ball_length_square);
                 h = (v + l).normalized();
         }
         const T pdf = pdf_ggx_cosine(sc, alpha, n, v, l, h);
