@@ -977,6 +977,267 @@ __global__ void __launch_bounds__(128) accumulate_warp_kernel(
         }
 }
 
+// The same merge with the scalar work of the neighbours done side by side,
+// for up to 32 samples per pixel: one warp per receiving pixel; first the
+// weights of every neighbour's samples (lanes over samples), then every
+// neighbour's group ordered on its own lane, then the groups merged in
+// increasing pixel index with the channels across the lanes, as
+// accumulate_warp_kernel merges them.
+inline constexpr int SMALL_GROUP = 32;
+
+template <int N, typename T, int C>
+__global__ void __launch_bounds__(128) accumulate_warp_small_kernel(
+        const Screen<N> screen,
+        const long long pixel_count,
+        const int spp,
+        const T* __restrict__ points,
+        const float* __restrict__ colors,
+        const float* __restrict__ lum,
+        const unsigned char* __restrict__ valid,
+        const T alpha,
+        const T exp_radius,
+        PixelState<C>* __restrict__ state)
+{
+        static_assert(C % 32 == 0);
+        constexpr int K = C / 32;
+        constexpr int WARPS = 4;
+        static_assert(N <= 4, "the shared-memory tables hold 3^(N-1) <= 27 neighbours");
+        constexpr int NB = N == 3 ? 9 : 27;
+        __shared__ float s_weight[WARPS][NB][SMALL_GROUP];
+        __shared__ float s_contribution[WARPS][NB][SMALL_GROUP];
+        __shared__ unsigned char s_kind[WARPS][NB][SMALL_GROUP]; // 0 none, 1 colour, 2 background
+        __shared__ unsigned char s_order[WARPS][NB][SMALL_GROUP];
+        __shared__ unsigned char s_order_bg[WARPS][NB][SMALL_GROUP];
+        __shared__ int s_counts[WARPS][NB][2];
+        __shared__ int s_order_int[WARPS][SMALL_GROUP];
+        __shared__ float s_sorted[WARPS][SMALL_GROUP];
+
+        const int warp = threadIdx.x / 32;
+        const int lane = threadIdx.x & 31;
+        const long long t = blockIdx.x * static_cast<long long>(WARPS) + warp;
+        if (t >= pixel_count)
+        {
+                return; // the whole warp
+        }
+
+        int tc[N - 1];
+        {
+                long long rest = t;
+#pragma unroll
+                for (int d = 0; d < N - 1; ++d)
+                {
+                        tc[d] = static_cast<int>(rest % screen.size[d]);
+                        rest /= screen.size[d];
+                }
+        }
+        // neighbour nb's pixel, or -1 outside the screen
+        const auto neighbour = [&](const int nb, int* pc) -> long long
+        {
+                int rest = nb;
+                bool inside = true;
+#pragma unroll
+                for (int d = 0; d < N - 1; ++d)
+                {
+                        pc[d] = tc[d] + (rest % 3) - 1;
+                        rest /= 3;
+                        inside = inside && pc[d] >= 0 && pc[d] < screen.size[d];
+                }
+                if (!inside)
+                {
+                        return -1;
+                }
+                long long p = 0;
+#pragma unroll
+                for (int d = N - 2; d >= 0; --d)
+                {
+                        p = p * screen.size[d] + pc[d];
+                }
+                return p;
+        };
+
+        // weights and kinds (pixel_filter.h:57-69), lanes over the samples
+        for (int nb = 0; nb < NB; ++nb)
+        {
+                int pc[N - 1];
+                const long long p = neighbour(nb, pc);
+                if (p < 0 || lane >= spp)
+                {
+                        continue;
+                }
+                const int j = lane;
+                const long long sidx = p * spp + j;
+                const T x0 = (static_cast<T>(tc[0] - pc[0]) + T(0.5)) - points[sidx * (N - 1)];
+                T weight = max_value(T(0), exp(alpha * x0 * x0) - exp_radius);
+#pragma unroll
+                for (int d = 1; d < N - 1; ++d)
+                {
+                        const T x = (static_cast<T>(tc[d] - pc[d]) + T(0.5)) - points[sidx * (N - 1) + d];
+                        weight *= max_value(T(0), exp(alpha * x * x) - exp_radius);
+                }
+                unsigned char k = 0;
+                if (weight > 0)
+                {
+                        const float wf = static_cast<float>(weight);
+                        s_weight[warp][nb][j] = wf;
+                        if (valid[sidx])
+                        {
+                                s_contribution[warp][nb][j] = wf * lum[sidx];
+                                k = 1;
+                        }
+                        else
+                        {
+                                k = 2;
+                        }
+                }
+                s_kind[warp][nb][j] = k;
+        }
+        __syncwarp();
+
+        // every neighbour's group ordered on its own lane (com/select.h:28-47,
+        // samples/com/sort.h:26-46)
+        if (lane < NB)
+        {
+                const int nb = lane;
+                int pc[N - 1];
+                const long long p = neighbour(nb, pc);
+                int nc = 0;
+                int nbg = 0;
+                if (p >= 0)
+                {
+                        int order[SMALL_GROUP];
+                        int order_bg[SMALL_GROUP];
+                        for (int j = 0; j < spp; ++j)
+                        {
+                                const unsigned char k = s_kind[warp][nb][j];
+                                if (k == 1)
+                                {
+                                        order[nc++] = j;
+                                }
+                                else if (k == 2)
+                                {
+                                        order_bg[nbg++] = j;
+                                }
+                        }
+                        const float* const contribution = s_contribution[warp][nb];
+                        const float* const w = s_weight[warp][nb];
+                        order_group(order, nc, [&](const int i) { return contribution[i]; });
+                        order_group(order_bg, nbg, [&](const int i) { return w[i]; });
+                        for (int k = 0; k < nc; ++k)
+                        {
+                                s_order[warp][nb][k] = static_cast<unsigned char>(order[k]);
+                        }
+                        for (int k = 0; k < nbg; ++k)
+                        {
+                                s_order_bg[warp][nb][k] = static_cast<unsigned char>(order_bg[k]);
+                        }
+                }
+                s_counts[warp][nb][0] = nc;
+                s_counts[warp][nb][1] = nbg;
+        }
+        __syncwarp();
+
+        // this lane's channels of the pixel state, and its scalars
+        PixelState<C>& global = state[t];
+        ColorSet<K> cs;
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+        {
+                cs.color_sum[k] = global.color.color_sum[lane + 32 * k];
+#pragma unroll
+                for (int j = 0; j < HELD_OUT; ++j)
+                {
+                        cs.colors[j][k] = global.color.colors[j][lane + 32 * k];
+                }
+        }
+        cs.weight_sum = global.color.weight_sum;
+#pragma unroll
+        for (int j = 0; j < HELD_OUT; ++j)
+        {
+                cs.weights[j] = global.color.weights[j];
+                cs.contributions[j] = global.color.contributions[j];
+        }
+        cs.count = global.color.count;
+        cs.full = global.color.full;
+        BackgroundSet bs = global.background;
+
+        int* const order = s_order_int[warp];
+        float* const sorted = s_sorted[warp];
+        for (int nb = 0; nb < NB; ++nb)
+        {
+                const int nc = s_counts[warp][nb][0];
+                const int nbg = s_counts[warp][nb][1];
+                if (nc == 0 && nbg == 0)
+                {
+                        continue;
+                }
+                int pc[N - 1];
+                const long long p = neighbour(nb, pc);
+                const float* const w = s_weight[warp][nb];
+                if (lane < nc)
+                {
+                        order[lane] = s_order[warp][nb][lane];
+                }
+                if (lane < nbg)
+                {
+                        sorted[lane] = w[s_order_bg[warp][nb][lane]];
+                }
+                __syncwarp();
+                if (nc > 0)
+                {
+                        const ColorGroup<K> g{colors + p * spp * C, w, s_contribution[warp][nb], order, nc, C, 32, lane};
+                        float g_sum[K];
+                        float g_wsum = 0;
+#pragma unroll
+                        for (int k = 0; k < K; ++k)
+                        {
+                                g_sum[k] = 0;
+                        }
+                        const bool g_full = nc > HELD_OUT;
+                        if (g_full)
+                        {
+                                for (int k = HELD_OUT / 2; k < nc - HELD_OUT / 2; ++k)
+                                {
+#pragma unroll
+                                        for (int c = 0; c < K; ++c)
+                                        {
+                                                g_sum[c] += g.color(k, c);
+                                        }
+                                        g_wsum += w[order[k]];
+                                }
+                        }
+                        merge_color_group(cs, g, g_sum, g_wsum, g_full);
+                }
+                if (nbg > 0)
+                {
+                        merge_background_group(bs, sorted, nbg);
+                }
+                __syncwarp();
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+        {
+                global.color.color_sum[lane + 32 * k] = cs.color_sum[k];
+#pragma unroll
+                for (int j = 0; j < HELD_OUT; ++j)
+                {
+                        global.color.colors[j][lane + 32 * k] = cs.colors[j][k];
+                }
+        }
+        if (lane == 0)
+        {
+                global.color.weight_sum = cs.weight_sum;
+#pragma unroll
+                for (int j = 0; j < HELD_OUT; ++j)
+                {
+                        global.color.weights[j] = cs.weights[j];
+                        global.color.contributions[j] = cs.contributions[j];
+                }
+                global.color.count = cs.count;
+                global.color.full = cs.full;
+                global.background = bs;
+        }
+}
+
 // ---------------------------------------------------------------------------
 // image resolve: merge_color / merge_color_alpha (samples/merge_color.cpp:45-177)
 // and the RGB of the colour (src/color/color.h rgb32).  The background is

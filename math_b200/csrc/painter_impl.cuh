@@ -2341,7 +2341,23 @@ public:
                         const T width = radius / T(2.5);
                         const T alpha = -1 / (2 * width * width);
                         const T exp_radius = std::exp(alpha * radius * radius);
-                        if constexpr (C % 32 == 0)
+                        if constexpr (C % 32 == 0 && N <= 4)
+                        {
+                                if (spp_ <= SMALL_GROUP)
+                                {
+                                        accumulate_warp_small_kernel<N, T, C>
+                                                <<<blocks_for(pixels_ * 32, 128), 128, 0, stream_>>>(
+                                                        screen, pixels_, spp_, points_.get(), colors_.get(), lum_.get(),
+                                                        valid_.get(), alpha, exp_radius, state_.get());
+                                }
+                                else
+                                {
+                                        accumulate_warp_kernel<N, T, C><<<blocks_for(pixels_ * 32, 128), 128, 0, stream_>>>(
+                                                screen, pixels_, spp_, points_.get(), colors_.get(), lum_.get(),
+                                                valid_.get(), alpha, exp_radius, state_.get());
+                                }
+                        }
+                        else if constexpr (C % 32 == 0)
                         {
                                 accumulate_warp_kernel<N, T, C><<<blocks_for(pixels_ * 32, 128), 128, 0, stream_>>>(
                                         screen, pixels_, spp_, points_.get(), colors_.get(), lum_.get(), valid_.get(),
