@@ -82,6 +82,7 @@ Server::Server(const int max_jobs, const long long memory_budget)
                 }
                 budget_ = static_cast<long long>(free * 0.8);
         }
+        initial_budget_ = budget_;
         {
                 // registered after the CUDA runtime initialised above, so it
                 // runs before the runtime's own exit handlers
@@ -312,6 +313,7 @@ void Server::finish_locked(Job& job, const JobState state, const std::string& er
         job.info.error = error;
         job.info.finished = now();
         used_ -= job.info.footprint;
+        budget_ = initial_budget_; // memory freed: admit by the estimate again
         if (job.done)
         {
                 cudaSetDevice(job.device);
@@ -364,7 +366,40 @@ void Server::run()
                                 if (!j->painter)
                                 {
                                         // a render created at admission
-                                        j->owned = j->scene->create_painter(j->spp, j->max_depth, j->seed);
+                                        try
+                                        {
+                                                j->owned = j->scene->create_painter(j->spp, j->max_depth, j->seed);
+                                        }
+                                        catch (const std::exception& e)
+                                        {
+                                                if (std::string(e.what()).find("out of memory") == std::string::npos)
+                                                {
+                                                        throw;
+                                                }
+                                                cudaGetLastError();
+                                                // the estimate let in more than the device holds: back to
+                                                // the head of the queue, and admit no more than what runs
+                                                // now until a job ends
+                                                const std::lock_guard lock(mutex_);
+                                                if (running_.size() <= 1)
+                                                {
+                                                        throw;
+                                                }
+                                                for (auto i = running_.begin(); i != running_.end(); ++i)
+                                                {
+                                                        if (i->get() == j.get())
+                                                        {
+                                                                running_.erase(i);
+                                                                break;
+                                                        }
+                                                }
+                                                used_ -= j->info.footprint;
+                                                j->info.state = JobState::QUEUED;
+                                                j->info.started = -1;
+                                                queue_.push_front(j);
+                                                budget_ = used_;
+                                                continue;
+                                        }
                                         j->painter = j->owned.get();
                                 }
                                 if (j->pass_in_flight)

@@ -83,6 +83,7 @@ private:
 
         int max_jobs_;
         long long budget_;
+        long long initial_budget_ = 0;
         long long used_ = 0;
         double start_;
         mutable std::mutex mutex_;
