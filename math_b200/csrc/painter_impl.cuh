@@ -227,10 +227,10 @@ std::array<T, M * M> inverse(std::array<T, M * M> a)
 
 // Runs f(begin, end) over [0, count) split across the host's threads.
 template <typename F>
-void parallel_ranges(const std::size_t count, const F& f)
+void parallel_ranges(const std::size_t count, const F& f, const std::size_t grain = 4096)
 {
         const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-        const std::size_t parts = std::min<std::size_t>(hw, std::max<std::size_t>(1, count / 4096));
+        const std::size_t parts = std::min<std::size_t>(hw, std::max<std::size_t>(1, count / grain));
         if (parts <= 1)
         {
                 f(std::size_t{0}, count);
@@ -258,11 +258,11 @@ void parallel_ranges(const std::size_t count, const F& f)
 
 // f(begin, end) over [0, count): in parts on the host threads, or at once
 template <typename F>
-void ranges(const bool parallel, const std::size_t count, const F& f)
+void ranges(const bool parallel, const std::size_t count, const F& f, const std::size_t grain = 4096)
 {
         if (parallel)
         {
-                parallel_ranges(count, f);
+                parallel_ranges(count, f, grain);
         }
         else
         {
@@ -400,24 +400,66 @@ std::vector<float> vertex_normals(const std::vector<float>& points, const std::v
                         }
                 });
         // the corners of every vertex in facet order, then each vertex's sum in
-        // that order (the vertices in parallel)
-        std::vector<std::size_t> first(vcount + 1, 0);
-        for (std::size_t c = 0; c < fcount * N; ++c)
+        // that order (the vertices in parallel).  The corner lists are built by
+        // parts of the facets: each part counts its corners per vertex, and a
+        // vertex's corners from part k follow those from parts before k.
+        const std::size_t corner_count = fcount * N;
+        const unsigned parts = parallel ? std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(),
+                                                                          static_cast<unsigned>(corner_count / 16384)))
+                                        : 1u;
+        const std::size_t step = (corner_count + parts - 1) / parts;
+        std::vector<std::vector<int>> part_count(parts, std::vector<int>(vcount, 0));
+        const auto each_part = [&](const auto& f)
         {
-                ++first[facets[c] + 1];
-        }
+                if (parts == 1)
+                {
+                        f(0u);
+                        return;
+                }
+                std::vector<std::thread> pool;
+                for (unsigned k = 1; k < parts; ++k)
+                {
+                        pool.emplace_back([&f, k] { f(k); });
+                }
+                f(0u);
+                for (std::thread& t : pool)
+                {
+                        t.join();
+                }
+        };
+        each_part(
+                [&](const unsigned k)
+                {
+                        std::vector<int>& count = part_count[k];
+                        const std::size_t e = std::min(corner_count, (k + 1) * step);
+                        for (std::size_t c = k * step; c < e; ++c)
+                        {
+                                ++count[facets[c]];
+                        }
+                });
+        std::vector<int> first(vcount + 1, 0);
         for (std::size_t v = 0; v < vcount; ++v)
         {
-                first[v + 1] += first[v];
-        }
-        std::vector<std::size_t> corners(fcount * N);
-        {
-                std::vector<std::size_t> fill(first.begin(), first.end() - 1);
-                for (std::size_t c = 0; c < fcount * N; ++c)
+                int offset = first[v];
+                for (unsigned k = 0; k < parts; ++k)
                 {
-                        corners[fill[facets[c]]++] = c;
+                        const int n = part_count[k][v];
+                        part_count[k][v] = offset; // where part k's corners of v go
+                        offset += n;
                 }
+                first[v + 1] = offset;
         }
+        std::vector<int> corners(corner_count);
+        each_part(
+                [&](const unsigned k)
+                {
+                        std::vector<int>& fill = part_count[k];
+                        const std::size_t e = std::min(corner_count, (k + 1) * step);
+                        for (std::size_t c = k * step; c < e; ++c)
+                        {
+                                corners[fill[facets[c]]++] = static_cast<int>(c);
+                        }
+                });
         std::vector<float> out(vcount * N, 0.0f);
         ranges(
                 parallel, vcount,
@@ -431,9 +473,9 @@ std::vector<float> vertex_normals(const std::vector<float>& points, const std::v
                                 }
                                 const Vec<N, double> reference = fn[corners[first[v]] / N];
                                 Vec<N, double> sum = Vec<N, double>::filled(0);
-                                for (std::size_t i = first[v]; i < first[v + 1]; ++i)
+                                for (int i = first[v]; i < first[v + 1]; ++i)
                                 {
-                                        const std::size_t c = corners[i];
+                                        const std::size_t c = static_cast<std::size_t>(corners[i]);
                                         const Vec<N, double>& n = fn[c / N];
                                         const Vec<N, double> wn = n * weight[c];
                                         if (dot(n, reference) >= 0)
@@ -451,7 +493,8 @@ std::vector<float> vertex_normals(const std::vector<float>& points, const std::v
                                         out[v * N + d] = static_cast<float>(n[d]);
                                 }
                         }
-                });
+                },
+                512);
         return out;
 }
 
