@@ -393,119 +393,133 @@ struct Bpt final
                 return abs_value(numerator / denominator);
         }
 
-        NBPT_CALL void walk(const bool camera_path, Color<C> beta, T pdf_forward, Ray<N, T> ray,
-                             PathVertex<N, T, C>* path, int& size) const
+        // A subpath walk in progress (walk, bpt.cpp:184-212): the throughput,
+        // the forward pdf, the ray to trace next and the bounces done.
+        struct Walk final
         {
-                Normals<N, T> normals;
-                Hit<N, T> surface = q.scene_intersect(nullptr, ray, normals);
+                Color<C> beta;
+                T pdf_forward;
+                Ray<N, T> ray;
+                int depth;
+                bool camera;
+        };
 
-                for (int depth = 0; depth < max_depth; ++depth)
+        // process_intersection (bpt.cpp:136-178) for the closest hit of
+        // w.ray: the vertex added to the walk's subpath, and true with w.ray
+        // set to the next ray (to be traced from normals.geometric) when the
+        // walk goes on.  The reference intersects the next ray of the last
+        // bounce as well and never uses the hit; the walk ends there instead,
+        // with the same vertices, random stream and tape.
+        NBPT_CALL bool walk_step(Walk& w, const Hit<N, T>& surface, const Normals<N, T>& normals)
+        {
+                PathVertex<N, T, C>* const path = w.camera ? camera : light;
+                int& size = w.camera ? camera_size : light_size;
+                const Vec<N, T> v = -w.ray.dir;
+                // surface_found (bpt.cpp:60-67)
+                if (!(surface && dot(normals.shading, v) > 0))
                 {
-                        const Vec<N, T> v = -ray.dir;
-                        // surface_found (bpt.cpp:60-67)
-                        if (!(surface && dot(normals.shading, v) > 0))
+                        // surface_not_found (bpt.cpp:84-100)
+                        if (w.camera)
                         {
-                                if (camera_path)
-                                {
-                                        path[size].type = static_cast<int>(VertexType::INFINITE);
-                                        ++size;
-                                }
-                                return;
-                        }
-
-                        // surface_sample_with_pdf (surface_sample.cpp:39-82)
-                        const int material = q.material(surface);
-                        const Material<T, C>& m = s.materials[material];
-                        const Vec<N, T>& n = normals.shading;
-                        BrdfTerms terms;
-                        const BrdfSample<N, C, T> bs =
-                                brdf_sample<N>(g, s.shading, m.roughness, m.f0, m.rho_ss, n, v, RECORD ? &terms : nullptr);
-                        bool ok = bs.pdf > 0 && !bs.brdf.is_black();
-                        T n_l = 0;
-                        if (ok)
-                        {
-                                ok = dot(bs.l, normals.geometric) > 0;
-                        }
-                        if (ok)
-                        {
-                                n_l = dot(n, bs.l);
-                                ok = n_l > 0;
-                        }
-                        if (!ok)
-                        {
-                                // sample_not_found (bpt.cpp:102-117)
-                                if (q.light(surface) >= 0)
-                                {
-                                        PathVertex<N, T, C>& next = path[size];
-                                        set_surface(next, surface, normals, beta, v);
-                                        next.pdf_fwd = prev_area_pdf(path[size - 1], pdf_forward, next.pos, next.nrm.shading);
-                                        ++size;
-                                }
-                                return;
-                        }
-                        const float sample_k = static_cast<float>(n_l / bs.pdf);
-                        const Color<C> sample_beta = bs.brdf * sample_k;
-                        const T pdf_reversed = brdf_pdf(s.shading, m.roughness, n, bs.l, v);
-
-                        // add_sample (bpt.cpp:119-134)
-                        {
-                                PathVertex<N, T, C>& next = path[size];
-                                set_surface(next, surface, normals, beta, v);
-                                PathVertex<N, T, C>& prev = path[size - 1];
-                                next.pdf_fwd = prev_area_pdf(prev, pdf_forward, next.pos, next.nrm.shading);
-                                if (prev.type == static_cast<int>(VertexType::SURFACE))
-                                {
-                                        prev.pdf_rev = area_pdf_pos(next.pos, pdf_reversed, prev.pos, &prev.nrm.shading);
-                                }
-                                else if (prev.type == static_cast<int>(VertexType::LIGHT))
-                                {
-                                        prev.pdf_rev = area_pdf_pos(next.pos, pdf_reversed, prev.pos,
-                                                                    prev.has_normal ? &prev.nrm.shading : nullptr);
-                                }
+                                path[size].type = static_cast<int>(VertexType::INFINITE);
                                 ++size;
                         }
-
-                        pdf_forward = bs.pdf;
-                        beta *= sample_beta;
-                        float normals_k = 1;
-                        if (!camera_path)
-                        {
-                                normals_k = static_cast<float>(correct_normals(normals, bs.l, v));
-                                beta *= normals_k;
-                        }
-                        if constexpr (RECORD)
-                        {
-                                tape.put(static_cast<int>(camera_path ? TapeRecord::CAMERA_BOUNCE
-                                                                      : TapeRecord::LIGHT_BOUNCE));
-                                tape.put(material);
-                                tape.put(terms);
-                                tape.put(sample_k);
-                                if (!camera_path)
-                                {
-                                        tape.put(normals_k);
-                                }
-                        }
-                        if (beta.is_black())
-                        {
-                                return;
-                        }
-                        ray = Ray<N, T>::make(surface.point, bs.l);
-                        const Vec<N, T> gn = normals.geometric;
-                        surface = q.scene_intersect(&gn, ray, normals);
+                        return false;
                 }
+
+                // surface_sample_with_pdf (surface_sample.cpp:39-82)
+                const int material = q.material(surface);
+                const Material<T, C>& m = s.materials[material];
+                const Vec<N, T>& n = normals.shading;
+                BrdfTerms terms;
+                const BrdfSample<N, C, T> bs =
+                        brdf_sample<N>(g, s.shading, m.roughness, m.f0, m.rho_ss, n, v, RECORD ? &terms : nullptr);
+                bool ok = bs.pdf > 0 && !bs.brdf.is_black();
+                T n_l = 0;
+                if (ok)
+                {
+                        ok = dot(bs.l, normals.geometric) > 0;
+                }
+                if (ok)
+                {
+                        n_l = dot(n, bs.l);
+                        ok = n_l > 0;
+                }
+                if (!ok)
+                {
+                        // sample_not_found (bpt.cpp:102-117)
+                        if (q.light(surface) >= 0)
+                        {
+                                PathVertex<N, T, C>& next = path[size];
+                                set_surface(next, surface, normals, w.beta, v);
+                                next.pdf_fwd = prev_area_pdf(path[size - 1], w.pdf_forward, next.pos, next.nrm.shading);
+                                ++size;
+                        }
+                        return false;
+                }
+                const float sample_k = static_cast<float>(n_l / bs.pdf);
+                const Color<C> sample_beta = bs.brdf * sample_k;
+                const T pdf_reversed = brdf_pdf(s.shading, m.roughness, n, bs.l, v);
+
+                // add_sample (bpt.cpp:119-134)
+                {
+                        PathVertex<N, T, C>& next = path[size];
+                        set_surface(next, surface, normals, w.beta, v);
+                        PathVertex<N, T, C>& prev = path[size - 1];
+                        next.pdf_fwd = prev_area_pdf(prev, w.pdf_forward, next.pos, next.nrm.shading);
+                        if (prev.type == static_cast<int>(VertexType::SURFACE))
+                        {
+                                prev.pdf_rev = area_pdf_pos(next.pos, pdf_reversed, prev.pos, &prev.nrm.shading);
+                        }
+                        else if (prev.type == static_cast<int>(VertexType::LIGHT))
+                        {
+                                prev.pdf_rev = area_pdf_pos(next.pos, pdf_reversed, prev.pos,
+                                                            prev.has_normal ? &prev.nrm.shading : nullptr);
+                        }
+                        ++size;
+                }
+
+                w.pdf_forward = bs.pdf;
+                w.beta *= sample_beta;
+                float normals_k = 1;
+                if (!w.camera)
+                {
+                        normals_k = static_cast<float>(correct_normals(normals, bs.l, v));
+                        w.beta *= normals_k;
+                }
+                if constexpr (RECORD)
+                {
+                        tape.put(static_cast<int>(w.camera ? TapeRecord::CAMERA_BOUNCE : TapeRecord::LIGHT_BOUNCE));
+                        tape.put(material);
+                        tape.put(terms);
+                        tape.put(sample_k);
+                        if (!w.camera)
+                        {
+                                tape.put(normals_k);
+                        }
+                }
+                if (w.beta.is_black() || ++w.depth == max_depth)
+                {
+                        return false;
+                }
+                w.ray = Ray<N, T>::make(surface.point, bs.l);
+                return true;
         }
 
-        __device__ void camera_path(const Ray<N, T>& ray)
+        // generate_camera_path (bpt.cpp:213-229) up to its first ray.
+        __device__ Walk camera_start(const Ray<N, T>& ray)
         {
                 camera_size = 1;
                 camera[0].type = static_cast<int>(VertexType::CAMERA);
                 camera[0].dir = -ray.dir;
                 camera[0].has_pos = false;
                 camera[0].has_normal = false;
-                walk(true, Color<C>::filled(1), T(1), ray, camera, camera_size);
+                return Walk{Color<C>::filled(1), T(1), ray, 0, true};
         }
 
-        __device__ void light_path()
+        // generate_light_path (bpt.cpp:231-264) up to its first ray: false,
+        // with no light subpath, when the light sample is unusable.
+        __device__ bool light_start(Walk& w)
         {
                 light_size = 0;
                 const int li = sample_light();
@@ -513,7 +527,7 @@ struct Bpt final
                 const LeaveSample<N, T, C> ls = leave_sample(l);
                 if (!(ls.pdf_pos > 0 && ls.pdf_dir > 0 && !ls.radiance.is_black()))
                 {
-                        return;
+                        return false;
                 }
                 const T dpdf = l.distribution_pdf;
                 PathVertex<N, T, C>& v = light[0];
@@ -532,14 +546,14 @@ struct Bpt final
                 const T pdf = dpdf * ls.pdf_pos * ls.pdf_dir;
                 const T k = max_value(T(0), dot(ls.n, ls.ray.dir));
                 const float start_k = static_cast<float>(k / pdf);
-                const Color<C> beta = ls.radiance * start_k;
                 if constexpr (RECORD)
                 {
                         tape.put(static_cast<int>(TapeRecord::LIGHT_START));
                         tape.put(li);
                         tape.put(start_k);
                 }
-                walk(false, beta, ls.pdf_dir, ls.ray, light, light_size);
+                w = Walk{ls.radiance * start_k, ls.pdf_dir, ls.ray, 0, false};
+                return true;
         }
 
         // -----------------------------------------------------------------
@@ -792,7 +806,7 @@ struct Bpt final
                 return true;
         }
 
-        // bpt() (bpt.cpp:267-292) up to the connections: BACKGROUND for a
+        // bpt() (bpt.cpp:267-292) after the camera subpath: BACKGROUND for a
         // camera ray that leaves the scene (the reference's nullopt), NO_LIGHT
         // when the camera subpath is the camera alone (black), CONNECT when
         // the light subpath is traced and the strategies follow.
@@ -803,9 +817,8 @@ struct Bpt final
                 CONNECT = 2
         };
 
-        __device__ Subpaths subpaths(const Ray<N, T>& ray)
+        __device__ Subpaths camera_outcome() const
         {
-                camera_path(ray);
                 if (camera_size == 1)
                 {
                         return Subpaths::NO_LIGHT;
@@ -814,43 +827,7 @@ struct Bpt final
                 {
                         return Subpaths::BACKGROUND;
                 }
-                light_path();
                 return Subpaths::CONNECT;
-        }
-
-        // connect() (connect.cpp:318-375): the strategies in the reference's
-        // order, their contributions summed
-        __device__ Color<C> connect()
-        {
-                Color<C> color = Color<C>::filled(0);
-                for (int t = 2; t <= camera_size; ++t)
-                {
-                        for (int sc = 0; sc <= light_size; ++sc)
-                        {
-                                if (t + sc - 2 > max_depth)
-                                {
-                                        continue;
-                                }
-                                Color<C> c;
-                                if (connect_strategy(sc, t, c))
-                                {
-                                        color += c;
-                                }
-                        }
-                }
-                return color;
-        }
-
-        // bpt(): false for a background sample
-        __device__ bool run(const Ray<N, T>& ray, Color<C>& out)
-        {
-                const Subpaths r = subpaths(ray);
-                if (r == Subpaths::BACKGROUND)
-                {
-                        return false;
-                }
-                out = r == Subpaths::CONNECT ? connect() : Color<C>::filled(0);
-                return true;
         }
 };
 } // namespace nbpt

@@ -194,8 +194,9 @@ __global__ void sj_points_kernel(
 // ---------------------------------------------------------------------------
 // Paths: one per pixel sample, with the random stream seed_seq{seed, pass,
 // p, i + 1}.  A chunk of pixels runs through four kernels:
-//   paths_walk_kernel     one thread per path: the camera and light subpaths
-//                         traced with colour channel 0 (tape.cuh), their
+//   paths_walk_kernel     one lane per path, one bounce per iteration: the
+//                         camera and light subpaths traced with colour
+//                         channel 0 (tape.cuh), their
 //                         vertices kept in global memory, the bounce records
 //                         on the path's tape, and one task queued per
 //                         strategy with s != 1;
@@ -312,9 +313,16 @@ __device__ inline unsigned reserve_together(unsigned* const counter, const unsig
         return base + before;
 }
 
-// Persistent: every thread takes paths from a shared counter until the
-// chunk is done, so lanes whose paths end early start new ones instead of
-// idling while the rest of their warp walks on.
+// Persistent, one bounce per iteration: every lane traces one ray and
+// processes its hit (Bpt::walk_step) in each iteration of the loop, whether
+// the ray belongs to a camera or a light subpath, so the warp's lanes run the
+// intersection and the shading together however their paths' lengths
+// differ.  A lane whose camera subpath ends starts its light subpath
+// (bpt.cpp:273-289) in the same iteration, and a lane whose path ends
+// finishes it and takes the next path from a shared counter until the chunk
+// is done.  Each path's random stream, vertices and tape are those of the
+// reference's sequential order (camera subpath, light sample, light
+// subpath).
 template <int N, typename T>
 __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_walk_kernel(
         const DeviceScene<N, T, 1> scene,
@@ -334,48 +342,76 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_walk_kernel(
         unsigned* __restrict__ next_path,
         PathStats* __restrict__ stats)
 {
+        using B = Bpt<N, T, 1, true>;
+        using S = typename B::Subpaths;
         const long long paths = (end - begin) * spp;
         QueryCounters counters{0, 0, 0, 0};
+        const SceneQueries<N, T, 1> q{scene, counters};
+        Pcg g{0, 0};
+        B bpt{q, scene, g, max_depth, nullptr, nullptr};
+        typename B::Walk w;
+        Vec<N, T> gn;
+        bool from_surface = false;
+        long long i = -1; // the lane's path; -1 when it takes the next one
         while (true)
         {
-                const long long i = reserve_together(next_path, 1);
-                if (i >= paths)
+                if (i < 0)
                 {
-                        break;
-                }
-                const long long local_pixel = i / spp;
-                const int sample = static_cast<int>(i - local_pixel * spp);
-                const long long p = begin + local_pixel;
-
-                Vec<N - 1, T> point;
-                {
-                        long long rest = p;
-#pragma unroll
-                        for (int d = 0; d < N - 1; ++d)
+                        i = reserve_together(next_path, 1);
+                        if (i >= paths)
                         {
-                                const int size = scene.projector.size[d];
-                                const long long q = rest / size;
-                                point[d] = static_cast<T>(static_cast<int>(rest - q * size)) + points[i * (N - 1) + d];
-                                rest = q;
+                                break;
                         }
+                        const long long local_pixel = i / spp;
+                        const int sample = static_cast<int>(i - local_pixel * spp);
+                        const long long p = begin + local_pixel;
+                        Vec<N - 1, T> point;
+                        {
+                                long long rest = p;
+#pragma unroll
+                                for (int d = 0; d < N - 1; ++d)
+                                {
+                                        const int size = scene.projector.size[d];
+                                        const long long r = rest / size;
+                                        point[d] = static_cast<T>(static_cast<int>(rest - r * size)) +
+                                                   points[i * (N - 1) + d];
+                                        rest = r;
+                                }
+                        }
+                        const std::uint32_t words[4] = {seed, pass, static_cast<std::uint32_t>(p),
+                                                        static_cast<std::uint32_t>(sample + 1)};
+                        g = seed_seq_pcg(words, 4);
+                        bpt.camera = vertices + i * 2 * (max_depth + 1);
+                        bpt.light = bpt.camera + max_depth + 1;
+                        bpt.light_size = 0;
+                        bpt.tape.w = tape + i * static_cast<long long>(words_per_path);
+                        bpt.tape.n = TAPE_HEADER;
+                        w = bpt.camera_start(scene.projector.ray(point));
+                        from_surface = false;
                 }
-                const Ray<N, T> ray = scene.projector.ray(point);
 
-                const std::uint32_t words[4] = {seed, pass, static_cast<std::uint32_t>(p),
-                                                static_cast<std::uint32_t>(sample + 1)};
-                Pcg g = seed_seq_pcg(words, 4);
-                const SceneQueries<N, T, 1> q{scene, counters};
-                PathVertex<N, T, 1>* const v = vertices + i * 2 * (max_depth + 1);
-                Bpt<N, T, 1, true> bpt{q, scene, g, max_depth, v, v + max_depth + 1};
-                std::uint32_t* const w = tape + i * static_cast<long long>(words_per_path);
-                bpt.tape.w = w;
-                using S = typename Bpt<N, T, 1, true>::Subpaths;
-                const S r = bpt.subpaths(ray);
+                Normals<N, T> normals;
+                const Hit<N, T> surface = q.scene_intersect(from_surface ? &gn : nullptr, w.ray, normals);
+                if (bpt.walk_step(w, surface, normals))
+                {
+                        gn = normals.geometric;
+                        from_surface = true;
+                        continue;
+                }
+                if (w.camera && bpt.camera_outcome() == S::CONNECT && bpt.light_start(w))
+                {
+                        from_surface = false;
+                        continue;
+                }
+
+                // the path's subpaths are done
+                const S r = bpt.camera_outcome();
                 const bool connect = r == S::CONNECT;
-                w[0] = static_cast<std::uint32_t>(bpt.tape.n);
-                w[1] = r != S::BACKGROUND ? 1u : 0u;
-                w[2] = static_cast<std::uint32_t>(connect ? bpt.camera_size : 1);
-                w[3] = static_cast<std::uint32_t>(connect ? bpt.light_size : 0);
+                std::uint32_t* const tw = bpt.tape.w;
+                tw[0] = static_cast<std::uint32_t>(bpt.tape.n);
+                tw[1] = r != S::BACKGROUND ? 1u : 0u;
+                tw[2] = static_cast<std::uint32_t>(connect ? bpt.camera_size : 1);
+                tw[3] = static_cast<std::uint32_t>(connect ? bpt.light_size : 0);
                 valid[i] = r != S::BACKGROUND ? 1 : 0;
                 rng[i] = g;
                 if (connect)
@@ -409,6 +445,7 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_walk_kernel(
                                 }
                         }
                 }
+                i = -1;
         }
         add_counters(counters, stats);
 }
