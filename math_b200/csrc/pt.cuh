@@ -224,14 +224,18 @@ __device__ float pt_brdf_channel(const BrdfTerms& t, const int zero, const Mater
 #define NBPT_PT_MIN_BLOCKS 16
 #endif
 
-// One path of the PT integrator per thread (pt.cpp:113-170), persistent: the
-// threads take paths from a shared counter.  The sample points, the path's
-// ray and its random stream are those of the BPT kernels (the same
-// stratified points, seed_seq{seed, pass, pixel, sample + 1}); the
-// reference's painter draws them the same way whichever integrator it runs
-// (painting.cpp:225-257).  beta stays in registers; the colour too for RGB,
-// while a spectrum accumulates in the output row.  `estimates` holds
-// 2 * light_count records per thread of the grid.
+// The PT integrator's paths (pt.cpp:113-170), one lane per path at a time
+// and one bounce per iteration of a persistent loop: every lane traces one
+// ray and processes its hit in each iteration, and a lane whose path ends
+// writes it out and takes the next path from a shared counter, so the
+// warp's lanes run together however many bounces Russian roulette gives
+// their paths.  The sample points, the path's ray and its random stream are
+// those of the BPT kernels (the same stratified points, seed_seq{seed, pass,
+// pixel, sample + 1}); the reference's painter draws them the same way
+// whichever integrator it runs (painting.cpp:225-257).  beta stays in
+// registers; the colour too for RGB, while a spectrum accumulates in the
+// output row.  `estimates` holds 2 * light_count records per thread of the
+// grid.
 template <int N, typename T, int C>
 __global__ void __launch_bounds__(128, NBPT_PT_MIN_BLOCKS) pt_paths_kernel(
         const DeviceScene<N, T, 1> scene,
@@ -257,56 +261,66 @@ __global__ void __launch_bounds__(128, NBPT_PT_MIN_BLOCKS) pt_paths_kernel(
                 estimates + (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) * 2 * scene.light_count;
         const ShadingConstants<T>& sc = scene.shading;
         QueryCounters counters{0, 0, 0, 0};
+        const SceneQueries<N, T, 1> q{scene, counters};
+        Pcg g{0, 0};
+        const Pt<N, T> pt{q, scene, g, Bpt<N, T, 1>{q, scene, g, 0, nullptr, nullptr}};
+        Ray<N, T> ray;
+        Vec<N, T> gn;
+        Color<IN_REGISTERS ? C : 1> reg;
+        Color<C> beta;
+        int depth = -1;   // the bounce whose hit is traced next; -1: the primary ray
+        long long i = -1; // the lane's path; -1 when it takes the next one
         while (true)
         {
-                const long long i = reserve_together(next_path, 1);
-                if (i >= paths)
+                if (i < 0)
                 {
-                        break;
-                }
-                const long long local_pixel = i / spp;
-                const int sample = static_cast<int>(i - local_pixel * spp);
-                const long long p = begin + local_pixel;
-
-                Vec<N - 1, T> point;
-                {
-                        long long rest = p;
-#pragma unroll
-                        for (int d = 0; d < N - 1; ++d)
+                        i = reserve_together(next_path, 1);
+                        if (i >= paths)
                         {
-                                const int size = scene.projector.size[d];
-                                const long long q = rest / size;
-                                point[d] = static_cast<T>(static_cast<int>(rest - q * size)) + points[i * (N - 1) + d];
-                                rest = q;
+                                break;
                         }
+                        const long long local_pixel = i / spp;
+                        const int sample = static_cast<int>(i - local_pixel * spp);
+                        const long long p = begin + local_pixel;
+                        Vec<N - 1, T> point;
+                        {
+                                long long rest = p;
+#pragma unroll
+                                for (int d = 0; d < N - 1; ++d)
+                                {
+                                        const int size = scene.projector.size[d];
+                                        const long long r = rest / size;
+                                        point[d] = static_cast<T>(static_cast<int>(rest - r * size)) +
+                                                   points[i * (N - 1) + d];
+                                        rest = r;
+                                }
+                        }
+                        ray = scene.projector.ray(point);
+                        const std::uint32_t words[4] = {seed, pass, static_cast<std::uint32_t>(p),
+                                                        static_cast<std::uint32_t>(sample + 1)};
+                        g = seed_seq_pcg(words, 4);
+                        depth = -1;
                 }
-                Ray<N, T> ray = scene.projector.ray(point);
-
-                const std::uint32_t words[4] = {seed, pass, static_cast<std::uint32_t>(p),
-                                                static_cast<std::uint32_t>(sample + 1)};
-                Pcg g = seed_seq_pcg(words, 4);
-                const SceneQueries<N, T, 1> q{scene, counters};
-                const Pt<N, T> pt{q, scene, g, Bpt<N, T, 1>{q, scene, g, 0, nullptr, nullptr}};
 
                 float* const out = colors + i * C;
                 Normals<N, T> normals;
-                Hit<N, T> surface = q.scene_intersect(nullptr, ray, normals);
-                if (!surface)
+                const Hit<N, T> surface = q.scene_intersect(depth < 0 ? nullptr : &gn, ray, normals);
+                if (depth < 0)
                 {
-#pragma unroll 8
-                        for (int c = 0; c < C; ++c)
+                        if (!surface)
                         {
-                                out[c] = 0.0f;
+#pragma unroll 8
+                                for (int c = 0; c < C; ++c)
+                                {
+                                        out[c] = 0.0f;
+                                }
+                                lum[i] = 0.0f;
+                                valid[i] = 0;
+                                i = -1;
+                                continue;
                         }
-                        lum[i] = 0.0f;
-                        valid[i] = 0;
-                        continue;
-                }
-
-                // the emitted radiance seen by the primary ray
-                // (LightSource::leave_radiance(-dir))
-                Color<IN_REGISTERS ? C : 1> reg;
-                {
+                        // the emitted radiance seen by the primary ray
+                        // (LightSource::leave_radiance(-dir))
                         const int li = q.light(surface);
                         const bool emits = li >= 0 && dot(-ray.dir, scene.lights[li].normal) > 0;
 #pragma unroll 8
@@ -322,18 +336,20 @@ __global__ void __launch_bounds__(128, NBPT_PT_MIN_BLOCKS) pt_paths_kernel(
                                         out[c] = e;
                                 }
                         }
+                        beta = Color<C>::filled(1);
+                        depth = 0;
                 }
-                Color<C> beta = Color<C>::filled(1);
 
-                for (int depth = 0; depth < PT_MAX_BOUNCES; ++depth)
+                // one bounce (pt.cpp:68-111); the path ends where the
+                // reference's loop breaks
+                bool go_on = static_cast<bool>(surface);
+                const Vec<N, T> v = -ray.dir;
+                if (go_on)
                 {
-                        // one bounce (pt.cpp:68-111)
-                        const Vec<N, T> v = -ray.dir;
-                        if (dot(normals.shading, v) <= 0)
-                        {
-                                break;
-                        }
-
+                        go_on = !(dot(normals.shading, v) <= 0);
+                }
+                if (go_on)
+                {
                         // direct_lighting (direct_lighting.cpp:150-167): both
                         // estimates of every light, summed in that order
                         int count = 0;
@@ -368,49 +384,50 @@ __global__ void __launch_bounds__(128, NBPT_PT_MIN_BLOCKS) pt_paths_kernel(
                         }
 
                         PtContinuation<N, T> next;
-                        if (!pt.continuation(surface, v, normals, next))
+                        go_on = pt.continuation(surface, v, normals, next);
+                        if (go_on)
                         {
-                                break;
-                        }
-#pragma unroll 8
-                        for (int c = 0; c < C; ++c)
-                        {
-                                beta.c[c] *= pt_brdf_channel(next.terms, 0, m, c, sc) * next.scale;
-                        }
-
-                        // terminate (pt.cpp:43-66)
-                        if (depth >= 4)
-                        {
-                                const float y = luminance(beta, cie_y);
-                                if (!(y > 0))
-                                {
-                                        break;
-                                }
-                                constexpr float MIN = 0.05f;
-                                constexpr float MAX = 0.95f;
-                                const float x = 1 - y;
-                                const float rr = (x < MIN) ? MIN : ((MAX < x) ? MAX : x);
-                                if (bernoulli(g, rr))
-                                {
-                                        break;
-                                }
-                                const float k = 1 - rr;
 #pragma unroll 8
                                 for (int c = 0; c < C; ++c)
                                 {
-                                        beta.c[c] /= k;
+                                        beta.c[c] *= pt_brdf_channel(next.terms, 0, m, c, sc) * next.scale;
                                 }
-                        }
 
-                        ray = Ray<N, T>::make(surface.point, next.l);
-                        const Vec<N, T> gn = normals.geometric;
-                        surface = q.scene_intersect(&gn, ray, normals);
-                        if (!surface)
-                        {
-                                break;
+                                // terminate (pt.cpp:43-66)
+                                if (depth >= 4)
+                                {
+                                        const float y = luminance(beta, cie_y);
+                                        go_on = y > 0;
+                                        if (go_on)
+                                        {
+                                                constexpr float MIN = 0.05f;
+                                                constexpr float MAX = 0.95f;
+                                                const float x = 1 - y;
+                                                const float rr = (x < MIN) ? MIN : ((MAX < x) ? MAX : x);
+                                                go_on = !bernoulli(g, rr);
+                                                if (go_on)
+                                                {
+                                                        const float k = 1 - rr;
+#pragma unroll 8
+                                                        for (int c = 0; c < C; ++c)
+                                                        {
+                                                                beta.c[c] /= k;
+                                                        }
+                                                }
+                                        }
+                                }
+                                // after the last bounce the path ends without
+                                // the next ray, whose hit the reference never uses
+                                if (go_on && ++depth < PT_MAX_BOUNCES)
+                                {
+                                        ray = Ray<N, T>::make(surface.point, next.l);
+                                        gn = normals.geometric;
+                                        continue;
+                                }
                         }
                 }
 
+                // the path is done
                 if constexpr (IN_REGISTERS)
                 {
 #pragma unroll
@@ -431,6 +448,7 @@ __global__ void __launch_bounds__(128, NBPT_PT_MIN_BLOCKS) pt_paths_kernel(
                         lum[i] = luminance(final_color, cie_y);
                 }
                 valid[i] = 1;
+                i = -1;
         }
         add_counters(counters, stats);
 }
