@@ -189,7 +189,7 @@ def cpu_baseline(small: bool, name: str = "cornell4d", precision: str = "float",
 # light, replay) on this workload in float, from the ncu capture summarised
 # in profiles/path_kernels_cornell4d_32.md (a 32^3 screen of the same scene;
 # traffic scales with the number of paths)
-TRAFFIC_PER_PATH = {"float": 23488.0}
+TRAFFIC_PER_PATH = {"float": 20636.0}
 
 
 def record_bytes(n: int, precision: str) -> dict:
