@@ -2,6 +2,7 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <cctype>
 #include <charconv>
 #include <cmath>
@@ -9,8 +10,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <filesystem>
-#include <fstream>
 #include <map>
+#include <memory>
 #include <set>
 #include <stdexcept>
 #include <string>
@@ -18,6 +19,10 @@
 #include <unordered_map>
 #include <thread>
 #include <vector>
+
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 namespace nbpt::host
 {
@@ -28,22 +33,92 @@ namespace
         throw std::runtime_error(message);
 }
 
-std::vector<char> read_bytes(const std::filesystem::path& path)
+// Host threads for `count` items of work in parts of at least `grain`.
+unsigned part_count(const std::size_t count, const std::size_t grain)
 {
-        std::ifstream f(path, std::ios::binary);
-        if (!f)
+        const std::size_t threads = std::max(1u, std::thread::hardware_concurrency());
+        return static_cast<unsigned>(std::max<std::size_t>(1, std::min(threads, count / grain)));
+}
+
+// fn(part, begin, end) over `parts` consecutive ranges of [0, count), part 0
+// on the calling thread; fn must not throw.
+template <typename F>
+void parallel_parts(const std::size_t count, const unsigned parts, const F& fn)
+{
+        const std::size_t step = (count + parts - 1) / parts;
+        std::vector<std::thread> pool;
+        for (unsigned t = 1; t < parts; ++t)
+        {
+                pool.emplace_back(
+                        [&, t]
+                        {
+                                fn(t, std::min(count, t * step), std::min(count, (t + 1) * step));
+                        });
+        }
+        fn(0u, std::size_t{0}, std::min(count, step));
+        for (std::thread& th : pool)
+        {
+                th.join();
+        }
+}
+
+// A file's bytes, with room for one byte more (a line end or a terminator).
+struct Bytes final
+{
+        std::unique_ptr<char[]> buffer;
+        std::size_t size = 0;
+
+        char* data()
+        {
+                return buffer.get();
+        }
+
+        const char* data() const
+        {
+                return buffer.get();
+        }
+};
+
+// The file read in parts by the host threads into an uninitialised buffer,
+// so that the buffer's pages are first touched by the readers in parallel.
+Bytes read_bytes(const std::filesystem::path& path)
+{
+        const int fd = ::open(path.c_str(), O_RDONLY);
+        if (fd < 0)
         {
                 fail("Failed to open file " + path.generic_string());
         }
-        f.seekg(0, std::ios::end);
-        const std::streamoff size = f.tellg();
-        f.seekg(0, std::ios::beg);
-        std::vector<char> data(static_cast<std::size_t>(size));
-        if (size > 0 && !f.read(data.data(), size))
+        struct stat st;
+        if (::fstat(fd, &st) != 0)
+        {
+                ::close(fd);
+                fail("Failed to read file " + path.generic_string());
+        }
+        Bytes bytes;
+        bytes.size = static_cast<std::size_t>(st.st_size);
+        bytes.buffer.reset(new char[bytes.size + 1]);
+        std::atomic<bool> ok{true};
+        parallel_parts(bytes.size, part_count(bytes.size, std::size_t{1} << 22),
+                       [&](unsigned, const std::size_t b, const std::size_t e)
+                       {
+                               std::size_t done = b;
+                               while (done < e)
+                               {
+                                       const ssize_t r = ::pread(fd, bytes.data() + done, e - done, static_cast<off_t>(done));
+                                       if (r <= 0)
+                                       {
+                                               ok = false;
+                                               return;
+                                       }
+                                       done += static_cast<std::size_t>(r);
+                               }
+                       });
+        ::close(fd);
+        if (!ok)
         {
                 fail("Failed to read file " + path.generic_string());
         }
-        return data;
+        return bytes;
 }
 
 // src/com/string/ascii.h
@@ -119,32 +194,57 @@ void read_floats(const char*& s, float* out, const int count)
 
 struct Lines final
 {
-        std::vector<char> data;
+        Bytes data;
         std::vector<std::size_t> begin;
 
-        explicit Lines(std::vector<char>&& text)
+        explicit Lines(Bytes&& text)
                 : data(std::move(text))
         {
-                if (data.empty())
+                if (data.size == 0)
                 {
                         return;
                 }
-                if (data.back() != '\n')
+                if (data.data()[data.size - 1] != '\n')
                 {
-                        data.push_back('\n');
+                        data.data()[data.size++] = '\n';
                 }
-                std::size_t start = 0;
-                for (std::size_t i = 0; i < data.size(); ++i)
+                if (std::memchr(data.data(), '\0', data.size) != nullptr)
                 {
-                        if (data[i] == '\0')
+                        fail("Text data contains null character");
+                }
+                // the line ends found in parts on the host threads, then
+                // joined in order
+                const unsigned parts = part_count(data.size, std::size_t{1} << 20);
+                std::vector<std::vector<std::size_t>> ends(parts);
+                parallel_parts(data.size, parts,
+                               [&](const unsigned t, const std::size_t b, const std::size_t e)
+                               {
+                                       char* p = data.data() + b;
+                                       char* const last = data.data() + e;
+                                       while (p < last)
+                                       {
+                                               p = static_cast<char*>(std::memchr(p, '\n', last - p));
+                                               if (p == nullptr)
+                                               {
+                                                       break;
+                                               }
+                                               ends[t].push_back(p - data.data());
+                                               *p++ = '\0';
+                                       }
+                               });
+                std::size_t lines = 0;
+                for (const std::vector<std::size_t>& part : ends)
+                {
+                        lines += part.size();
+                }
+                begin.reserve(lines);
+                std::size_t start = 0;
+                for (const std::vector<std::size_t>& part : ends)
+                {
+                        for (const std::size_t end : part)
                         {
-                                fail("Text data contains null character");
-                        }
-                        if (data[i] == '\n')
-                        {
-                                data[i] = '\0';
                                 begin.push_back(start);
-                                start = i + 1;
+                                start = end + 1;
                         }
                 }
         }
@@ -464,7 +564,6 @@ void read_obj(const std::filesystem::path& path, const int n, MeshFile& m)
         const int max_corners = (n == 3 ? 5 : 1) + n - 1;
         std::vector<int> texcoord_index; // per facet corner, -1 without
         int texcoord_count = 0;
-        int normal_count = 0;
         int material = -1;
         std::map<std::string, int, std::less<>> material_index; // materials still to find in the libraries
         std::vector<std::string> material_names;
@@ -475,34 +574,43 @@ void read_obj(const std::filesystem::path& path, const int n, MeshFile& m)
 
         // parse the lines in parts on the host threads, then apply them in order
         const std::size_t line_count = lines.size();
-        const unsigned threads = static_cast<unsigned>(std::max<std::size_t>(
-                1, std::min<std::size_t>(std::max(1u, std::thread::hardware_concurrency()), line_count / 4096)));
+        const unsigned threads = part_count(line_count, 4096);
         std::vector<ObjPart> parts(threads);
-        {
-                std::vector<std::thread> pool;
-                const std::size_t step = (line_count + threads - 1) / threads;
-                for (unsigned t = 1; t < threads; ++t)
-                {
-                        pool.emplace_back(
-                                [&, t]
-                                {
-                                        parse_obj_lines(lines, std::min(line_count, t * step),
-                                                        std::min(line_count, (t + 1) * step), n, max_corners, parts[t]);
-                                });
-                }
-                parse_obj_lines(lines, 0, std::min(line_count, step), n, max_corners, parts[0]);
-                for (std::thread& th : pool)
-                {
-                        th.join();
-                }
-        }
+        parallel_parts(line_count, threads,
+                       [&](const unsigned t, const std::size_t b, const std::size_t e)
+                       {
+                               parse_obj_lines(lines, b, e, n, max_corners, parts[t]);
+                       });
 
-        std::size_t i = 0;
-        for (const ObjPart& part : parts)
+        // In order over the parts: the running counts where each part starts
+        // and its facets' place, and the usemtl and mtllib lines, whose
+        // failures, like a part's parse error, come after the lines before
+        // them are taken.
+        struct PartStart final
         {
-                std::size_t value = 0;
+                std::size_t vertices = 0;
+                std::size_t normals = 0;
+                std::size_t texcoords = 0;
+                std::size_t facets = 0;
+                int material = -1;
+                std::vector<int> materials; // the material of each usemtl line of the part
+        };
+        std::vector<PartStart> starts(parts.size());
+        std::size_t vertices = 0;
+        std::size_t normals = 0;
+        std::size_t texcoords = 0;
+        std::size_t facets = 0;
+        std::size_t i = 0;
+        for (std::size_t p = 0; p < parts.size(); ++p)
+        {
+                const ObjPart& part = parts[p];
+                PartStart& start = starts[p];
+                start.vertices = vertices;
+                start.normals = normals;
+                start.texcoords = texcoords;
+                start.facets = facets;
+                start.material = material;
                 std::size_t facet_line = 0;
-                std::size_t corner = 0;
                 for (const LineKind kind : part.kind)
                 {
                         const std::size_t line = i++;
@@ -511,42 +619,18 @@ void read_obj(const std::filesystem::path& path, const int n, MeshFile& m)
                         case LineKind::NONE:
                                 break;
                         case LineKind::V:
-                                m.vertices.insert(m.vertices.end(), part.values.begin() + value,
-                                                  part.values.begin() + value + n);
-                                value += n;
+                                ++vertices;
                                 break;
                         case LineKind::VT:
-                                ++texcoord_count;
+                                ++texcoords;
                                 break;
                         case LineKind::VN:
-                                m.normals.insert(m.normals.end(), part.values.begin() + value,
-                                                 part.values.begin() + value + n);
-                                value += n;
-                                ++normal_count;
+                                ++normals;
                                 break;
                         case LineKind::F:
-                        {
-                                const int count = part.corner_count[facet_line++];
-                                const Corner* const c0 = &part.corners[corner];
-                                corner += count;
-                                const int vertex_count = static_cast<int>(m.vertices.size() / n);
-                                const bool normals = c0[0].normal != 0;
                                 // a fan around the first corner
-                                for (int f = 0; f + n - 1 < count; ++f)
-                                {
-                                        for (int k = 0; k < n; ++k)
-                                        {
-                                                const Corner& c = c0[k == 0 ? 0 : f + k];
-                                                const int v = c.vertex > 0 ? c.vertex - 1 : vertex_count + c.vertex;
-                                                m.facet_vertices.push_back(v);
-                                                m.facet_normals.push_back(absolute_index(c.normal, normal_count));
-                                                texcoord_index.push_back(absolute_index(c.texcoord, texcoord_count));
-                                        }
-                                        m.has_normal.push_back(normals ? 1 : 0);
-                                        m.facet_material.push_back(material);
-                                }
+                                facets += part.corner_count[facet_line++] - n + 1;
                                 break;
-                        }
                         case LineKind::USEMTL:
                         {
                                 const Split s = split(lines.line(line));
@@ -563,6 +647,7 @@ void read_obj(const std::filesystem::path& path, const int n, MeshFile& m)
                                         material = static_cast<int>(material_names.size()) - 1;
                                         material_index.emplace(name, material);
                                 }
+                                start.materials.push_back(material);
                                 break;
                         }
                         case LineKind::MTLLIB:
@@ -607,6 +692,84 @@ void read_obj(const std::filesystem::path& path, const int n, MeshFile& m)
                         fail(part.error);
                 }
         }
+        texcoord_count = static_cast<int>(texcoords);
+
+        // the parts' vertices, normals and facets written in parallel
+        m.vertices.resize(vertices * n);
+        m.normals.resize(normals * n);
+        m.facet_vertices.resize(facets * n);
+        m.facet_normals.resize(facets * n);
+        texcoord_index.resize(facets * n);
+        m.has_normal.resize(facets);
+        m.facet_material.resize(facets);
+        parallel_parts(
+                parts.size(), static_cast<unsigned>(parts.size()),
+                [&](unsigned, const std::size_t part_begin, const std::size_t part_end)
+                {
+                        for (std::size_t p = part_begin; p < part_end; ++p)
+                        {
+                                const ObjPart& part = parts[p];
+                                const PartStart& start = starts[p];
+                                std::size_t v = start.vertices;
+                                std::size_t vn = start.normals;
+                                std::size_t vt = start.texcoords;
+                                std::size_t f = start.facets;
+                                int facet_material = start.material;
+                                std::size_t usemtl = 0;
+                                std::size_t value = 0;
+                                std::size_t facet_line = 0;
+                                std::size_t corner = 0;
+                                for (const LineKind kind : part.kind)
+                                {
+                                        switch (kind)
+                                        {
+                                        case LineKind::V:
+                                                std::copy_n(part.values.begin() + value, n, m.vertices.begin() + v * n);
+                                                value += n;
+                                                ++v;
+                                                break;
+                                        case LineKind::VT:
+                                                ++vt;
+                                                break;
+                                        case LineKind::VN:
+                                                std::copy_n(part.values.begin() + value, n, m.normals.begin() + vn * n);
+                                                value += n;
+                                                ++vn;
+                                                break;
+                                        case LineKind::F:
+                                        {
+                                                const int count = part.corner_count[facet_line++];
+                                                const Corner* const c0 = &part.corners[corner];
+                                                corner += count;
+                                                const int vertex_count = static_cast<int>(v);
+                                                const bool with_normals = c0[0].normal != 0;
+                                                for (int fan = 0; fan + n - 1 < count; ++fan, ++f)
+                                                {
+                                                        for (int k = 0; k < n; ++k)
+                                                        {
+                                                                const Corner& c = c0[k == 0 ? 0 : fan + k];
+                                                                m.facet_vertices[f * n + k] =
+                                                                        c.vertex > 0 ? c.vertex - 1 : vertex_count + c.vertex;
+                                                                m.facet_normals[f * n + k] =
+                                                                        absolute_index(c.normal, static_cast<int>(vn));
+                                                                texcoord_index[f * n + k] =
+                                                                        absolute_index(c.texcoord, static_cast<int>(vt));
+                                                        }
+                                                        m.has_normal[f] = with_normals ? 1 : 0;
+                                                        m.facet_material[f] = facet_material;
+                                                }
+                                                break;
+                                        }
+                                        case LineKind::USEMTL:
+                                                facet_material = start.materials[usemtl++];
+                                                break;
+                                        case LineKind::NONE:
+                                        case LineKind::MTLLIB:
+                                                break;
+                                        }
+                                }
+                        }
+                });
         if (m.has_normal.empty())
         {
                 fail("No facets found in OBJ file");
@@ -736,93 +899,146 @@ bool starts_with_keyword(const char* p, const char* const last, const std::strin
         return !(q < last && !is_space(*q));
 }
 
-// vertices equal as float vectors (+0 equals -0, NaN equals nothing) share an index
-class UniqueVertices final
+// A corner's coordinates as a map key: the float bits with -0 as +0.
+struct VertexKey final
 {
-        struct Key final
+        std::array<std::uint32_t, 5> bits{};
+
+        bool operator==(const VertexKey&) const = default;
+};
+
+struct VertexKeyHash final
+{
+        std::size_t operator()(const VertexKey& k) const
         {
-                std::array<std::uint32_t, 5> bits{};
-
-                bool operator==(const Key&) const = default;
-        };
-
-        struct Hash final
-        {
-                std::size_t operator()(const Key& k) const
+                std::size_t h = 1469598103934665603ull;
+                for (const std::uint32_t b : k.bits)
                 {
-                        std::size_t h = 1469598103934665603ull;
-                        for (const std::uint32_t b : k.bits)
-                        {
-                                h = (h ^ b) * 1099511628211ull;
-                        }
-                        return h;
+                        h = (h ^ b) * 1099511628211ull;
                 }
-        };
-
-        std::unordered_map<Key, int, Hash> map_;
-        MeshFile& m_;
-
-public:
-        explicit UniqueVertices(MeshFile& m)
-                : m_(m)
-        {
-        }
-
-        int index(const float* v)
-        {
-                const int n = m_.n;
-                Key key;
-                bool nan = false;
-                for (int i = 0; i < n; ++i)
-                {
-                        const float x = v[i] == 0.0f ? 0.0f : v[i];
-                        nan = nan || x != x;
-                        std::memcpy(&key.bits[i], &x, sizeof(float));
-                }
-                if (!nan)
-                {
-                        const auto it = map_.find(key);
-                        if (it != map_.end())
-                        {
-                                return it->second;
-                        }
-                }
-                const int index = static_cast<int>(m_.vertices.size() / n);
-                m_.vertices.insert(m_.vertices.end(), v, v + n);
-                if (!nan)
-                {
-                        map_.emplace(key, index);
-                }
-                return index;
+                return h;
         }
 };
 
-void add_stl_facet(MeshFile& m, UniqueVertices& unique, const float* vertices)
+// false for a corner with a NaN coordinate
+bool vertex_key(const float* const v, const int n, VertexKey& key)
 {
-        for (int k = 0; k < m.n; ++k)
+        for (int i = 0; i < n; ++i)
         {
-                m.facet_vertices.push_back(unique.index(vertices + k * m.n));
-                m.facet_normals.push_back(-1);
+                const float x = v[i] == 0.0f ? 0.0f : v[i];
+                if (x != x)
+                {
+                        return false;
+                }
+                std::memcpy(&key.bits[i], &x, sizeof(float));
         }
-        m.has_normal.push_back(0);
-        m.facet_material.push_back(-1);
+        return true;
+}
+
+// The STL facets from their corners: facet f's n corners of n floats start
+// at base + f * stride.  Corners equal as float vectors (+0 equals -0, NaN
+// equals nothing) share one vertex, and the vertices are numbered in order
+// of first appearance, as one map filled corner by corner numbers them.  The
+// corners are hashed into one group per host thread; each thread fills its
+// group's map in corner order, so it meets each of its vertices first where
+// the vertex first appears, and the numbering is a running count of first
+// appearances over all corners.  The per-corner scratch is left
+// uninitialised, so that its pages are first touched by the threads.
+void add_stl_facets(MeshFile& m, const char* const base, const std::size_t stride, const std::size_t facets)
+{
+        const int n = m.n;
+        const std::size_t count = facets * n;
+        const auto corner = [&](const std::size_t c, float* const v)
+        {
+                std::memcpy(v, base + (c / n) * stride + (c % n) * n * sizeof(float), n * sizeof(float));
+        };
+        constexpr std::uint32_t NO_GROUP = 0xffffffffu;
+        const unsigned groups = part_count(count, std::size_t{1} << 15);
+
+        const std::unique_ptr<std::uint32_t[]> group(new std::uint32_t[count]);
+        const std::unique_ptr<std::size_t[]> first(new std::size_t[count]); // where the vertex first appears
+        parallel_parts(count, groups,
+                       [&](unsigned, const std::size_t b, const std::size_t e)
+                       {
+                               float v[5];
+                               for (std::size_t c = b; c < e; ++c)
+                               {
+                                       corner(c, v);
+                                       VertexKey key;
+                                       if (vertex_key(v, n, key))
+                                       {
+                                               group[c] = static_cast<std::uint32_t>(VertexKeyHash()(key) % groups);
+                                       }
+                                       else
+                                       {
+                                               group[c] = NO_GROUP;
+                                       }
+                                       first[c] = c;
+                               }
+                       });
+        parallel_parts(groups, groups,
+                       [&](const unsigned t, std::size_t, std::size_t)
+                       {
+                               std::unordered_map<VertexKey, std::size_t, VertexKeyHash> map;
+                               float v[5];
+                               for (std::size_t c = 0; c < count; ++c)
+                               {
+                                       if (group[c] != t)
+                                       {
+                                               continue;
+                                       }
+                                       corner(c, v);
+                                       VertexKey key;
+                                       vertex_key(v, n, key);
+                                       first[c] = map.try_emplace(key, c).first->second;
+                               }
+                       });
+
+        // vertex numbers at first appearances (in the group array, no longer
+        // needed), then every corner's vertex and the vertices' coordinates
+        std::uint32_t* const number = group.get();
+        std::uint32_t vertices = 0;
+        for (std::size_t c = 0; c < count; ++c)
+        {
+                if (first[c] == c)
+                {
+                        number[c] = vertices++;
+                }
+        }
+        m.vertices.resize(static_cast<std::size_t>(vertices) * n);
+        m.facet_vertices.resize(count);
+        parallel_parts(count, groups,
+                       [&](unsigned, const std::size_t b, const std::size_t e)
+                       {
+                               for (std::size_t c = b; c < e; ++c)
+                               {
+                                       const std::uint32_t v = number[first[c]];
+                                       m.facet_vertices[c] = static_cast<int>(v);
+                                       if (first[c] == c)
+                                       {
+                                               corner(c, &m.vertices[static_cast<std::size_t>(v) * n]);
+                                       }
+                               }
+                       });
+        m.facet_normals.assign(count, -1);
+        m.has_normal.assign(facets, 0);
+        m.facet_material.assign(facets, -1);
 }
 
 void read_stl(const std::filesystem::path& path, const int n, MeshFile& m)
 {
-        std::vector<char> data = read_bytes(path);
-        UniqueVertices unique(m);
+        Bytes data = read_bytes(path);
         const std::size_t header = 80;
         const std::size_t offset = header + sizeof(std::uint32_t);
         const std::size_t facet_bytes = static_cast<std::size_t>(n + n * n) * sizeof(float);
         bool binary = false;
         std::uint32_t count = 0;
-        if (data.size() > offset)
+        if (data.size > offset)
         {
-                std::memcpy(&count, &data[header], sizeof(count));
+                std::memcpy(&count, data.data() + header, sizeof(count));
                 const std::size_t required = offset + static_cast<std::size_t>(count) * facet_bytes;
-                binary = data.size() >= required && data.size() <= required + sizeof(std::uint16_t) &&
-                         std::any_of(data.begin(), data.end(),
+                binary = data.size >= required && data.size <= required + sizeof(std::uint16_t) &&
+                         std::any_of(data.data(), data.data() + data.size,
                                      [](const char c)
                                      {
                                              return !is_print(c) && !is_space(c);
@@ -830,20 +1046,15 @@ void read_stl(const std::filesystem::path& path, const int n, MeshFile& m)
         }
         if (binary)
         {
-                std::vector<float> v(static_cast<std::size_t>(n) * n);
-                const char* p = data.data() + offset + n * sizeof(float);
-                for (std::uint32_t f = 0; f < count; ++f)
-                {
-                        std::memcpy(v.data(), p, v.size() * sizeof(float));
-                        add_stl_facet(m, unique, v.data());
-                        p += facet_bytes;
-                }
+                // per facet: n normal floats (unused), then n corners of n floats
+                add_stl_facets(m, data.data() + offset + n * sizeof(float), facet_bytes, count);
         }
         else
         {
-                data.push_back('\0');
+                std::vector<float> corners; // each facet's n corners
+                data.data()[data.size] = '\0';
                 const char* p = data.data();
-                const char* const last = data.data() + data.size() - 1;
+                const char* const last = data.data() + data.size;
                 p = skip(p, last, is_space);
                 p = keyword(p, last, "solid");
                 p = skip(p, last, not_new_line);
@@ -885,8 +1096,11 @@ void read_stl(const std::filesystem::path& path, const int n, MeshFile& m)
                         p = keyword(p, last, "endloop");
                         p = skip(p, last, is_space);
                         p = keyword(p, last, "endfacet");
-                        add_stl_facet(m, unique, v.data());
+                        corners.insert(corners.end(), v.begin(), v.end());
                 }
+                const std::size_t facet_floats = static_cast<std::size_t>(n) * n;
+                add_stl_facets(m, reinterpret_cast<const char*>(corners.data()), facet_floats * sizeof(float),
+                               corners.size() / facet_floats);
         }
 }
 
