@@ -1405,6 +1405,86 @@ int oracle_load_mesh_file(const char* const path, const int n, const int stl, lo
                 });
 }
 
+// model::mesh::file::load_from_obj_file / load_from_stl_file alone, as
+// arrays: counts[0] vertices, [1] normals, [2] facets; with non-null
+// buffers also the vertices [V][n], the normals [M][n], and per facet its n
+// vertex indices, its n normal indices (-1 where it has none), has_normal
+// and its material (-1: none)
+int oracle_mesh_file_arrays(
+        const char* const path,
+        const int n,
+        const int stl,
+        long long* const counts,
+        float* const vertices,
+        float* const normals,
+        int* const facet_vertices,
+        int* const facet_normals,
+        unsigned char* const has_normal,
+        int* const facet_material)
+{
+        return guarded(
+                [&]
+                {
+                        ns::progress::Ratio progress(nullptr);
+                        const std::filesystem::path file(path);
+                        const auto fill = [&](const auto& mesh)
+                        {
+                                const int M = n;
+                                counts[0] = mesh->vertices.size();
+                                counts[1] = mesh->normals.size();
+                                counts[2] = mesh->facets.size();
+                                if (vertices == nullptr)
+                                {
+                                        return;
+                                }
+                                for (std::size_t i = 0; i < mesh->vertices.size(); ++i)
+                                {
+                                        for (int d = 0; d < M; ++d)
+                                        {
+                                                vertices[i * M + d] = mesh->vertices[i][d];
+                                        }
+                                }
+                                for (std::size_t i = 0; i < mesh->normals.size(); ++i)
+                                {
+                                        for (int d = 0; d < M; ++d)
+                                        {
+                                                normals[i * M + d] = mesh->normals[i][d];
+                                        }
+                                }
+                                for (std::size_t f = 0; f < mesh->facets.size(); ++f)
+                                {
+                                        const auto& facet = mesh->facets[f];
+                                        for (int k = 0; k < M; ++k)
+                                        {
+                                                facet_vertices[f * M + k] = facet.vertices[k];
+                                                facet_normals[f * M + k] = facet.has_normal ? facet.normals[k] : -1;
+                                        }
+                                        has_normal[f] = facet.has_normal ? 1 : 0;
+                                        facet_material[f] = facet.material;
+                                }
+                        };
+                        if (n == 3)
+                        {
+                                stl ? fill(ns::model::mesh::file::load_from_stl_file<3>(file, &progress, false))
+                                    : fill(ns::model::mesh::file::load_from_obj_file<3>(file, &progress));
+                        }
+                        else if (n == 4)
+                        {
+                                stl ? fill(ns::model::mesh::file::load_from_stl_file<4>(file, &progress, false))
+                                    : fill(ns::model::mesh::file::load_from_obj_file<4>(file, &progress));
+                        }
+                        else if (n == 5)
+                        {
+                                stl ? fill(ns::model::mesh::file::load_from_stl_file<5>(file, &progress, false))
+                                    : fill(ns::model::mesh::file::load_from_obj_file<5>(file, &progress));
+                        }
+                        else
+                        {
+                                throw std::runtime_error("dimension must be 3, 4 or 5");
+                        }
+                });
+}
+
 int oracle_scene_add_mesh(void* const scene)
 {
         int index = -1;

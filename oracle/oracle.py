@@ -50,6 +50,7 @@ def lib():
             "oracle_scene_add_mesh": (ctypes.c_int, [_P]),
             "oracle_scene_add_mesh_file": (ctypes.c_int, [_P, ctypes.c_char_p, _D, ctypes.c_double, ctypes.c_double, _F, ctypes.c_double]),
             "oracle_load_mesh_file": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _L]),
+            "oracle_mesh_file_arrays": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _L, _F, _F, _I, _I, _B, _I]),
             "oracle_scene_add_parallelotope_light": (ctypes.c_int, [_P, ctypes.c_int, _D, _F]),
             "oracle_scene_add_ball_light": (ctypes.c_int, [_P, _D, _D, ctypes.c_double, _F]),
             "oracle_scene_set_perspective": (ctypes.c_int, [_P, _D, _D, _D, ctypes.c_double, _I]),
@@ -362,3 +363,23 @@ def load_mesh_file(path, n: int) -> dict:
     stl = 1 if ".stl" in str(path).lower() else 0
     _check(lib().oracle_load_mesh_file(str(path).encode(), n, stl, ptr(counts, _L)))
     return {"vertices": int(counts[0]), "normals": int(counts[1]), "facets": int(counts[2])}
+
+
+def mesh_file_arrays(path, n: int) -> dict:
+    """The mesh the reference's own OBJ / STL loader reads from `path`, as
+    arrays: vertices [V, n], normals [M, n], and per facet its vertex and
+    normal indices [F, n] (-1 where the facet has no normals), has_normal [F]
+    and material [F] (-1: none)."""
+    counts = np.zeros(3, np.int64)
+    stl = 1 if ".stl" in str(path).lower() else 0
+    null = (None,) * 6
+    _check(lib().oracle_mesh_file_arrays(str(path).encode(), n, stl, ptr(counts, _L), *null))
+    v, m, f = (int(x) for x in counts)
+    out = {"vertices": np.zeros((v, n), np.float32), "normals": np.zeros((m, n), np.float32),
+           "facet_vertices": np.zeros((f, n), np.int32), "facet_normals": np.zeros((f, n), np.int32),
+           "has_normal": np.zeros(f, np.uint8), "facet_material": np.zeros(f, np.int32)}
+    _check(lib().oracle_mesh_file_arrays(
+        str(path).encode(), n, stl, ptr(counts, _L), ptr(out["vertices"], _F), ptr(out["normals"], _F),
+        ptr(out["facet_vertices"], _I), ptr(out["facet_normals"], _I), ptr(out["has_normal"], _B),
+        ptr(out["facet_material"], _I)))
+    return out

@@ -1,7 +1,9 @@
 """Mesh files (n-dimensional OBJ and STL) without a GPU: the library's loader
 accepts and rejects the same files as the reference's loaders
 (src/model/mesh/file/load_obj.cpp, load_stl.cpp, compiled into the oracle),
-and names file dimensions as file_type.cpp does."""
+reads the same arrays from them (tests/mesh_file_check.cpp against
+oracle_mesh_file_arrays, on files large enough for the loader's host
+threads), and names file dimensions as file_type.cpp does."""
 
 import numpy as np
 import pytest
@@ -125,3 +127,97 @@ def test_dimension_mismatch(tmp_path):
     path.write_text("v 0 0 0 0\n")
     r, err = add_file(L, 3, path)
     assert r < 0 and "dimension" in err
+
+
+# --------------------------------------------------------------------------
+# what the loader reads, array for array against the reference's loaders
+
+
+def build_check(tmp_path):
+    """tests/mesh_file_check.cpp with the library's loader, compiled here."""
+    import shutil
+    import subprocess
+    from pathlib import Path
+
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not available")
+    here = Path(__file__).resolve().parent
+    csrc = here.parent / "math_b200" / "csrc"
+    exe = tmp_path / "mesh_file_check"
+    subprocess.run(["g++", "-std=c++20", "-O2", "-ffp-contract=off", f"-I{csrc}", str(here / "mesh_file_check.cpp"),
+                    str(csrc / "mesh_files.cpp"), "-pthread", "-o", str(exe)], check=True)
+    return exe
+
+
+def read_check(exe, path, n, out):
+    import subprocess
+
+    subprocess.run([str(exe), str(path), str(n), str(out)], check=True)
+    data = out.read_bytes()
+    v, m, f = np.frombuffer(data[:24], np.int64)
+    o = 24
+    arrays = {}
+    for name, dtype, shape in (("vertices", np.float32, (v, n)), ("normals", np.float32, (m, n)),
+                               ("facet_vertices", np.int32, (f, n)), ("facet_normals", np.int32, (f, n)),
+                               ("has_normal", np.uint8, (f,)), ("facet_material", np.int32, (f,))):
+        size = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        arrays[name] = np.frombuffer(data[o:o + size], dtype).reshape(shape)
+        o += size
+    assert o == len(data)
+    return arrays
+
+
+def big_mesh(n):
+    """Meshes large enough that the loader splits the work over host threads
+    (more than 65,536 STL corners, more than 8,192 OBJ lines)."""
+    if n == 3:
+        p, f = scenes.icosphere(6)
+    else:
+        p, f = scenes.convex_hull_mesh(scenes.sphere_points(n, 5000 if n == 4 else 1500, 6))
+    p = np.asarray(p, np.float32)
+    # signed zeros, which the loaders merge, in some coordinates
+    p[::5, 0] = 0.0
+    p[2::5, 0] = -0.0
+    return p, np.asarray(f)
+
+
+@pytest.mark.parametrize("n", [3, 4, 5])
+def test_loaded_arrays_match_the_reference(tmp_path, n, oracle_lib):
+    """Vertices (merged STL corners numbered by first appearance), normals,
+    facet indices, flags and materials equal the reference loaders' output
+    bit for bit, for OBJ with normals on some facets, materials and relative
+    indices, and for ASCII and binary STL, one of them with NaN corners."""
+    import struct
+
+    from mesh_file_writers import facet_normals
+
+    exe = build_check(tmp_path)
+    p, f = big_mesh(n)
+    nrm = p / np.maximum(np.linalg.norm(p, axis=1, keepdims=True), 1e-30)
+    files = {"obj": tmp_path / ("m" + obj_extension(n)), "ascii": tmp_path / ("a" + stl_extension(n)),
+             "binary": tmp_path / ("b" + stl_extension(n)), "nan": tmp_path / ("c" + stl_extension(n))}
+    write_obj(files["obj"], p, f, normals=nrm, with_normals=(np.arange(len(f)) // 40) % 3 != 0,
+              materials={"red": (0.8, 0.1, 0.1), "blue": (0.1, 0.1, 0.8)},
+              facet_material=[("red", None, "blue")[(i // 70) % 3] for i in range(len(f))], relative_every=3)
+    write_stl_ascii(files["ascii"], p, f)
+    write_stl_binary(files["binary"], p, f)
+    q = p.copy()
+    q[7, 1] = np.nan
+    q[11, 0] = np.nan
+    fn = facet_normals(p.astype(np.float64), f).astype(np.float32)
+    with open(files["nan"], "wb") as h:
+        h.write(b"binary STL with NaN corners".ljust(80, b" "))
+        h.write(struct.pack("<I", len(f)))
+        for facet, normal in zip(f, fn):
+            h.write(normal.tobytes())
+            h.write(q[facet].tobytes())
+    for kind, path in files.items():
+        mine = read_check(exe, path, n, tmp_path / f"{kind}.bin")
+        ref = oracle_lib.mesh_file_arrays(path, n)
+        for name in ("vertices", "normals"):
+            assert mine[name].tobytes() == ref[name].tobytes(), (kind, name)
+        for name in ("facet_vertices", "facet_normals", "has_normal", "facet_material"):
+            assert np.array_equal(mine[name], ref[name]), (kind, name)
+        if kind != "obj":
+            # STL corners merged: fewer vertices than corners
+            assert len(mine["vertices"]) < len(f) * n
