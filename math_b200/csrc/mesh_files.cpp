@@ -132,6 +132,15 @@ bool is_print(const char c)
         return c >= '\x20' && c <= '\x7e';
 }
 
+// ASCII letters and digits (std::isalnum of the C locale, without its call)
+// and the other characters strtof's forms use: . + - ( ) _
+bool number_char(const char c)
+{
+        const char lower = static_cast<char>(c | 0x20);
+        return (c >= '0' && c <= '9') || (lower >= 'a' && lower <= 'z') || c == '.' || c == '+' || c == '-' ||
+               c == '(' || c == ')' || c == '_';
+}
+
 // What strtof reads (leading white space, an optional sign, decimal,
 // hexadecimal, infinity or NaN forms), with the reference's checks
 // (src/com/read.h): a number must be read, and it must be finite.  Decimal
@@ -146,8 +155,7 @@ bool read_float(const char*& s, float& out)
         const char* q = (*p == '+' && p[1] != '+' && p[1] != '-') ? p + 1 : p;
         // the characters a number can be made of; the text ends with a zero
         const char* line_end = q;
-        while (std::isalnum(static_cast<unsigned char>(*line_end)) || *line_end == '.' || *line_end == '+' ||
-               *line_end == '-' || *line_end == '(' || *line_end == ')' || *line_end == '_')
+        while (number_char(*line_end))
         {
                 ++line_end;
         }
