@@ -203,7 +203,7 @@ void read_floats(const char*& s, float* out, const int count)
 struct Lines final
 {
         Bytes data;
-        std::vector<std::size_t> begin;
+        std::vector<std::size_t> begin; // each line's start, then the end of the text
 
         explicit Lines(Bytes&& text)
                 : data(std::move(text))
@@ -245,28 +245,26 @@ struct Lines final
                 {
                         lines += part.size();
                 }
-                begin.reserve(lines);
-                std::size_t start = 0;
+                begin.reserve(lines + 1);
+                begin.push_back(0);
                 for (const std::vector<std::size_t>& part : ends)
                 {
                         for (const std::size_t end : part)
                         {
-                                begin.push_back(start);
-                                start = end + 1;
+                                begin.push_back(end + 1);
                         }
                 }
         }
 
         std::size_t size() const
         {
-                return begin.size();
+                return begin.empty() ? 0 : begin.size() - 1;
         }
 
         // the line without its terminator
         std::string_view line(const std::size_t i) const
         {
-                const char* const b = data.data() + begin[i];
-                return {b, std::strlen(b)};
+                return {data.data() + begin[i], begin[i + 1] - begin[i] - 1};
         }
 };
 
@@ -299,11 +297,8 @@ Split split(const std::string_view line)
         {
                 return {{p, static_cast<std::size_t>(q - p)}, q, q};
         }
-        const char* e = q;
-        while (e < last && *e != '#')
-        {
-                ++e;
-        }
+        const void* const comment = std::memchr(q, '#', last - q);
+        const char* const e = comment != nullptr ? static_cast<const char*>(comment) : last;
         return {{p, static_cast<std::size_t>(q - p)}, q, e};
 }
 
