@@ -232,10 +232,11 @@ __device__ float pt_brdf_channel(const BrdfTerms& t, const int zero, const Mater
 // their paths.  The sample points, the path's ray and its random stream are
 // those of the BPT kernels (the same stratified points, seed_seq{seed, pass,
 // pixel, sample + 1}); the reference's painter draws them the same way
-// whichever integrator it runs (painting.cpp:225-257).  beta stays in
-// registers; the colour too for RGB, while a spectrum accumulates in the
-// output row.  `estimates` holds 2 * light_count records per thread of the
-// grid.
+// whichever integrator it runs (painting.cpp:225-257).  Each lane keeps its
+// path's beta (all C channels: in registers for RGB, in the thread's local
+// memory for a spectrum) and, for RGB, its colour; a spectrum accumulates in
+// the output row.  `estimates` holds 2 * light_count records per thread of
+// the grid.
 template <int N, typename T, int C>
 __global__ void __launch_bounds__(128, NBPT_PT_MIN_BLOCKS) pt_paths_kernel(
         const DeviceScene<N, T, 1> scene,
