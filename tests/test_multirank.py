@@ -4,6 +4,7 @@ every rank's work (weak scaling; the path needs no data-path collective)."""
 
 from __future__ import annotations
 
+import datetime
 import os
 import socket
 
@@ -29,7 +30,8 @@ def rank_main(rank: int, world: int, port: int, out):
 
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
-    dist.init_process_group("gloo", rank=rank, world_size=world)
+    # a rank that never arrives ends the other's collective with an error
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
         seconds = [1.5, 2.5][rank]
         slowest = bench.slowest_rank(seconds, world, "cpu")
@@ -38,6 +40,7 @@ def rank_main(rank: int, world: int, port: int, out):
         dist.destroy_process_group()
 
 
+@pytest.mark.timeout(300)
 def test_two_ranks_take_the_slowest_time_and_count_all_work():
     world = 2
     port = free_port()
