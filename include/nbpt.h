@@ -69,6 +69,14 @@ typedef struct nbpt_statistics
         unsigned long long facets;     /* facet records tested, last pass */
         unsigned long long shapes;     /* other shapes tested, last pass */
         long long kernel_launches;     /* kernels launched by the last pass */
+        /* samples of all passes whose colour has a NaN or infinite channel:
+         * kept in the image and counted, as the reference logs them
+         * (src/painter/pixels/pixels.cpp:107-113) */
+        long long nonfinite_samples;
+        /* ray queries of all passes that found the BVH traversal stack full
+         * (none for trees the scene build accepts); nbpt_painter_wait fails
+         * when this is not zero */
+        long long stack_overflows;
 } nbpt_statistics;
 
 const char* nbpt_last_error(void);
@@ -342,6 +350,13 @@ int nbpt_scene_light_sample(
 /* raw PCG32 draws and uniform [0, 1) draws of a seed_seq stream, computed on the GPU */
 int nbpt_test_pcg(const unsigned* seed, int seed_words, int count, unsigned* out);
 int nbpt_test_canonical(const unsigned* seed, int seed_words, int count, int use_double, double* out);
+/* the host BVH build alone (no GPU needed): node count and the depth of the
+ * deepest leaf of the facet BVH of a mesh (vertices [vertex_count][dimension],
+ * facets [facet_count][dimension]); NBPT_ERROR when the tree is deeper than the
+ * traversal stack (64 entries, the reference's BvhStack:
+ * src/geometry/accelerators/bvh_stack.h:26), as nbpt_scene_finalize reports */
+int nbpt_test_bvh_build(int dimension, int precision, const double* vertices, long long vertex_count,
+                        const int* facets, long long facet_count, long long* nodes, int* depth);
 /* stratified jittered points of one pixel; returns the point count */
 int nbpt_test_sj_points(int dimension, int use_double, int spp, const unsigned* seed, int seed_words, double* out);
 

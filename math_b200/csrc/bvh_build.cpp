@@ -9,6 +9,7 @@
 #include <optional>
 #include <span>
 #include <stdexcept>
+#include <string>
 #include <vector>
 
 namespace nbpt::host
@@ -511,11 +512,12 @@ struct Layout final
                 return index;
         }
 
-        unsigned place(const TreeNode<N, T>& t)
+        unsigned place(const TreeNode<N, T>& t, const int depth)
         {
                 const unsigned node = push_node(t.bounds);
                 if (!t.first)
                 {
+                        out->depth = std::max(out->depth, depth);
                         out->offset[node] = out->indices.size();
                         out->count[node] = t.objects.size();
                         for (const Object<N, T>& o : t.objects)
@@ -525,8 +527,8 @@ struct Layout final
                         return node;
                 }
                 out->axis[node] = t.axis;
-                place(*t.first);
-                const unsigned second = place(*t.second);
+                place(*t.first, depth + 1);
+                const unsigned second = place(*t.second, depth + 1);
                 out->offset[node] = second;
                 return node;
         }
@@ -578,7 +580,13 @@ BuiltBvh<N, T> build_facet_bvh(const std::vector<T>& vertices, const std::vector
         out.lo.reserve(4 * count * N);
         out.hi.reserve(4 * count * N);
         Layout<N, T> layout{&out};
-        layout.place(*tree);
+        layout.place(*tree, 0);
+        if (out.depth > BVH_MAX_DEPTH)
+        {
+                throw std::runtime_error(
+                        "BVH depth " + std::to_string(out.depth) + " exceeds the traversal stack of " +
+                        std::to_string(BVH_MAX_DEPTH) + " entries (a degenerate mesh)");
+        }
         return out;
 }
 

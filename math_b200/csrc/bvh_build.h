@@ -20,6 +20,13 @@ namespace nbpt::host
 inline constexpr double BOX_R_RATE = 2.4e9;
 inline constexpr double SIMPLEX_RATE = 0.8e9;
 
+// Entries of the traversal stack (the reference's BvhStack holds 64,
+// src/geometry/accelerators/bvh_stack.h:26).  Depth-first traversal keeps at
+// most one entry per interior node above the current node, so a tree whose
+// leaves are at most this deep (root at depth 0) never overflows it; both
+// builders refuse deeper trees, which only degenerate meshes produce.
+inline constexpr int BVH_MAX_DEPTH = 64;
+
 template <int N, typename T>
 struct BuiltBvh final
 {
@@ -29,9 +36,11 @@ struct BuiltBvh final
         std::vector<std::uint32_t> count;  // 0 for interior nodes
         std::vector<std::uint32_t> axis;
         std::vector<std::uint32_t> indices; // facet per leaf slot
+        int depth = 0;                      // of the deepest leaf, the root at 0
 };
 
-// vertices: [V][N] in T; facets: [F][N] vertex indices.
+// vertices: [V][N] in T; facets: [F][N] vertex indices.  Throws
+// std::runtime_error if a leaf lies deeper than BVH_MAX_DEPTH.
 template <int N, typename T>
 BuiltBvh<N, T> build_facet_bvh(const std::vector<T>& vertices, const std::vector<int>& facets);
 } // namespace nbpt::host

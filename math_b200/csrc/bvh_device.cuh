@@ -163,6 +163,7 @@ struct BvhCounters final
                          // 4: a depth-first position out of range
         int root;        // reference of the root
         int root_size;
+        int depth;       // of the deepest leaf, the root at 0
 };
 
 // ---------------------------------------------------------------------------
@@ -1258,16 +1259,19 @@ __global__ void bvh_sizes_kernel(
 }
 
 template <int N, typename T>
-__device__ int bvh_preorder(int parent, int side, const BvhBuildNode<N, T>* inner)
+__device__ int bvh_preorder(int parent, int side, const BvhBuildNode<N, T>* inner, int* depth)
 {
         int index = 0;
+        int d = 0;
         while (parent >= 0)
         {
                 const BvhBuildNode<N, T>& p = inner[parent];
                 index += 1 + (side == 1 ? p.size[0] : 0);
                 side = p.side;
                 parent = p.parent;
+                ++d;
         }
+        *depth = d;
         return index;
 }
 
@@ -1278,18 +1282,21 @@ __global__ void bvh_preorder_kernel(
         const int* __restrict__ inner_list,
         const int inner_count,
         BvhBuildNode<N, T>* __restrict__ leaves,
-        BvhBuildNode<N, T>* __restrict__ inner)
+        BvhBuildNode<N, T>* __restrict__ inner,
+        BvhCounters* __restrict__ counters)
 {
         const int i = blockIdx.x * blockDim.x + threadIdx.x;
+        int depth = 0;
         if (i < leaf_count)
         {
                 BvhBuildNode<N, T>& n = leaves[leaf_list[i]];
-                n.preorder = bvh_preorder<N, T>(n.parent, n.side, inner);
+                n.preorder = bvh_preorder<N, T>(n.parent, n.side, inner, &depth);
+                atomicMax(&counters->depth, depth);
         }
         else if (i < leaf_count + inner_count)
         {
                 BvhBuildNode<N, T>& n = inner[inner_list[i - leaf_count]];
-                n.preorder = bvh_preorder<N, T>(n.parent, n.side, inner);
+                n.preorder = bvh_preorder<N, T>(n.parent, n.side, inner, &depth);
         }
 }
 

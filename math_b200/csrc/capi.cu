@@ -2,7 +2,9 @@
 // the thread-local error message around the C++ scene/painter classes.
 #include "../../include/nbpt.h"
 
+#include "bvh_build.h"
 #include "core.cuh"
+#include "cuda_error.h"
 #include "device_pool.h"
 #include "mesh_files.h"
 #include "painter_api.h"
@@ -42,12 +44,6 @@ namespace
 {
 thread_local std::string g_error;
 
-class CudaError final : public std::runtime_error
-{
-public:
-        using std::runtime_error::runtime_error;
-};
-
 template <typename F>
 int guarded(const F& f)
 {
@@ -55,18 +51,15 @@ int guarded(const F& f)
         {
                 return f();
         }
+        catch (const nbpt::CudaError& e)
+        {
+                g_error = e.what();
+                cudaGetLastError(); // a non-sticky error is cleared for the next call
+                return NBPT_CUDA_ERROR;
+        }
         catch (const std::exception& e)
         {
                 g_error = e.what();
-                const cudaError_t last = cudaGetLastError();
-                if (last != cudaSuccess || g_error.find("cuda") != std::string::npos)
-                {
-                        if (last != cudaSuccess)
-                        {
-                                g_error += std::string(" (") + cudaGetErrorString(last) + ")";
-                        }
-                        return NBPT_CUDA_ERROR;
-                }
                 return NBPT_ERROR;
         }
         catch (...)
@@ -142,6 +135,8 @@ void copy_statistics(const nbpt::Statistics& s, nbpt_statistics* statistics)
         statistics->facets = s.facets;
         statistics->shapes = s.shapes;
         statistics->kernel_launches = s.kernel_launches;
+        statistics->nonfinite_samples = s.nonfinite_samples;
+        statistics->stack_overflows = s.stack_overflows;
 }
 
 void require_device()
@@ -209,10 +204,7 @@ struct Buffer final
         X* p = nullptr;
         explicit Buffer(const std::size_t n)
         {
-                if (cudaMalloc(&p, n * sizeof(X)) != cudaSuccess)
-                {
-                        throw CudaError("cudaMalloc failed");
-                }
+                nbpt::cuda_check(cudaMalloc(&p, n * sizeof(X)), "cudaMalloc");
         }
         ~Buffer()
         {
@@ -257,10 +249,7 @@ int sj_points(const int dimension, const int spp, const std::uint32_t* seed, con
         cudaMemcpy(d_seed.p, seed, words * sizeof(std::uint32_t), cudaMemcpyHostToDevice);
         cudaMemcpy(d_offsets.p, offsets.data(), (k + 1) * sizeof(T), cudaMemcpyHostToDevice);
         sj_kernel<T><<<1, 1>>>(d_seed.p, words, dimension, k, d_offsets.p, d_out.p);
-        if (cudaDeviceSynchronize() != cudaSuccess)
-        {
-                throw CudaError("sj kernel failed");
-        }
+        nbpt::cuda_check(cudaDeviceSynchronize(), "sj kernel");
         cudaMemcpy(out, d_out.p, static_cast<std::size_t>(count) * dimension * sizeof(double), cudaMemcpyDeviceToHost);
         return count;
 }
@@ -1000,7 +989,7 @@ unsigned char* trace_scratch()
         const cudaError_t e = cudaGetDevice(&device);
         if (e != cudaSuccess)
         {
-                throw CudaError(std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+                throw nbpt::CudaError("cudaGetDevice", e);
         }
         if (device < 0 || device >= NOALLOC_MAX_DEVICES)
         {
@@ -1014,8 +1003,8 @@ unsigned char* trace_scratch()
                 const cudaError_t r = cudaGetSymbolAddress(&address, g_trace_scratch);
                 if (r != cudaSuccess || !address)
                 {
-                        throw CudaError(std::string("cudaGetSymbolAddress of the trace scratch: ") +
-                                        cudaGetErrorString(r));
+                        throw nbpt::CudaError("cudaGetSymbolAddress of the trace scratch",
+                                              r != cudaSuccess ? r : cudaErrorInvalidSymbol);
                 }
                 g_trace_scratch_address[device] = static_cast<unsigned char*>(address);
         }
@@ -1027,7 +1016,7 @@ void copy_checked(void* to, const void* from, const long long bytes, const cudaM
         const cudaError_t e = cudaMemcpy(to, from, static_cast<std::size_t>(bytes), kind);
         if (e != cudaSuccess)
         {
-                throw CudaError(std::string("cudaMemcpy: ") + cudaGetErrorString(e));
+                throw nbpt::CudaError("cudaMemcpy", e);
         }
 }
 } // namespace
@@ -1175,10 +1164,7 @@ int nbpt_test_pcg(const unsigned* seed, const int seed_words, const int count, u
                         Buffer<std::uint32_t> d_out(count);
                         cudaMemcpy(d_seed.p, seed, seed_words * sizeof(std::uint32_t), cudaMemcpyHostToDevice);
                         pcg_kernel<<<1, 1>>>(d_seed.p, seed_words, count, d_out.p);
-                        if (cudaDeviceSynchronize() != cudaSuccess)
-                        {
-                                throw CudaError("pcg kernel failed");
-                        }
+                        nbpt::cuda_check(cudaDeviceSynchronize(), "pcg kernel");
                         cudaMemcpy(out, d_out.p, count * sizeof(std::uint32_t), cudaMemcpyDeviceToHost);
                         return 0;
                 });
@@ -1194,10 +1180,7 @@ int nbpt_test_canonical(const unsigned* seed, const int seed_words, const int co
                         Buffer<double> d_out(count);
                         cudaMemcpy(d_seed.p, seed, seed_words * sizeof(std::uint32_t), cudaMemcpyHostToDevice);
                         canonical_kernel<<<1, 1>>>(d_seed.p, seed_words, count, use_double, d_out.p);
-                        if (cudaDeviceSynchronize() != cudaSuccess)
-                        {
-                                throw CudaError("canonical kernel failed");
-                        }
+                        nbpt::cuda_check(cudaDeviceSynchronize(), "canonical kernel");
                         cudaMemcpy(out, d_out.p, count * sizeof(double), cudaMemcpyDeviceToHost);
                         return 0;
                 });
@@ -1226,4 +1209,69 @@ int nbpt_test_sj_points(
                                           : sj_points<float>(dimension, spp, seed, seed_words, out);
                 });
 }
+}
+
+namespace
+{
+template <int N, typename T>
+void host_bvh_depth(const double* vertices, const long long vertex_count, const int* facets,
+                    const long long facet_count, long long* nodes, int* depth)
+{
+        std::vector<T> v(static_cast<std::size_t>(vertex_count) * N);
+        for (std::size_t i = 0; i < v.size(); ++i)
+        {
+                v[i] = static_cast<T>(vertices[i]);
+        }
+        std::vector<int> f(facets, facets + facet_count * N);
+        for (const int k : f)
+        {
+                if (k < 0 || k >= vertex_count)
+                {
+                        throw std::runtime_error("facet vertex index out of range");
+                }
+        }
+        const nbpt::host::BuiltBvh<N, T> bvh = nbpt::host::build_facet_bvh<N, T>(v, f);
+        if (nodes)
+        {
+                *nodes = static_cast<long long>(bvh.count.size());
+        }
+        if (depth)
+        {
+                *depth = bvh.depth;
+        }
+}
+} // namespace
+
+int nbpt_test_bvh_build(const int dimension, const int precision, const double* vertices, const long long vertex_count,
+                        const int* facets, const long long facet_count, long long* nodes, int* depth)
+{
+        return guarded(
+                [&]
+                {
+                        require(vertices, "vertices");
+                        require(facets, "facets");
+                        if (facet_count <= 0 || vertex_count <= 0)
+                        {
+                                throw std::runtime_error("No objects to build BVH");
+                        }
+                        const bool d = precision == NBPT_DOUBLE;
+                        switch (dimension)
+                        {
+                        case 3:
+                                d ? host_bvh_depth<3, double>(vertices, vertex_count, facets, facet_count, nodes, depth)
+                                  : host_bvh_depth<3, float>(vertices, vertex_count, facets, facet_count, nodes, depth);
+                                break;
+                        case 4:
+                                d ? host_bvh_depth<4, double>(vertices, vertex_count, facets, facet_count, nodes, depth)
+                                  : host_bvh_depth<4, float>(vertices, vertex_count, facets, facet_count, nodes, depth);
+                                break;
+                        case 5:
+                                d ? host_bvh_depth<5, double>(vertices, vertex_count, facets, facet_count, nodes, depth)
+                                  : host_bvh_depth<5, float>(vertices, vertex_count, facets, facet_count, nodes, depth);
+                                break;
+                        default:
+                                throw std::runtime_error("dimension must be 3, 4 or 5");
+                        }
+                        return 0;
+                });
 }

@@ -1,6 +1,8 @@
 // Device memory cache of the library's buffers (device_pool.h).
 #include "device_pool.h"
 
+#include "cuda_error.h"
+
 #include <cuda_runtime.h>
 
 #include <map>
@@ -62,7 +64,7 @@ void* allocate(const std::size_t bytes, int* const device)
         cudaError_t e = cudaGetDevice(&d);
         if (e != cudaSuccess)
         {
-                throw std::runtime_error(std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+                throw CudaError("cudaGetDevice", e);
         }
         *device = d;
         const std::size_t size = rounded(bytes);
@@ -93,8 +95,7 @@ void* allocate(const std::size_t bytes, int* const device)
         if (e != cudaSuccess)
         {
                 cudaGetLastError();
-                throw std::runtime_error(std::string("cudaMalloc of ") + std::to_string(size) +
-                                         " bytes: " + cudaGetErrorString(e));
+                throw CudaError("cudaMalloc of " + std::to_string(size) + " bytes", e);
         }
         return p;
 }

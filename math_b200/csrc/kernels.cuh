@@ -218,6 +218,8 @@ struct PathStats final
         unsigned long long nodes;
         unsigned long long facets;
         unsigned long long shapes;
+        unsigned long long overflows; // ray queries ended on a full traversal stack (an error)
+        unsigned long long nonfinite; // samples whose colour has a NaN or infinite channel
 };
 
 template <int C>
@@ -264,6 +266,24 @@ __device__ inline void add_counters(const QueryCounters& counters, PathStats* co
                 atomicAdd(&stats->facets, c);
                 atomicAdd(&stats->shapes, d);
         }
+        if (counters.overflows != 0)
+        {
+                atomicAdd(&stats->overflows, static_cast<unsigned long long>(counters.overflows));
+        }
+}
+
+// A sample colour with a NaN or infinite channel is counted, as the
+// reference logs it (src/painter/pixels/pixels.cpp:107-113), and kept.
+template <int K>
+__device__ inline bool all_finite(const float (&c)[K])
+{
+        bool ok = true;
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+        {
+                ok = ok && isfinite(c[k]);
+        }
+        return ok;
 }
 
 // A queued strategy: the path's index in its chunk, t and s.
@@ -615,7 +635,8 @@ __global__ void __launch_bounds__(128) paths_replay_kernel(
         const int words_per_path,
         float* __restrict__ colors,
         float* __restrict__ lum,
-        const float* __restrict__ cie_y)
+        const float* __restrict__ cie_y,
+        PathStats* __restrict__ stats)
 {
         static_assert(C % LANES == 0 && 32 % LANES == 0);
         constexpr int K = C / LANES;
@@ -772,6 +793,10 @@ __global__ void __launch_bounds__(128) paths_replay_kernel(
                         c.c[k] = color[k];
                 }
                 lum[i] = has ? luminance(c, cie_y) : 0.0f;
+                if (has && !all_finite(color))
+                {
+                        atomicAdd(&stats->nonfinite, 1ull);
+                }
         }
         else
         {
@@ -791,6 +816,11 @@ __global__ void __launch_bounds__(128) paths_replay_kernel(
                 if (lane == 0)
                 {
                         lum[i] = has ? sum : 0.0f;
+                }
+                const bool bad = __any_sync(0xffffffffu, !all_finite(color));
+                if (lane == 0 && has && bad)
+                {
+                        atomicAdd(&stats->nonfinite, 1ull);
                 }
         }
 }

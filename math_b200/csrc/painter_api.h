@@ -20,6 +20,8 @@ struct Statistics final
         unsigned long long facets;     // facet records tested, last pass
         unsigned long long shapes;     // other shapes tested, last pass
         long long kernel_launches;     // kernels launched by the last pass
+        long long nonfinite_samples;   // samples with a NaN or infinite colour, all passes
+        long long stack_overflows;     // ray queries cut short by a full traversal stack, all passes
 };
 
 // painter::Integrator (src/painter/painter.h:143-147), same order

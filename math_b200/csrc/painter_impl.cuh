@@ -13,6 +13,7 @@
 
 #include "bvh_build.h"
 #include "bvh_device.cuh"
+#include "cuda_error.h"
 #include "mesh_files.h"
 #include "device_pool.h"
 #include "estimator.cuh"
@@ -28,6 +29,7 @@
 #include <array>
 #include <chrono>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -42,14 +44,6 @@
 
 namespace nbpt
 {
-inline void cuda_check(const cudaError_t e, const char* what)
-{
-        if (e != cudaSuccess)
-        {
-                throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
-        }
-}
-
 #define NBPT_CUDA(x) ::nbpt::cuda_check((x), #x)
 
 template <typename X>
@@ -622,8 +616,14 @@ int build_device_bvh(
                 throw std::runtime_error("BVH build: the tree does not reach every node");
         }
         bvh_preorder_kernel<N, T><<<blocks_for(h.leaves + h.inner, 128), 128>>>(
-                leaf_list.get(), h.leaves, inner_list.get(), h.inner, leaves.get(), inner.get());
+                leaf_list.get(), h.leaves, inner_list.get(), h.inner, leaves.get(), inner.get(), counters.get());
         NBPT_CUDA(cudaGetLastError());
+        NBPT_CUDA(cudaMemcpy(&h, counters.get(), sizeof(h), cudaMemcpyDeviceToHost));
+        if (h.depth > host::BVH_MAX_DEPTH)
+        {
+                throw std::runtime_error("BVH depth " + std::to_string(h.depth) + " exceeds the traversal stack of " +
+                                         std::to_string(host::BVH_MAX_DEPTH) + " entries (a degenerate mesh)");
+        }
         const int node_count = h.leaves + h.inner;
         nodes.allocate(node_count);
         bvh_write_kernel<N, T><<<blocks_for(node_count, 128), 128>>>(
@@ -2228,6 +2228,7 @@ public:
                 valid_.allocate(samples);
                 state_.allocate(pixels_);
                 stats_.allocate(1);
+                NBPT_CUDA(cudaMemsetAsync(stats_.get(), 0, sizeof(PathStats), stream_));
                 rgb_.allocate(pixels_ * 3);
                 rgba_.allocate(pixels_ * 4);
                 int device = 0;
@@ -2303,7 +2304,9 @@ public:
                 for (int k = 0; k < passes; ++k)
                 {
                         const std::uint32_t pass = static_cast<std::uint32_t>(pass_++);
-                        NBPT_CUDA(cudaMemsetAsync(stats_.get(), 0, sizeof(PathStats), stream_));
+                        // per-pass counters; overflows and nonfinite count over the
+                        // painter's life
+                        NBPT_CUDA(cudaMemsetAsync(stats_.get(), 0, offsetof(PathStats, overflows), stream_));
                         NBPT_CUDA(cudaEventRecord(ev_start_, stream_));
                         sj_points_kernel<N - 1, T><<<blocks_for(pixels_, 128), 128, 0, stream_>>>(
                                 0, pixels_, seed_, pass, strata_, offsets_.get(), points_.get());
@@ -2369,7 +2372,7 @@ public:
                                                 scene_->device_materials(), scene_->device_lights(),
                                                 scene.shading.fresnel_a, scene.shading.fresnel_b, max_depth_, n, tape_.get(),
                                                 tape_words_, colors_.get() + b * spp_ * C, lum_.get() + b * spp_,
-                                                scene_->cie() + 64);
+                                                scene_->cie() + 64, stats_.get());
                                         NBPT_CUDA(cudaGetLastError());
                                         launches += 4;
                                 }
@@ -2437,6 +2440,14 @@ public:
                 statistics_.facets = s.facets;
                 statistics_.shapes = s.shapes;
                 statistics_.kernel_launches = launches_;
+                statistics_.nonfinite_samples = static_cast<long long>(s.nonfinite);
+                statistics_.stack_overflows = static_cast<long long>(s.overflows);
+                if (s.overflows != 0)
+                {
+                        throw std::runtime_error(std::to_string(s.overflows) +
+                                                 " ray queries found the BVH traversal stack full; the image is "
+                                                 "incomplete");
+                }
         }
 
         void images(float* rgb, float* rgba) override

@@ -1,6 +1,8 @@
 // Passes of a painter on a worker thread (pass_stream.h).
 #include "pass_stream.h"
 
+#include "cuda_error.h"
+
 #include <cuda_runtime.h>
 
 #include <stdexcept>
@@ -14,7 +16,7 @@ void check(const cudaError_t e, const char* what)
 {
         if (e != cudaSuccess)
         {
-                throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+                throw CudaError(what, e);
         }
 }
 

@@ -437,6 +437,10 @@ __global__ void __launch_bounds__(128, NBPT_PT_MIN_BLOCKS) pt_paths_kernel(
                                 out[c] = reg.c[c];
                         }
                         lum[i] = luminance(reg, cie_y);
+                        if (!all_finite(reg.c))
+                        {
+                                atomicAdd(&stats->nonfinite, 1ull);
+                        }
                 }
                 else
                 {
@@ -447,6 +451,10 @@ __global__ void __launch_bounds__(128, NBPT_PT_MIN_BLOCKS) pt_paths_kernel(
                                 final_color.c[c] = out[c];
                         }
                         lum[i] = luminance(final_color, cie_y);
+                        if (!all_finite(final_color.c))
+                        {
+                                atomicAdd(&stats->nonfinite, 1ull);
+                        }
                 }
                 valid[i] = 1;
                 i = -1;

@@ -19,6 +19,7 @@
 // closest hit, any hit) and src/painter/shapes/*.cpp (per-shape tests).
 #pragma once
 
+#include "bvh_build.h"
 #include "core.cuh"
 #include "geometry.cuh"
 #include "shading.cuh"
@@ -214,6 +215,7 @@ struct QueryCounters final
         std::uint32_t nodes;
         std::uint32_t facets;
         std::uint32_t shapes;
+        std::uint32_t overflows; // queries that ended on a full traversal stack
 };
 
 template <int N, typename T, int C>
@@ -241,7 +243,7 @@ struct SceneQueries final
                 const std::uint32_t* const indices = s.indices + mesh.index_offset;
                 const Facet<N, T>* const facets = s.facets + mesh.facet_offset;
 
-                std::uint32_t stack[64];
+                std::uint32_t stack[host::BVH_MAX_DEPTH];
                 int top = 0;
                 std::uint32_t node_index = 0;
                 int result = -1;
@@ -254,6 +256,13 @@ struct SceneQueries final
                         {
                                 if (node.count == 0)
                                 {
+                                        if (top == host::BVH_MAX_DEPTH)
+                                        {
+                                                // the builders refuse trees this deep; end the
+                                                // query rather than write past the stack
+                                                ++counters.overflows;
+                                                break;
+                                        }
                                         if ((neg >> node.axis) & 1u)
                                         {
                                                 stack[top++] = node_index + 1;
@@ -317,7 +326,7 @@ struct SceneQueries final
                 const std::uint32_t* const indices = s.indices + mesh.index_offset;
                 const Facet<N, T>* const facets = s.facets + mesh.facet_offset;
 
-                std::uint32_t stack[64];
+                std::uint32_t stack[host::BVH_MAX_DEPTH];
                 int top = 0;
                 std::uint32_t node_index = 0;
                 while (true)
@@ -329,6 +338,13 @@ struct SceneQueries final
                         {
                                 if (node.count == 0)
                                 {
+                                        if (top == host::BVH_MAX_DEPTH)
+                                        {
+                                                // the builders refuse trees this deep; end the
+                                                // query rather than write past the stack
+                                                ++counters.overflows;
+                                                return false;
+                                        }
                                         if ((neg >> node.axis) & 1u)
                                         {
                                                 stack[top++] = node_index + 1;

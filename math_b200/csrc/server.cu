@@ -1,6 +1,9 @@
 // Render-job server (server.h).
 #include "server.h"
 
+#include "cuda_error.h"
+
+
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -356,6 +359,9 @@ void Server::run()
                 }
 
                 bool progressed = false;
+                // renders whose creation ran out of device memory go back to the
+                // head of the queue in their admission (= arrival) order
+                std::size_t returned = 0;
                 for (const std::shared_ptr<Job>& j : running)
                 {
                         std::string error;
@@ -370,9 +376,9 @@ void Server::run()
                                         {
                                                 j->owned = j->scene->create_painter(j->spp, j->max_depth, j->seed);
                                         }
-                                        catch (const std::exception& e)
+                                        catch (const CudaError& e)
                                         {
-                                                if (std::string(e.what()).find("out of memory") == std::string::npos)
+                                                if (e.code() != cudaErrorMemoryAllocation)
                                                 {
                                                         throw;
                                                 }
@@ -396,7 +402,8 @@ void Server::run()
                                                 used_ -= j->info.footprint;
                                                 j->info.state = JobState::QUEUED;
                                                 j->info.started = -1;
-                                                queue_.push_front(j);
+                                                queue_.insert(queue_.begin() + static_cast<std::ptrdiff_t>(returned), j);
+                                                ++returned;
                                                 budget_ = used_;
                                                 continue;
                                         }
@@ -411,8 +418,7 @@ void Server::run()
                                         }
                                         if (e != cudaSuccess)
                                         {
-                                                throw std::runtime_error(std::string("pass failed: ") +
-                                                                         cudaGetErrorString(e));
+                                                throw CudaError("pass failed", e);
                                         }
                                         j->pass_in_flight = false;
                                         progressed = true;
@@ -430,18 +436,12 @@ void Server::run()
                                 {
                                         if (!j->done)
                                         {
-                                                if (cudaEventCreateWithFlags(&j->done, cudaEventDisableTiming) !=
-                                                    cudaSuccess)
-                                                {
-                                                        throw std::runtime_error("cudaEventCreate failed");
-                                                }
+                                                cuda_check(cudaEventCreateWithFlags(&j->done, cudaEventDisableTiming),
+                                                           "cudaEventCreateWithFlags");
                                         }
                                         j->painter->enqueue_passes(1);
-                                        if (cudaEventRecord(j->done, static_cast<cudaStream_t>(j->painter->stream())) !=
-                                            cudaSuccess)
-                                        {
-                                                throw std::runtime_error("cudaEventRecord failed");
-                                        }
+                                        cuda_check(cudaEventRecord(j->done, static_cast<cudaStream_t>(j->painter->stream())),
+                                                   "cudaEventRecord");
                                         j->pass_in_flight = true;
                                         progressed = true;
                                 }

@@ -58,6 +58,8 @@ class Statistics(ctypes.Structure):
         ("facets", ctypes.c_ulonglong),
         ("shapes", ctypes.c_ulonglong),
         ("kernel_launches", ctypes.c_longlong),
+        ("nonfinite_samples", ctypes.c_longlong),
+        ("stack_overflows", ctypes.c_longlong),
     ]
 
     def as_dict(self) -> dict:
@@ -123,6 +125,7 @@ SIGNATURES = [
     ("nbpt_test_pcg", ctypes.c_int, [_U, ctypes.c_int, ctypes.c_int, _U]),
     ("nbpt_test_canonical", ctypes.c_int, [_U, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D]),
     ("nbpt_test_sj_points", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _U, ctypes.c_int, _D]),
+    ("nbpt_test_bvh_build", ctypes.c_int, [ctypes.c_int, ctypes.c_int, _D, ctypes.c_longlong, _I, ctypes.c_longlong, _L, _I]),
 ]
 
 

@@ -323,16 +323,22 @@ MIXED_SCREENS = {3: (128, 512), 4: (32, 96), 5: (16, 32)}
 MIXED_POINTS = {3: (2000, 200000), 4: (2000, 200000), 5: (2000, 50000)}
 
 
+def _mixed_scene_args(a):
+    return mixed_scene(*a)
+
+
 def mixed_batch(count: int = 64, seed: int = 4, points_scale: float = 1.0, screen_scale: float = 1.0,
-                spp=(4, 64), depth=(5, 8)) -> list[dict]:
+                spp=(4, 64), depth=(5, 8), workers: int = 1) -> list[dict]:
     """Jobs of the batched mixed-scene workload: dimension uniform in
     {3, 4, 5}; hull of N points on the unit sphere with N log-uniform in the
     dimension's range (MIXED_POINTS: 2k-200k, at most 50k in 5-space, where
     hulls grow fastest); screen edge uniform in MIXED_SCREENS; samples per
     pixel log-uniform in `spp`; maximum depth uniform in `depth`.  The scale
-    arguments shrink hulls and screens for quick runs."""
+    arguments shrink hulls and screens for quick runs.  With `workers` > 1
+    the hulls are computed in that many processes (started with `spawn`, so
+    a process that already uses the GPU can call it); the jobs are the same."""
     rng = np.random.default_rng(seed)
-    jobs = []
+    params = []
     for k in range(count):
         n = int(rng.integers(3, 6))
         lo, hi = MIXED_POINTS[n]
@@ -342,9 +348,21 @@ def mixed_batch(count: int = 64, seed: int = 4, points_scale: float = 1.0, scree
         edge = max(4, int(round(rng.uniform(a, b) * screen_scale)))
         job_spp = int(round(math.exp(rng.uniform(math.log(spp[0]), math.log(spp[1])))))
         job_depth = int(rng.integers(depth[0], depth[1] + 1))
-        jobs.append({"desc": mixed_scene(n, points, [edge] * (n - 1), seed * 1000 + k),
-                     "spp": job_spp, "max_depth": job_depth, "points": points})
-    return jobs
+        params.append(((n, points, [edge] * (n - 1), seed * 1000 + k), job_spp, job_depth, points))
+    args = [p[0] for p in params]
+    if workers > 1 and count > 1:
+        import multiprocessing
+
+        # largest hulls first, so the pool's last tasks are short
+        order = sorted(range(count), key=lambda i: -(args[i][1] * 4 ** args[i][0]))
+        with multiprocessing.get_context("spawn").Pool(min(workers, count)) as pool:
+            built = pool.map(_mixed_scene_args, [args[i] for i in order], chunksize=1)
+        descs = [None] * count
+        for i, d in zip(order, built):
+            descs[i] = d
+    else:
+        descs = [mixed_scene(*a) for a in args]
+    return [{"desc": d, "spp": p[1], "max_depth": p[2], "points": p[3]} for d, p in zip(descs, params)]
 
 
 CONFIGS = {
