@@ -1,20 +1,26 @@
 """Benchmark: bidirectional path tracing paths/s on one B200.
 
-Workload (the configuration the headline metric is quoted on): the 4-space
-Cornell box with a 3-sphere hull mesh (20,000 points on S^3, ~135k
-3-simplex facets), a rotated 4-parallelotope and one 3-parallelotope light,
-64-bin spectral colour, a 64x64x64 voxel screen, 16 requested samples per
-voxel (27 rendered: the stratified sampler rounds up to 3^3), maximum path
-depth 6.  Inputs are synthetic, generated from fixed seeds
+Headline workload (the default, `--workload batch`): the mixed-scene batch
+the metric is quoted on.  64 scenes (seed 4), dimension uniform in
+{3, 4, 5}: a box of parallelotope walls, one parallelotope light and the
+convex hull of N points on the unit (n-1)-sphere (N log-uniform in
+[2k, 200k]; 5-space hulls capped at 50k points), screens 128^2-512^2,
+32^3-96^3 or 16^4-32^4, 4-64 samples per pixel log-uniform, maximum depth
+5-8, RGB.  Inputs are synthetic, generated from fixed seeds
 (math_b200/scenes.py).
 
-One step is one painter pass: every voxel's 27 paths traced, connected and
-folded into the pixel estimator (7,077,888 paths).  `value` is paths/s over
-the timed steps on the device (CUDA events on the painter's stream, L2
-flushed between steps), `e2e` the same through the C ABI with the image read
-back to host memory every step.  `--impl reference` runs the reference's own
-CPU painter (compiled from its sources, oracle/_ref) on this machine's host
-cores on a bounded slab of the same workload.
+One step is one pass of every job (770 M paths) through the job server in
+FP32, all jobs submitted at once.  `value` is paths/s over the timed steps
+on the device (CUDA events on the jobs' streams, first kernel to last, L2
+flushed between steps); `plain_fp64` the same jobs in FP64 one at a time;
+`e2e` the whole batch through the C ABI from host arrays (scene builds,
+copies, images back); `serve` a Poisson stream of renders into the server
+with its p50/p99 latency.  `--impl reference` runs the reference's own CPU
+painter (compiled from its sources, oracle/_ref) on this machine's host
+cores, one job at a time, on bounded samples of every job.
+
+The single-scene workloads (`cornell4d`, `cornell3d`, `sphere4d`) time
+painter passes of one scene the same way.
 """
 
 from __future__ import annotations
@@ -63,11 +69,11 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--screen", type=int, default=None,
                    help="edge of the voxel screen (default: the workload's 64), for smaller profiling runs")
-    p.add_argument("--workload", default="cornell4d", choices=["cornell4d", "cornell3d", "sphere4d", "batch", "serve", "meshfile"],
-                   help="cornell4d: the headline benchmark; cornell3d, sphere4d: the other single-scene "
-                        "workloads; batch: the mixed-scene batch, FP32 through the "
-                        "job server against plain FP64 one job at a time; serve: Poisson arrivals of renders "
-                        "into the job server, with completion latencies")
+    p.add_argument("--workload", default="batch", choices=["batch", "cornell4d", "cornell3d", "sphere4d", "serve", "meshfile"],
+                   help="batch (the headline): the 64-scene mixed batch, FP32 through the job server against "
+                        "plain FP64 one job at a time, with a served stream beside it; cornell4d, cornell3d, "
+                        "sphere4d: single-scene workloads; serve: Poisson arrivals of renders into the job server "
+                        "at --rate for --duration; meshfile: OBJ / STL reading")
     p.add_argument("--integrator", default="bpt", choices=["bpt", "pt"],
                    help="single-scene workloads: bidirectional (the headline) or path tracing")
     p.add_argument("--jobs", type=int, default=64, help="batch: scenes in the batch")
@@ -77,6 +83,16 @@ def parse():
     p.add_argument("--duration", type=float, default=20.0, help="serve: seconds of arrivals")
     p.add_argument("--pool", type=int, default=16, help="serve: distinct scenes the jobs draw from")
     p.add_argument("--max-jobs", type=int, default=16, help="batch/serve: jobs the server runs at once")
+    p.add_argument("--waves", type=int, default=4,
+                   help="batch: the batch is split into this many waves of about equal paths; a step is one wave")
+    p.add_argument("--e2e-steps", type=int, default=0,
+                   help="batch: steps (waves) of the end-to-end measurement (0: one whole batch)")
+    p.add_argument("--serve-duration", type=float, default=20.0,
+                   help="batch: seconds of arrivals of the served stream beside it (0: none)")
+    p.add_argument("--serve-load", type=float, default=0.7,
+                   help="batch: offered load of that stream, as a fraction of the measured batched throughput")
+    p.add_argument("--ref-target", type=int, default=100000,
+                   help="batch: paths per job of the reference painter's bounded samples")
     args = p.parse_args()
     if args.precision is None:
         args.precision = workload_of(args)["precision"]
@@ -433,106 +449,146 @@ def rel_rmse(a, b) -> float:
     return float(np.sqrt(((a.astype(np.float64) - b) ** 2).sum() / den)) if den > 0 else 0.0
 
 
-def run_batch(args):
-    """The mixed-scene batch: every job rendered once (one pass of its
-    samples per pixel) in FP64 one job at a time, then in FP32 through the
-    job server, all jobs submitted at once; wall time of each whole batch
-    with the scenes resident."""
-    from math_b200 import painter as P
-    from math_b200 import scenes
+# ---------------------------------------------------------------------------
+# The headline workload: 64 mixed scenes in 3/4/5-space (seed 4), batched
+# FP32 through the job server against the plain FP64 path one job at a time
 
+BATCH_SEED = 4
+SERVE_SEED = 5
+BATCH_LABEL = ("mixed-scene batch: 64 scenes, dimension uniform in {3,4,5}, box of parallelotope walls, one "
+               "parallelotope light and the convex hull of N points on the unit (n-1)-sphere (N log-uniform in "
+               "[2k, 200k], 5-space capped at 50k), screens 128^2-512^2 / 32^3-96^3 / 16^4-32^4, 4-64 spp "
+               "log-uniform (rounded up by the stratified sampler), depth 5-8, RGB, seed 4")
+
+
+def rank_jobs(paths: list[int], world: int) -> list[list[int]]:
+    """Whole jobs per rank (no data-path collective): the largest job first,
+    each to the rank with the fewest paths so far."""
+    loads = [0] * world
+    out: list[list[int]] = [[] for _ in range(world)]
+    for i in sorted(range(len(paths)), key=lambda k: -paths[k]):
+        r = min(range(world), key=lambda q: (loads[q], q))
+        out[r].append(i)
+        loads[r] += paths[i]
+    return [sorted(x) for x in out]
+
+
+def sample_desc(desc: dict, spp_actual: int, target: int) -> dict:
+    """The job's scene with its screen edge cut so one pass renders at most
+    about `target` paths at the job's own samples per pixel.  The projector's
+    field of view (or extent) is kept, so the rays keep their distribution
+    and every path costs what it costs in the full job."""
+    import copy
+
+    n = desc["n"]
+    d = copy.deepcopy(desc)
+    size = d["projector"]["size"]
+    edge = max(2, min(size[0], int((target / spp_actual) ** (1.0 / (n - 1)))))
+    if d["projector"]["type"] == "parallel":
+        d["projector"]["units_per_pixel"] *= size[0] / edge
+    d["projector"]["size"] = [edge] * (n - 1)
+    return d
+
+
+def reference_job_rates(jobs: list[dict], target: int, threads: int, steps: int = 1, warmup: int = 0) -> dict:
+    """The reference's own painter (create_painter, float, RGB, all `threads`
+    host threads) over a bounded sample of every job: the job's scene and
+    samples per pixel on a screen cut to about `target` paths (sample_desc).
+    Returns per-job paths/s (mean over `steps` passes) and the batch's
+    paths/s extrapolated to the full jobs: sum(paths) / sum(paths / rate)."""
+    from oracle import oracle
+
+    built = []
     t0 = time.perf_counter()
-    jobs = scenes.mixed_batch(args.jobs, seed=4, points_scale=args.points_scale, screen_scale=args.screen_scale)
-    generate_s = time.perf_counter() - t0
-    fp64 = [P.Scene(j["desc"], "double", False) for j in jobs]
-    fp32 = [P.Scene(j["desc"], "float", False) for j in jobs]
-    paths = sum(s.pixels * s.actual_spp(j["spp"]) for s, j in zip(fp32, jobs))
-
-    def plain():
-        images = []
-        for s, j in zip(fp64, jobs):
-            p = s.painter(j["spp"], j["max_depth"], seed=1)
-            p.run(1)
-            images.append(p.images()[0])
-            p.close()
-        return images
-
-    server = P.Server(max_jobs=args.max_jobs)
-    try:
-        batch_timed(args, server, jobs, fp64, fp32, paths, generate_s, plain)
-    finally:
-        server.close()
+    for j in jobs:
+        aspp = j["paths"] // int(np.prod(j["desc"]["projector"]["size"]))
+        built.append(oracle.Scene(sample_desc(j["desc"], aspp, target), "float", False))
+    build_s = time.perf_counter() - t0
+    rates = [[] for _ in jobs]
+    sampled = 0
+    seconds = 0.0
+    for step in range(warmup + steps):
+        for k, (s, j) in enumerate(zip(built, jobs)):
+            st, _ = s.paint(j["spp"], j["max_depth"], passes=1, threads=threads)
+            if step >= warmup:
+                rates[k].append(st["sample_count"] / st["pass_duration"])
+                sampled += st["sample_count"]
+                seconds += st["pass_duration"]
+    rate = [float(np.mean(r)) for r in rates]
+    full = sum(j["paths"] for j in jobs) / sum(j["paths"] / r for j, r in zip(jobs, rate))
+    return {"value": full, "job_rates": rate, "sampled_paths": sampled, "sampled_seconds": seconds,
+            "scene_build_s": build_s}
 
 
-def batch_timed(args, server, jobs, fp64, fp32, paths, generate_s, plain):
-    from math_b200 import scenes
-
-    def batched():
-        ids = [server.submit_render(s, j["spp"], j["max_depth"], seed=1, passes=1) for s, j in zip(fp32, jobs)]
-        images = []
-        for s, i in zip(fp32, ids):
-            server.wait(i)
+def batch_step(server, built: list, jobs: list[dict], seed: int = 1, read_images: bool = True) -> dict:
+    """One step of the batch: every job one pass (its samples per pixel)
+    through the job server, all submitted at once; the images read back.
+    `span` is the device time from the first job's first kernel to the last
+    job's last (CUDA events on the jobs' streams)."""
+    ids = [server.submit_render(s, j["spp"], j["max_depth"], seed=seed, passes=1) for s, j in zip(built, jobs)]
+    first, last = [], []
+    totals = {"paths": 0, "launches": 0, "bytes": 0.0, "rays": 0, "nodes": 0, "facets": 0, "nonfinite": 0}
+    images = []
+    for s, i in zip(built, ids):
+        info = server.wait(i)
+        st = server.statistics(i)
+        first.append(info["device_started"])
+        last.append(info["device_finished"])
+        size = record_bytes(s.n, s.precision)
+        totals["paths"] += st["sample_count"]
+        totals["launches"] += st["kernel_launches"] + 1  # + the images' resolve kernel
+        totals["bytes"] += st["nodes"] * size["node"] + st["facets"] * size["facet"] + st["shapes"] * size["shape"]
+        totals["rays"] += st["ray_count"]
+        totals["nodes"] += st["nodes"]
+        totals["facets"] += st["facets"]
+        totals["nonfinite"] += st["nonfinite_samples"]
+        if read_images:
             images.append(server.images(i, s.pixels)[0])
-            server.release(i)
-        return images
-
-    for _ in range(max(1, args.warmup)):
-        batched()
-    plain()
-    t0 = time.perf_counter()
-    ref = plain()
-    plain_s = time.perf_counter() - t0
-    best = None
-    for _ in range(max(1, args.steps)):
-        t0 = time.perf_counter()
-        img = batched()
-        dt = time.perf_counter() - t0
-        best = dt if best is None else min(best, dt)
-    rmse = [rel_rmse(a, b) for a, b in zip(img, ref)]
-    dims = [j["desc"]["n"] for j in jobs]
-    line = {
-        "metric": "batched_fp32_paths_per_second", "value": paths / best, "unit": "paths/s",
-        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-        "plain_fp64": {"value": paths / plain_s, "seconds": plain_s,
-                       "note": "one job at a time: painter, one pass, image read back"},
-        "batched_fp32": {"value": paths / best, "seconds": best,
-                         "note": f"all jobs submitted to the job server ({args.max_jobs} at once), "
-                                 "created at admission, images read back; best of the timed batches"},
-        "speedup_vs_plain_fp64": plain_s / best,
-        "same_seed_rel_rmse_fp32_vs_fp64": {
-            "median": float(np.median(rmse)), "max": float(np.max(rmse)),
-            "note": "one pass each: float rounding moves paths off their double twins, so this is sample "
-                    "noise, not bias; bias is tested against converged double images in tests/"},
-        "dtype": "f32 (batched) / f64 (plain)", "data": "synthetic (seeded generators)",
-        "config": {"workload": "mixed-scene batch: box, ceiling light and sphere hull in 3/4/5-space, RGB",
-                   "jobs": len(jobs), "dims": {str(n): dims.count(n) for n in (3, 4, 5)},
-                   "paths": paths, "facets_max": max(scenes.describe(j["desc"])["facets"] for j in jobs),
-                   "points_scale": args.points_scale, "screen_scale": args.screen_scale,
-                   "generate_s": generate_s},
-    }
-    print(json.dumps(line), flush=True)
+        server.release(i)
+    totals["span"] = max(last) - min(first)
+    totals["images"] = images
+    return totals
 
 
-def run_serve(args):
-    """Poisson arrivals of renders into the job server: each job draws a
-    scene from a pool of mixed-batch scenes (resident, FP32) and a sample
-    budget log-uniform in [16, 256] samples per pixel; the server creates the
-    render when it admits the job.  Latency is completion minus arrival."""
+def e2e_step(server, jobs: list[dict], precision: str, builders: int = 4) -> dict:
+    """One step of the batch end to end through the public API: every
+    scene built from host arrays (nbpt_scene_* on `builders` host threads,
+    each job submitted as soon as its scene is on the device), one pass per
+    job through the job server, RGB and RGBA images read back."""
+    from concurrent.futures import ThreadPoolExecutor
+
     from math_b200 import painter as P
-    from math_b200 import scenes
 
-    def note(msg):
-        print(f"serve: {msg}", file=sys.stderr, flush=True)
+    t0 = time.perf_counter()
+    h2d = d2h = 0
+    with ThreadPoolExecutor(builders) as ex:
+        futures = [ex.submit(P.Scene, j["desc"], precision, False) for j in jobs]
+        built, ids = [], []
+        for f, j in zip(futures, jobs):
+            s = f.result()
+            built.append(s)
+            ids.append(server.submit_render(s, j["spp"], j["max_depth"], seed=1, passes=1))
+        for s, i in zip(built, ids):
+            server.wait(i)
+            rgb, rgba = server.images(i, s.pixels)
+            d2h += rgb.nbytes + rgba.nbytes
+            h2d += s.upload_bytes()
+            server.release(i)
+            s.close()
+    return {"seconds": time.perf_counter() - t0, "h2d": h2d, "d2h": d2h}
 
-    pool = scenes.mixed_batch(args.pool, seed=5, points_scale=args.points_scale, screen_scale=args.screen_scale)
-    built = [P.Scene(j["desc"], "float", False) for j in pool]
-    note(f"{len(built)} pool scenes built")
-    rng = np.random.default_rng(5)
+
+def serve_stream(server, pool: list[dict], built: list, rate: float, duration: float, seed: int) -> dict:
+    """Poisson arrivals of renders into the job server (continuous batching):
+    each job draws a resident scene from the pool and a sample budget
+    log-uniform in [16, 256] samples per pixel; the server creates the render
+    when it admits the job.  Latency is completion minus arrival."""
+    rng = np.random.default_rng(seed)
     arrivals = []
     t = 0.0
     while True:
-        t += rng.exponential(1.0 / args.rate)
-        if t > args.duration:
+        t += rng.exponential(1.0 / rate)
+        if t > duration:
             break
         k = int(rng.integers(0, len(pool)))
         spp = int(round(math.exp(rng.uniform(math.log(16), math.log(256)))))
@@ -541,41 +597,6 @@ def run_serve(args):
         while built[k].actual_spp(spp) > 256:
             spp -= 1
         arrivals.append((t, k, spp))
-    server = P.Server(max_jobs=args.max_jobs)
-    try:
-        run_arrivals(args, server, pool, built, arrivals, note)
-    finally:
-        server.close()
-
-
-def wait_with_watchdog(server, job, all_jobs, note, limit: float = 60.0):
-    """Waits for a job by polling; if no job of the run progresses for
-    `limit` seconds, reports every job's state and gives up."""
-    last_change = time.perf_counter()
-    last = None
-    while True:
-        info = server.job(job)
-        if info["state"] in (2, 3):
-            return server.wait(job)
-        snapshot = [(j, server.job(j)["state"], server.job(j)["passes_done"]) for j in all_jobs]
-        if snapshot != last:
-            last = snapshot
-            last_change = time.perf_counter()
-        elif time.perf_counter() - last_change > limit:
-            note("no progress: " + ", ".join(f"{j}:{st}/{pd}" for j, st, pd in snapshot))
-            raise RuntimeError(f"job {job} made no progress for {limit} s")
-        time.sleep(0.01)
-
-
-def run_arrivals(args, server, pool, built, arrivals, note):
-    """Submits the arrivals on their schedule, waits for every job and
-    prints the serve line."""
-    # warm-up: one render of every pool scene
-    for s, j in zip(built, pool):
-        i = server.submit_render(s, 4, j["max_depth"], seed=1)
-        server.wait(i)
-        server.release(i)
-    note("warm-up done")
     t_start = server.time()
     submitted = []
     for a, k, spp in arrivals:
@@ -584,33 +605,317 @@ def run_arrivals(args, server, pool, built, arrivals, note):
         s = built[k]
         i = server.submit_render(s, spp, pool[k]["max_depth"], seed=len(submitted) + 1)
         submitted.append((i, t_start + a, s.pixels * s.actual_spp(spp)))
-    note(f"{len(submitted)} jobs submitted")
     latencies, waits = [], []
     last = t_start
-    pending = [j for j, _, _ in submitted]
     for i, arrival, _ in submitted:
-        info = wait_with_watchdog(server, i, pending, note)
-        pending.remove(i)
+        info = server.wait(i)
         latencies.append(info["finished"] - arrival)
         waits.append(info["started"] - arrival)
         last = max(last, info["finished"])
         server.release(i)
     paths = sum(p for _, _, p in submitted)
-    lat = np.array(latencies)
-    line = {
-        "metric": "served_job_latency_p99", "value": float(np.percentile(lat, 99)), "unit": "s",
-        "higher_is_better": False, "n_gpus": 1,
-        "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-        "mean_queue_wait_s": float(np.mean(waits)),
-        "jobs": len(submitted), "throughput_paths_per_second": paths / (last - t_start),
-        "offered_paths_per_second": paths / args.duration,
-        "makespan_s": last - t_start,
+    lat = np.array(latencies) if latencies else np.zeros(1)
+    return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "mean_queue_wait_s": float(np.mean(waits)) if waits else 0.0, "jobs": len(submitted),
+            "rate_per_s": rate, "duration_s": duration,
+            "throughput_paths_per_second": paths / (last - t_start) if last > t_start else None,
+            "offered_paths_per_second": paths / duration, "makespan_s": last - t_start}
+
+
+def flush_l2(buf):
+    import torch
+
+    buf.fill_(1)
+    torch.cuda.synchronize()
+
+
+def run_batch(args, rank: int, world: int, local: int):
+    import torch
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from math_b200 import painter as P
+    from math_b200 import scenes
+
+    workers = max(1, (os.cpu_count() or 1) // max(1, world))
+    all_paths = scenes.mixed_batch_paths(args.jobs, BATCH_SEED, args.screen_scale)
+    mine = rank_jobs(all_paths, world)[rank]
+    t0 = time.perf_counter()
+    jobs = scenes.mixed_batch(args.jobs, seed=BATCH_SEED, points_scale=args.points_scale,
+                              screen_scale=args.screen_scale, workers=workers, select=mine)
+    generate_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    fp32 = [P.Scene(j["desc"], "float", False) for j in jobs]
+    build_s = time.perf_counter() - t0
+    paths_per_batch = sum(j["paths"] for j in jobs)
+    # the rank's jobs in waves of about equal paths; a step renders one wave
+    waves = [[jobs[k] for k in w] for w in rank_jobs([j["paths"] for j in jobs], min(args.waves, len(jobs)))]
+    wave_scenes = [[fp32[jobs.index(j)] for j in w] for w in waves]
+    wave_paths = [sum(j["paths"] for j in w) for w in waves]
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    server = P.Server(max_jobs=args.max_jobs)
+    try:
+        for k in range(args.warmup):
+            flush_l2(flush)
+            w = k % len(waves)
+            batch_step(server, wave_scenes[w], waves[w], read_images=False)
+        if world > 1:
+            torch.distributed.barrier()
+        clocks = ClockSampler(local)
+        clocks.start()
+        spans = [[] for _ in waves]
+        totals = {"launches": 0, "bytes": 0.0, "rays": 0, "nodes": 0, "facets": 0, "nonfinite": 0, "paths": 0}
+        images = {}
+        for k in range(args.steps):
+            flush_l2(flush)
+            w = k % len(waves)
+            r = batch_step(server, wave_scenes[w], waves[w])
+            spans[w].append(r["span"])
+            for key in totals:
+                totals[key] += r[key]
+            for j, img in zip(waves[w], r["images"]):
+                images[j["index"]] = img
+        clock_info = clocks.stop()
+        torch.cuda.synchronize()
+        step_seconds = float(sum(sum(x) for x in spans))
+        if all(spans):
+            # every wave timed: the batch's rate from each wave's mean span
+            # (the plain sum when the steps cover whole batches)
+            batch_seconds = sum(float(np.mean(x)) for x in spans)
+            rank_rate = paths_per_batch / batch_seconds
+        else:
+            rank_rate = totals["paths"] / step_seconds
+        # whole batch over the slowest rank: every rank renders its jobs
+        batch_seconds = slowest_rank(paths_per_batch / rank_rate, world, "cuda")
+        value = sum(all_paths) / batch_seconds
+
+        # end to end through the public API: each wave's scenes from host
+        # arrays, its jobs through the server, images back
+        e2e_steps = max(1, args.e2e_steps if args.e2e_steps > 0 else len(waves))
+        e2e = {"seconds": 0.0, "h2d": 0, "d2h": 0}
+        e2e_paths = 0
+        for k in range(e2e_steps):
+            w = k % len(waves)
+            r = e2e_step(server, waves[w], "float")
+            e2e_paths += wave_paths[w]
+            for key in e2e:
+                e2e[key] += r[key]
+        e2e_rate = e2e_paths / e2e["seconds"]
+        e2e_value = sum(all_paths) / slowest_rank(paths_per_batch / e2e_rate, world, "cuda")
+
+        plain = None
+        serve = None
+        if world == 1:
+            plain = plain_fp64(args, jobs, paths_per_batch, [images.get(j["index"]) for j in jobs], flush)
+            if args.serve_duration > 0:
+                serve = serve_sub(args, server, workers, value)
+    finally:
+        server.close()
+
+    if rank == 0:
+        peaks = {}
+        try:
+            peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        except (OSError, ValueError):
+            pass
+        peak = peaks.get("hbm_gbs", 6650.0)
+        achieved = totals["bytes"] / step_seconds / 1e9 if step_seconds > 0 else None
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            cpu = batch_cpu_baseline(args, jobs)
+        dims = [j["desc"]["n"] for j in jobs]
+        line = {
+            "metric": "batched_fp32_paths_per_second", "value": value, "unit": "paths/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * step_seconds / args.steps,
+            "higher_is_better": True, "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded generators)",
+            "config": {"workload": BATCH_LABEL, "jobs": args.jobs, "jobs_this_rank": len(jobs),
+                       "dims": {str(n): dims.count(n) for n in (3, 4, 5)}, "paths_per_batch": sum(all_paths),
+                       "facets_max": max(scenes.describe(j["desc"])["facets"] for j in jobs),
+                       "waves": len(waves), "wave_paths": wave_paths,
+                       "step": (f"one wave: {len(jobs) // len(waves)} of the batch's jobs (the batch split into "
+                                f"{len(waves)} waves of about equal paths), one pass each at its own samples "
+                                "per pixel, all submitted to the job server at once, images read back; value = "
+                                "paths of the whole batch / the sum of the waves' mean device spans"),
+                       "max_jobs": args.max_jobs, "points_scale": args.points_scale,
+                       "screen_scale": args.screen_scale, "generate_s": generate_s, "scene_build_s": build_s,
+                       "l2": "flushed (256 MiB write) before every step; scenes and buffers exceed L2",
+                       "timing": "device span per step: CUDA events on the jobs' streams, from the first kernel of "
+                                 "the wave's first job to the last kernel of its last job"},
+            "plain_fp64": plain,
+            "speedup_vs_plain_fp64": (value / plain["value"]) if plain else None,
+            "e2e": {"value": e2e_value, "unit": "paths/s",
+                    "h2d_bytes_per_step": int(e2e["h2d"] / e2e_steps), "d2h_bytes_per_step": int(e2e["d2h"] / e2e_steps),
+                    "steps": e2e_steps, "seconds": e2e["seconds"],
+                    "note": "every step one wave through the C ABI: each scene built from host arrays (mesh "
+                            "ingestion, host->device copies, BVH build and facet setup on the GPU) on 4 host threads "
+                            "and submitted when ready, one pass per job, RGB and RGBA images read back; host clock"},
+            "serve": serve,
+            "gpu_launches": totals["launches"],
+            "nonfinite_samples": totals["nonfinite"],
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "traffic": None,
+                         "kernel": "whole steps: path kernels, estimator and resolve of all jobs, overlapped across "
+                                   "jobs (algorithmic scene bytes counted on the device / device span)",
+                         "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                         "algorithmic_bytes_per_path": totals["bytes"] / totals["paths"],
+                         "node_visits_per_path": totals["nodes"] / totals["paths"],
+                         "facet_tests_per_path": totals["facets"] / totals["paths"],
+                         "rays_per_path": totals["rays"] / totals["paths"]},
+            "clocks": clock_info,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def plain_fp64(args, jobs, paths_per_step, fp32_images, flush) -> dict:
+    """The plain comparator: the same jobs in FP64, one at a time (a job
+    server with one slot), the same kernels; one warm-up job per dimension,
+    then one timed batch."""
+    from math_b200 import painter as P
+
+    t0 = time.perf_counter()
+    fp64 = [P.Scene(j["desc"], "double", False) for j in jobs]
+    build_s = time.perf_counter() - t0
+    one = P.Server(max_jobs=1)
+    try:
+        seen = set()
+        for s, j in zip(fp64, jobs):
+            if j["desc"]["n"] not in seen:
+                seen.add(j["desc"]["n"])
+                batch_step(one, [s], [j], read_images=False)
+        flush_l2(flush)
+        w0 = time.perf_counter()
+        r = batch_step(one, fp64, jobs)
+        wall = time.perf_counter() - w0
+    finally:
+        one.close()
+    rmse = [rel_rmse(a, b) for a, b in zip(fp32_images or [], r["images"]) if a is not None]
+    for s in fp64:
+        s.close()
+    return {"value": paths_per_step / r["span"], "seconds": r["span"], "wall_seconds": wall,
+            "scene_build_s": build_s, "steps": 1,
+            "note": "FP64 scenes, one job at a time through a job server with one slot (painter created at "
+                    "admission, one pass, images read back), device span as for value",
+            "same_seed_rel_rmse_fp32_vs_fp64": {
+                "median": float(np.median(rmse)) if rmse else None, "max": float(np.max(rmse)) if rmse else None,
+                "note": "one pass each on the same streams: float rounding moves paths off their double twins, "
+                        "so this is per-pass sample noise, not bias (bias against converged FP64 images is in "
+                        "tests/test_config_parity.py)"}}
+
+
+def serve_sub(args, server, workers: int, capacity: float) -> dict:
+    """Served stream beside the batch: Poisson arrivals at a rate that offers
+    `serve_load` of the measured batched throughput (the stated 40 jobs/s
+    offers about 30 times what one B200 renders, so its queue only grows)."""
+    from math_b200 import painter as P
+    from math_b200 import scenes
+
+    pool = scenes.mixed_batch(args.pool, seed=SERVE_SEED, workers=workers)
+    built = [P.Scene(j["desc"], "float", False) for j in pool]
+    # mean paths per job of the arrival mix: pool scene x spp log-uniform [16, 256]
+    sizes = []
+    for s, j in zip(built, pool):
+        sp = [min(256, s.actual_spp(int(round(math.exp(x))))) for x in np.linspace(math.log(16), math.log(256), 9)]
+        sizes.append(s.pixels * float(np.mean(sp)))
+    mean_paths = float(np.mean(sizes))
+    rate = args.serve_load * capacity / mean_paths
+    for s, j in zip(built, pool):  # warm-up: one small render of every pool scene
+        i = server.submit_render(s, 4, j["max_depth"], seed=1)
+        server.wait(i)
+        server.release(i)
+    out = serve_stream(server, pool, built, rate, args.serve_duration, SERVE_SEED)
+    out["offered_load"] = args.serve_load
+    out["note"] = (f"Poisson arrivals for {args.serve_duration:.0f} s at {rate:.2f} jobs/s, offering "
+                   f"{args.serve_load:.0%} of the measured batched throughput; scenes drawn as in the batch "
+                   f"(seed {SERVE_SEED}, a resident pool of {args.pool}), 16-256 spp log-uniform.  The stated 40 "
+                   "jobs/s offers about 30x what one B200 renders: its queue grows without bound and p99 is set "
+                   "by the stream's length")
+    for s in built:
+        s.close()
+    return out
+
+
+def batch_cpu_baseline(args, jobs) -> dict:
+    """The reference painter on the host cores over a bounded sample of the
+    batch: every fourth job, each on a screen cut to about 100k paths."""
+    from oracle import oracle
+
+    if not oracle.available():
+        return {"value": None, "unit": "paths/s", "cores": 0, "kind": "reference",
+                "sample": "oracle library not built"}
+    subset = jobs[::4]
+    cores = os.cpu_count() or 1
+    r = reference_job_rates(subset, args.ref_target, cores, steps=1)
+    return {"value": r["value"], "unit": "paths/s", "cores": cores, "kind": "reference",
+            "sample": (f"the reference's create_painter (float, RGB) on {len(subset)} of the {len(jobs)} jobs "
+                       f"(every fourth), each job's scene, samples per pixel and depth on a screen cut to about "
+                       f"{args.ref_target} paths; {r['sampled_paths']} paths in {r['sampled_seconds']:.1f} s; "
+                       "value = sum(paths) / sum(paths / job rate) over the full jobs")}
+
+
+def run_reference_batch(args, rank: int):
+    """--impl reference on the batch: the reference's own CPU painter, one
+    job at a time, every job of the batch each step on a bounded sample."""
+    if rank != 0:
+        return
+    from math_b200 import scenes
+    from oracle import oracle
+
+    if not oracle.available():
+        print(json.dumps({"impl": "reference", "unavailable": "the reference painter (oracle/_ref) is not built"}))
+        return
+    cores = os.cpu_count() or 1
+    jobs = scenes.mixed_batch(args.jobs, seed=BATCH_SEED, points_scale=args.points_scale,
+                              screen_scale=args.screen_scale, workers=cores)
+    r = reference_job_rates(jobs, args.ref_target, cores, steps=args.steps, warmup=args.warmup)
+    value = r["value"]
+    paths = sum(j["paths"] for j in jobs)
+    sample = (f"each step: the reference's create_painter (float, RGB, {cores} threads) on every one of the "
+              f"{len(jobs)} jobs, one at a time, each job's scene, samples per pixel and depth on a screen cut to "
+              f"about {args.ref_target} paths; value = sum(paths) / sum(paths / job rate) over the full jobs "
+              f"({r['sampled_paths']} paths sampled in {r['sampled_seconds']:.1f} s)")
+    print(json.dumps({
+        "metric": "batched_fp32_paths_per_second", "value": value, "unit": "paths/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * paths / value, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded generators)",
-        "config": {"workload": "Poisson render arrivals into the job server", "rate_per_s": args.rate,
-                   "duration_s": args.duration, "pool_scenes": len(pool), "spp": "log-uniform 16-256",
-                   "max_jobs": args.max_jobs, "points_scale": args.points_scale,
-                   "screen_scale": args.screen_scale},
-    }
+        "config": {"workload": BATCH_LABEL, "jobs": args.jobs, "paths_per_step": paths},
+        "cpu_baseline": {"value": value, "unit": "paths/s", "cores": cores, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_serve(args):
+    """Poisson arrivals of renders into the job server at --rate jobs/s for
+    --duration s (C5 as stated: 40 jobs/s), with completion latencies."""
+    from math_b200 import painter as P
+    from math_b200 import scenes
+
+    pool = scenes.mixed_batch(args.pool, seed=SERVE_SEED, points_scale=args.points_scale,
+                              screen_scale=args.screen_scale, workers=os.cpu_count() or 1)
+    built = [P.Scene(j["desc"], "float", False) for j in pool]
+    server = P.Server(max_jobs=args.max_jobs)
+    try:
+        for s, j in zip(built, pool):
+            i = server.submit_render(s, 4, j["max_depth"], seed=1)
+            server.wait(i)
+            server.release(i)
+        out = serve_stream(server, pool, built, args.rate, args.duration, SERVE_SEED)
+    finally:
+        server.close()
+    line = {"metric": "served_job_latency_p99", "value": out["p99_s"], "unit": "s", "higher_is_better": False,
+            "n_gpus": 1, **out, "dtype": "f32", "data": "synthetic (seeded generators)",
+            "config": {"workload": "Poisson render arrivals into the job server", "rate_per_s": args.rate,
+                       "duration_s": args.duration, "pool_scenes": len(pool), "spp": "log-uniform 16-256",
+                       "max_jobs": args.max_jobs}}
     print(json.dumps(line), flush=True)
 
 
@@ -674,11 +979,13 @@ def main():
     args = parse()
     rank, world, local = dist_env()
     if args.impl == "reference":
-        run_reference(args, rank)
+        if args.workload == "batch":
+            run_reference_batch(args, rank)
+        else:
+            run_reference(args, rank)
         return
     if args.workload == "batch":
-        if rank == 0:
-            run_batch(args)
+        run_batch(args, rank, world, local)
         return
     if args.workload == "serve":
         if rank == 0:

@@ -121,6 +121,8 @@ void copy_info(const nbpt::JobInfo& j, nbpt_job_info* info)
         info->submitted = j.submitted;
         info->started = j.started;
         info->finished = j.finished;
+        info->device_started = j.device_started;
+        info->device_finished = j.device_finished;
 }
 
 void copy_statistics(const nbpt::Statistics& s, nbpt_statistics* statistics)
@@ -803,6 +805,25 @@ void* nbpt_painter_stream(nbpt_painter* painter)
         return s;
 }
 
+int nbpt_painter_cancel(nbpt_painter* painter)
+{
+        return guarded(
+                [&]
+                {
+                        if (!painter || !painter->impl)
+                        {
+                                throw std::runtime_error("null painter");
+                        }
+                        // allowed while the worker runs: Painter::cancel is thread safe
+                        if (painter->stream)
+                        {
+                                painter->stream->request_stop();
+                        }
+                        painter->impl->cancel();
+                        return 0;
+                });
+}
+
 nbpt_server* nbpt_server_create(const int max_jobs, const long long memory_budget)
 {
         nbpt_server* out = nullptr;
@@ -917,6 +938,26 @@ double nbpt_server_time(nbpt_server* server)
                         return 0;
                 });
         return t;
+}
+
+int nbpt_server_cancel(nbpt_server* server, const long long job)
+{
+        return guarded(
+                [&]
+                {
+                        server_of(server).cancel(job);
+                        return 0;
+                });
+}
+
+int nbpt_test_server_fail_allocations(nbpt_server* server, const int count)
+{
+        return guarded(
+                [&]
+                {
+                        server_of(server).fail_next_creations(count);
+                        return 0;
+                });
 }
 
 int nbpt_scene_trace(

@@ -286,6 +286,13 @@ __device__ inline bool all_finite(const float (&c)[K])
         return ok;
 }
 
+// The painter's cancel word, written by the host on another stream while a
+// pass runs (Painter::cancel); read from L2 on every test.
+__device__ inline bool cancelled(const unsigned* const cancel)
+{
+        return *static_cast<const volatile unsigned*>(cancel) != 0;
+}
+
 // A queued strategy: the path's index in its chunk, t and s.
 inline constexpr int TASK_PATH_SHIFT = 8;
 inline constexpr long long TASK_MAX_PATHS = 1LL << (32 - TASK_PATH_SHIFT);
@@ -360,7 +367,8 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_walk_kernel(
         unsigned char* __restrict__ valid,
         const TaskQueues queues,
         unsigned* __restrict__ next_path,
-        PathStats* __restrict__ stats)
+        PathStats* __restrict__ stats,
+        const unsigned* __restrict__ cancel)
 {
         using B = Bpt<N, T, 1, true>;
         using S = typename B::Subpaths;
@@ -377,6 +385,10 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_walk_kernel(
         {
                 if (i < 0)
                 {
+                        if (cancelled(cancel))
+                        {
+                                break; // the paths not taken keep no tape: the later kernels skip the chunk
+                        }
                         i = reserve_together(next_path, 1);
                         if (i >= paths)
                         {
@@ -550,11 +562,13 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_light_kernel
         std::uint32_t* __restrict__ tape,
         const int words_per_path,
         Arrival<N, T>* __restrict__ arrivals,
-        const TaskQueues queues)
+        const TaskQueues queues,
+        const unsigned* __restrict__ cancel)
 {
         const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
         unsigned queued = 0; // bit t - 2: strategy (1, t) queued
-        if (i < paths)
+        // a cancelled pass has paths without tapes (see paths_replay_kernel)
+        if (i < paths && !cancelled(cancel))
         {
                 std::uint32_t* const w = tape + i * static_cast<long long>(words_per_path);
                 const int camera_size = static_cast<int>(w[2]);
@@ -636,10 +650,17 @@ __global__ void __launch_bounds__(128) paths_replay_kernel(
         float* __restrict__ colors,
         float* __restrict__ lum,
         const float* __restrict__ cie_y,
-        PathStats* __restrict__ stats)
+        PathStats* __restrict__ stats,
+        const unsigned* __restrict__ cancel)
 {
         static_assert(C % LANES == 0 && 32 % LANES == 0);
         constexpr int K = C / LANES;
+        // a cancelled pass has paths without tapes: no thread reads them (a
+        // walk that stopped early wrote the word before this launch began)
+        if (__shfl_sync(0xffffffffu, cancelled(cancel) ? 1 : 0, 0) != 0)
+        {
+                return;
+        }
         const long long i = (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) / LANES;
         const int lane = static_cast<int>(threadIdx.x % LANES);
         if (i >= paths)

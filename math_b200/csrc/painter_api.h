@@ -48,6 +48,14 @@ public:
         virtual void* stream() = 0;
         // device bytes of the painter's buffers plus those of its scene
         virtual long long device_bytes() const = 0;
+        // Asks the passes in flight to take no more paths, as the reference's
+        // painter threads test their stop flag before every pixel
+        // (src/painter/painting/integrator_bpt.cpp:90-93); callable from any
+        // thread while a pass runs.  The pass ends early with an incomplete
+        // image, the next wait() reports the cancellation, and the painter
+        // takes no more passes.
+        virtual void cancel() = 0;
+        virtual bool cancelled() const = 0;
 };
 
 class Scene

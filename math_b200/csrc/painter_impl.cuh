@@ -2115,6 +2115,10 @@ class PainterT final : public Painter
         DeviceArray<unsigned char> valid_;
         DeviceArray<PixelState<C>> state_;
         DeviceArray<PathStats> stats_;
+        DeviceArray<unsigned> cancel_; // nonzero: the passes take no more paths
+        cudaStream_t cancel_stream_ = nullptr;
+        std::mutex cancel_mutex_;
+        std::atomic<bool> cancelled_{false};
         DeviceArray<float> rgb_;
         DeviceArray<float> rgba_;
         // per-path buffers of one chunk of pixels: subpath vertices, random
@@ -2229,6 +2233,8 @@ public:
                 state_.allocate(pixels_);
                 stats_.allocate(1);
                 NBPT_CUDA(cudaMemsetAsync(stats_.get(), 0, sizeof(PathStats), stream_));
+                cancel_.allocate(1);
+                NBPT_CUDA(cudaMemsetAsync(cancel_.get(), 0, sizeof(unsigned), stream_));
                 rgb_.allocate(pixels_ * 3);
                 rgba_.allocate(pixels_ * 4);
                 int device = 0;
@@ -2274,6 +2280,11 @@ public:
                         cudaStreamSynchronize(stream_);
                         cudaStreamDestroy(stream_);
                 }
+                if (cancel_stream_)
+                {
+                        cudaStreamSynchronize(cancel_stream_);
+                        cudaStreamDestroy(cancel_stream_);
+                }
                 for (cudaEvent_t e : {ev_start_, ev_paths_, ev_paths_end_, ev_end_})
                 {
                         if (e)
@@ -2298,8 +2309,33 @@ public:
                 return stream_;
         }
 
+        void cancel() override
+        {
+                const std::lock_guard lock(cancel_mutex_);
+                if (cancelled_)
+                {
+                        return;
+                }
+                if (!cancel_stream_)
+                {
+                        NBPT_CUDA(cudaStreamCreateWithFlags(&cancel_stream_, cudaStreamNonBlocking));
+                }
+                // on its own stream, so the word changes while the pass runs
+                NBPT_CUDA(cudaMemsetAsync(cancel_.get(), 1, 1, cancel_stream_));
+                cancelled_ = true;
+        }
+
+        bool cancelled() const override
+        {
+                return cancelled_;
+        }
+
         void enqueue_passes(const int passes) override
         {
+                if (cancelled_)
+                {
+                        throw std::runtime_error("the painter was cancelled");
+                }
                 const DeviceScene<N, T, C>& scene = scene_->device();
                 for (int k = 0; k < passes; ++k)
                 {
@@ -2328,7 +2364,7 @@ public:
                                                         points_.get() + b * spp_ * (N - 1), colors_.get() + b * spp_ * C,
                                                         lum_.get() + b * spp_, valid_.get() + b * spp_,
                                                         pt_estimates_.get(), next_path_.get(), stats_.get(),
-                                                        scene_->cie() + 64);
+                                                        scene_->cie() + 64, cancel_.get());
                                         NBPT_CUDA(cudaGetLastError());
                                         launches += 1;
                                 }
@@ -2357,11 +2393,11 @@ public:
                                                                   stream_>>>(
                                                 scene_1, b, e, spp_, max_depth_, seed_, pass, points_.get() + b * spp_ * (N - 1),
                                                 vertices_.get(), rng_.get(), tape_.get(), tape_words_, valid_.get() + b * spp_,
-                                                queues, next_path_.get(), stats_.get());
+                                                queues, next_path_.get(), stats_.get(), cancel_.get());
                                         NBPT_CUDA(cudaGetLastError());
                                         paths_light_kernel<N, T><<<blocks_for(n, 128), 128, 0, stream_>>>(
                                                 scene_1, n, max_depth_, vertices_.get(), rng_.get(), tape_.get(), tape_words_,
-                                                arrivals_.get(), queues);
+                                                arrivals_.get(), queues, cancel_.get());
                                         NBPT_CUDA(cudaGetLastError());
                                         paths_connect_kernel<N, T><<<connect_blocks_, 128, 0, stream_>>>(
                                                 scene_1, max_depth_, vertices_.get(), tape_.get(), tape_words_, arrivals_.get(),
@@ -2372,7 +2408,7 @@ public:
                                                 scene_->device_materials(), scene_->device_lights(),
                                                 scene.shading.fresnel_a, scene.shading.fresnel_b, max_depth_, n, tape_.get(),
                                                 tape_words_, colors_.get() + b * spp_ * C, lum_.get() + b * spp_,
-                                                scene_->cie() + 64, stats_.get());
+                                                scene_->cie() + 64, stats_.get(), cancel_.get());
                                         NBPT_CUDA(cudaGetLastError());
                                         launches += 4;
                                 }
@@ -2425,6 +2461,10 @@ public:
         void wait() override
         {
                 NBPT_CUDA(cudaStreamSynchronize(stream_));
+                if (cancelled_)
+                {
+                        throw std::runtime_error("cancelled: the pass in flight ended early and its image is incomplete");
+                }
                 PathStats s{};
                 stats_.download_on(&s, 1, stream_);
                 float ms = 0;

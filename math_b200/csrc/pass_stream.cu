@@ -111,6 +111,11 @@ void PassStream::stop()
         join();
 }
 
+void PassStream::request_stop()
+{
+        stop_ = true;
+}
+
 void PassStream::join()
 {
         const std::lock_guard lock(join_mutex_);

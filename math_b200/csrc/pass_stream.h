@@ -50,6 +50,8 @@ public:
 
         // asks the worker to stop after the pass in flight and waits for it
         void stop();
+        // asks the worker to stop after the pass in flight, without waiting
+        void request_stop();
         // waits for the worker to end
         void join();
         bool running() const;

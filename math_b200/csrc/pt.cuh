@@ -254,7 +254,8 @@ __global__ void __launch_bounds__(128, NBPT_PT_MIN_BLOCKS) pt_paths_kernel(
         PtEstimate* __restrict__ estimates,
         unsigned* __restrict__ next_path,
         PathStats* __restrict__ stats,
-        const float* __restrict__ cie_y)
+        const float* __restrict__ cie_y,
+        const unsigned* __restrict__ cancel)
 {
         constexpr bool IN_REGISTERS = C <= 4;
         const long long paths = (end - begin) * spp;
@@ -275,6 +276,10 @@ __global__ void __launch_bounds__(128, NBPT_PT_MIN_BLOCKS) pt_paths_kernel(
         {
                 if (i < 0)
                 {
+                        if (cancelled(cancel))
+                        {
+                                break;
+                        }
                         i = reserve_together(next_path, 1);
                         if (i >= paths)
                         {

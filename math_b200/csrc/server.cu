@@ -6,6 +6,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <chrono>
 #include <cstdlib>
 #include <set>
@@ -55,8 +56,11 @@ struct Server::Job final
         std::unique_ptr<Painter> owned;
         int device;
         JobInfo info;
-        cudaEvent_t done = nullptr; // marks the end of the pass in flight
+        cudaEvent_t first = nullptr; // marks the start of the first pass
+        cudaEvent_t done = nullptr;  // marks the end of the pass in flight
         bool pass_in_flight = false;
+        std::atomic<bool> cancel_requested{false};
+        bool cancel_sent = false;
 };
 
 Server::Server(const int max_jobs, const long long memory_budget)
@@ -87,6 +91,12 @@ Server::Server(const int max_jobs, const long long memory_budget)
         }
         initial_budget_ = budget_;
         {
+                cudaEvent_t e = nullptr;
+                cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+                reference_event_ = e;
+                cuda_check(cudaEventRecord(e, nullptr), "cudaEventRecord");
+        }
+        {
                 // registered after the CUDA runtime initialised above, so it
                 // runs before the runtime's own exit handlers
                 const std::lock_guard lock(g_live_mutex);
@@ -116,6 +126,10 @@ void Server::shutdown()
 Server::~Server()
 {
         shutdown();
+        if (reference_event_)
+        {
+                cudaEventDestroy(static_cast<cudaEvent_t>(reference_event_));
+        }
         const std::lock_guard lock(g_live_mutex);
         if (g_live)
         {
@@ -317,12 +331,65 @@ void Server::finish_locked(Job& job, const JobState state, const std::string& er
         job.info.finished = now();
         used_ -= job.info.footprint;
         budget_ = initial_budget_; // memory freed: admit by the estimate again
-        if (job.done)
+        cudaSetDevice(job.device);
+        if (state == JobState::DONE && job.first && job.done)
         {
-                cudaSetDevice(job.device);
-                cudaEventDestroy(job.done);
-                job.done = nullptr;
+                const cudaEvent_t reference = static_cast<cudaEvent_t>(reference_event_);
+                float a = 0;
+                float b = 0;
+                if (cudaEventElapsedTime(&a, reference, job.first) == cudaSuccess &&
+                    cudaEventElapsedTime(&b, reference, job.done) == cudaSuccess)
+                {
+                        job.info.device_started = a * 1e-3;
+                        job.info.device_finished = b * 1e-3;
+                }
+                else
+                {
+                        cudaGetLastError();
+                }
         }
+        for (cudaEvent_t* e : {&job.first, &job.done})
+        {
+                if (*e)
+                {
+                        cudaEventDestroy(*e);
+                        *e = nullptr;
+                }
+        }
+}
+
+void Server::cancel(const long long job)
+{
+        {
+                const std::lock_guard lock(mutex_);
+                const std::shared_ptr<Job> j = find_locked(job);
+                if (j->info.state == JobState::QUEUED)
+                {
+                        for (auto i = queue_.begin(); i != queue_.end(); ++i)
+                        {
+                                if (i->get() == j.get())
+                                {
+                                        queue_.erase(i);
+                                        break;
+                                }
+                        }
+                        // a queued job holds no device memory or budget
+                        j->info.state = JobState::FAILED;
+                        j->info.error = "cancelled";
+                        j->info.finished = now();
+                }
+                else if (j->info.state == JobState::RUNNING)
+                {
+                        j->cancel_requested = true;
+                }
+        }
+        changed_.notify_all();
+}
+
+void Server::fail_next_creations(const int count)
+{
+        const std::lock_guard lock(mutex_);
+        fail_creations_ = count;
 }
 
 // The worker keeps one pass of every running job in flight, on the job's own
@@ -369,11 +436,29 @@ void Server::run()
                         try
                         {
                                 cudaSetDevice(j->device);
+                                if (!j->painter && j->cancel_requested)
+                                {
+                                        throw std::runtime_error("cancelled");
+                                }
                                 if (!j->painter)
                                 {
                                         // a render created at admission
                                         try
                                         {
+                                                bool fail = false;
+                                                {
+                                                        const std::lock_guard lock(mutex_);
+                                                        if (fail_creations_ > 0)
+                                                        {
+                                                                --fail_creations_;
+                                                                fail = true;
+                                                        }
+                                                }
+                                                if (fail)
+                                                {
+                                                        throw CudaError("cudaMalloc (a failure the test asked for)",
+                                                                        cudaErrorMemoryAllocation);
+                                                }
                                                 j->owned = j->scene->create_painter(j->spp, j->max_depth, j->seed);
                                         }
                                         catch (const CudaError& e)
@@ -409,6 +494,24 @@ void Server::run()
                                         }
                                         j->painter = j->owned.get();
                                 }
+                                if (j->cancel_requested)
+                                {
+                                        if (j->pass_in_flight)
+                                        {
+                                                if (!j->cancel_sent)
+                                                {
+                                                        j->painter->cancel();
+                                                        j->cancel_sent = true;
+                                                }
+                                                const cudaError_t e = cudaEventQuery(j->done);
+                                                if (e == cudaErrorNotReady)
+                                                {
+                                                        continue;
+                                                }
+                                                j->pass_in_flight = false;
+                                        }
+                                        throw std::runtime_error("cancelled");
+                                }
                                 if (j->pass_in_flight)
                                 {
                                         const cudaError_t e = cudaEventQuery(j->done);
@@ -436,8 +539,14 @@ void Server::run()
                                 {
                                         if (!j->done)
                                         {
-                                                cuda_check(cudaEventCreateWithFlags(&j->done, cudaEventDisableTiming),
-                                                           "cudaEventCreateWithFlags");
+                                                cuda_check(cudaEventCreate(&j->done), "cudaEventCreate");
+                                        }
+                                        if (!j->first)
+                                        {
+                                                cuda_check(cudaEventCreate(&j->first), "cudaEventCreate");
+                                                cuda_check(cudaEventRecord(j->first,
+                                                                           static_cast<cudaStream_t>(j->painter->stream())),
+                                                           "cudaEventRecord");
                                         }
                                         j->painter->enqueue_passes(1);
                                         cuda_check(cudaEventRecord(j->done, static_cast<cudaStream_t>(j->painter->stream())),

@@ -40,6 +40,11 @@ struct JobInfo final
         double submitted;    // seconds since the server started
         double started;      // admitted (-1 while queued)
         double finished;     // done or failed (-1 before)
+        // device clock of the job's first pass start and last pass end, in
+        // seconds after the server's reference event (-1 before the job is
+        // done): CUDA events on the job's stream
+        double device_started = -1;
+        double device_finished = -1;
         std::string error;
 };
 
@@ -67,6 +72,13 @@ public:
         void release(long long job);
         JobInfo info(long long job) const;
         JobInfo wait(long long job);
+        // A queued job fails at once with the error "cancelled"; a running
+        // one stops taking paths in its pass in flight (Painter::cancel),
+        // then fails the same way.  A finished job is left as it is.
+        void cancel(long long job);
+        // test hook: the next `count` renders the server creates fail as if
+        // cudaMalloc had run out of device memory
+        void fail_next_creations(int count);
         double now() const;
         // finishes the running jobs, fails the queued ones and stops the
         // worker; the destructor calls it, and so does process exit for a
@@ -93,6 +105,8 @@ private:
         std::deque<std::shared_ptr<Job>> running_;
         long long next_id_ = 0;
         bool stop_ = false;
+        int fail_creations_ = 0;
+        void* reference_event_ = nullptr; // cudaEvent_t recorded at construction
         std::thread worker_;
 };
 } // namespace nbpt

@@ -40,6 +40,8 @@ class JobInfo(ctypes.Structure):
         ("submitted", ctypes.c_double),
         ("started", ctypes.c_double),
         ("finished", ctypes.c_double),
+        ("device_started", ctypes.c_double),
+        ("device_finished", ctypes.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -106,6 +108,7 @@ SIGNATURES = [
     ("nbpt_painter_samples", ctypes.c_int, [_P, _D, _F, _B]),
     ("nbpt_painter_statistics", ctypes.c_int, [_P, ctypes.POINTER(Statistics)]),
     ("nbpt_painter_stream", _P, [_P]),
+    ("nbpt_painter_cancel", ctypes.c_int, [_P]),
     ("nbpt_server_create", _P, [ctypes.c_int, ctypes.c_longlong]),
     ("nbpt_server_destroy", None, [_P]),
     ("nbpt_server_submit", ctypes.c_longlong, [_P, _P, ctypes.c_int]),
@@ -116,12 +119,14 @@ SIGNATURES = [
     ("nbpt_server_job", ctypes.c_int, [_P, ctypes.c_longlong, ctypes.POINTER(JobInfo)]),
     ("nbpt_server_wait", ctypes.c_int, [_P, ctypes.c_longlong, ctypes.POINTER(JobInfo)]),
     ("nbpt_server_time", ctypes.c_double, [_P]),
+    ("nbpt_server_cancel", ctypes.c_int, [_P, ctypes.c_longlong]),
     ("nbpt_scene_trace", ctypes.c_int, [_P, _D, ctypes.c_longlong, ctypes.c_int, _I, _I, _D, _D]),
     ("nbpt_scene_trace_noalloc", ctypes.c_int, [_P, _D, ctypes.c_longlong, ctypes.c_int, _I, _I, _D, _D]),
     ("nbpt_scene_mesh_export", ctypes.c_int, [_P, ctypes.c_int, _L, _D, _D, _D, _U, _U, _I]),
     ("nbpt_scene_brdf", ctypes.c_int, [_P, ctypes.c_int, _D, _D, _D, _F, _D]),
     ("nbpt_scene_brdf_sample", ctypes.c_int, [_P, ctypes.c_int, _D, _D, _U, ctypes.c_int, _D, _D, _F]),
     ("nbpt_scene_light_sample", ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, _U, ctypes.c_int, _D, _D, _F]),
+    ("nbpt_test_server_fail_allocations", ctypes.c_int, [_P, ctypes.c_int]),
     ("nbpt_test_pcg", ctypes.c_int, [_U, ctypes.c_int, ctypes.c_int, _U]),
     ("nbpt_test_canonical", ctypes.c_int, [_U, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D]),
     ("nbpt_test_sj_points", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _U, ctypes.c_int, _D]),
@@ -414,6 +419,9 @@ class Painter:
     def is_running(self) -> bool:
         return _check(lib().nbpt_painter_is_running(self.h)) == 1
 
+    def cancel(self):
+        _check(lib().nbpt_painter_cancel(self.h))
+
     def __del__(self):
         self.close()
 
@@ -521,6 +529,21 @@ class Server:
 
     def time(self) -> float:
         return lib().nbpt_server_time(self.h)
+
+    def cancel(self, job: int):
+        _check(lib().nbpt_server_cancel(self.h, job))
+
+    def try_wait(self, job: int) -> dict:
+        """wait() that returns the failed job's info (with "error") instead of raising."""
+        info = JobInfo()
+        r = lib().nbpt_server_wait(self.h, job, ctypes.byref(info))
+        d = info.as_dict()
+        d["error"] = lib().nbpt_last_error().decode() if r < 0 else None
+        return d
+
+    def fail_next_allocations(self, count: int):
+        """test hook: the next `count` renders created at admission fail as out of device memory"""
+        _check(lib().nbpt_test_server_fail_allocations(self.h, count))
 
     def close(self):
         h = getattr(self, "h", None)

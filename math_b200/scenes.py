@@ -327,8 +327,18 @@ def _mixed_scene_args(a):
     return mixed_scene(*a)
 
 
+def stratified_spp(spp: int, dimension: int) -> int:
+    """Samples per pixel the stratified jittered sampler renders: spp rounded
+    up to k^dimension (src/sampling/sj_sampler.h:51-75)."""
+    v = spp ** (1.0 / dimension)
+    k = int(math.floor(v))
+    if k ** dimension < spp:
+        k = int(math.ceil(v))
+    return k ** dimension
+
+
 def mixed_batch(count: int = 64, seed: int = 4, points_scale: float = 1.0, screen_scale: float = 1.0,
-                spp=(4, 64), depth=(5, 8), workers: int = 1) -> list[dict]:
+                spp=(4, 64), depth=(5, 8), workers: int = 1, select=None) -> list[dict]:
     """Jobs of the batched mixed-scene workload: dimension uniform in
     {3, 4, 5}; hull of N points on the unit sphere with N log-uniform in the
     dimension's range (MIXED_POINTS: 2k-200k, at most 50k in 5-space, where
@@ -336,7 +346,9 @@ def mixed_batch(count: int = 64, seed: int = 4, points_scale: float = 1.0, scree
     pixel log-uniform in `spp`; maximum depth uniform in `depth`.  The scale
     arguments shrink hulls and screens for quick runs.  With `workers` > 1
     the hulls are computed in that many processes (started with `spawn`, so
-    a process that already uses the GPU can call it); the jobs are the same."""
+    a process that already uses the GPU can call it); the jobs are the same.
+    `select`: indices of the jobs to build (the others are left out); every
+    job carries "paths", its paths per pass."""
     rng = np.random.default_rng(seed)
     params = []
     for k in range(count):
@@ -349,6 +361,9 @@ def mixed_batch(count: int = 64, seed: int = 4, points_scale: float = 1.0, scree
         job_spp = int(round(math.exp(rng.uniform(math.log(spp[0]), math.log(spp[1])))))
         job_depth = int(rng.integers(depth[0], depth[1] + 1))
         params.append(((n, points, [edge] * (n - 1), seed * 1000 + k), job_spp, job_depth, points))
+    chosen = list(range(count)) if select is None else sorted(set(select))
+    params = [params[i] for i in chosen]
+    count = len(params)
     args = [p[0] for p in params]
     if workers > 1 and count > 1:
         import multiprocessing
@@ -362,7 +377,24 @@ def mixed_batch(count: int = 64, seed: int = 4, points_scale: float = 1.0, scree
             descs[i] = d
     else:
         descs = [mixed_scene(*a) for a in args]
-    return [{"desc": d, "spp": p[1], "max_depth": p[2], "points": p[3]} for d, p in zip(descs, params)]
+    return [{"desc": d, "spp": p[1], "max_depth": p[2], "points": p[3], "index": i,
+             "paths": int(np.prod(p[0][2])) * stratified_spp(p[1], p[0][0] - 1)}
+            for i, d, p in zip(chosen, descs, params)]
+
+
+def mixed_batch_paths(count: int = 64, seed: int = 4, screen_scale: float = 1.0, spp=(4, 64)) -> list[int]:
+    """Paths per pass of each job of mixed_batch, without building scenes."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(rng.integers(3, 6))
+        rng.uniform()  # hull points
+        a, b = MIXED_SCREENS[n]
+        edge = max(4, int(round(rng.uniform(a, b) * screen_scale)))
+        job_spp = int(round(math.exp(rng.uniform(math.log(spp[0]), math.log(spp[1])))))
+        rng.integers(5, 9)  # depth
+        out.append(edge ** (n - 1) * stratified_spp(job_spp, n - 1))
+    return out
 
 
 CONFIGS = {
