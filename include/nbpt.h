@@ -236,6 +236,13 @@ int nbpt_painter_statistics(nbpt_painter* painter, nbpt_statistics* statistics);
 /* the CUDA stream (cudaStream_t) the painter's passes run on, for callers
  * that order their own work or events with it */
 void* nbpt_painter_stream(nbpt_painter* painter);
+/* Stops the painter as the reference's Painter destructor does (stop flag,
+ * src/painter/painter.cpp:129-134), from any thread and without waiting: the
+ * pass in flight takes no more paths (its image stays incomplete), a worker
+ * started by nbpt_painter_start ends after it and reports "cancelled"
+ * through on_error, nbpt_painter_wait returns NBPT_ERROR, and the painter
+ * takes no more passes. */
+int nbpt_painter_cancel(nbpt_painter* painter);
 
 /* ---- job server: continuous batching of renders on one GPU ----
  *
@@ -264,6 +271,11 @@ typedef struct nbpt_job_info
         double submitted;     /* seconds since the server started */
         double started;       /* admitted; -1 while queued */
         double finished;      /* done or failed; -1 before */
+        /* device clock (CUDA events on the job's stream) of the start of its
+         * first pass and the end of its last, in seconds after the server's
+         * creation; -1 until the job is done */
+        double device_started;
+        double device_finished;
 } nbpt_job_info;
 
 /* max_jobs jobs run at once within memory_budget device bytes (0: 80 % of
@@ -290,6 +302,12 @@ int nbpt_server_job(nbpt_server* server, long long job, nbpt_job_info* info);
 int nbpt_server_wait(nbpt_server* server, long long job, nbpt_job_info* info);
 /* seconds since the server started, on the clock of nbpt_job_info */
 double nbpt_server_time(nbpt_server* server);
+/* nbpt_job_cancel: a queued job fails at once with the error "cancelled"; a
+ * running job's pass in flight takes no more paths (the reference's painter
+ * threads test their stop flag before each pixel,
+ * src/painter/painting/integrator_bpt.cpp:90-93), then the job fails the
+ * same way; a finished job is left as it is.  Returns without waiting. */
+int nbpt_server_cancel(nbpt_server* server, long long job);
 
 /* ---- verification entry points (same arithmetic as the render path) ---- */
 
@@ -333,6 +351,15 @@ int nbpt_scene_mesh_export(
         nbpt_scene* scene, int mesh, long long* counts, double* planes, double* node_lo, double* node_hi,
         unsigned* node_info, unsigned* indices, int* normal_info);
 
+/* the mesh `mesh` (order of creation among meshes) as ingested on the host,
+ * before or after nbpt_scene_finalize, no GPU needed: counts = (vertices,
+ * facets, normals); vertices and normals [V][N] transformed as the painter's
+ * mesh data (src/painter/shapes/mesh/data.cpp:88-111), the normals computed
+ * as src/model/mesh/normals.cpp does when a mesh object has none; facets
+ * [F][N].  Any output pointer may be NULL. */
+int nbpt_scene_ingested_mesh(nbpt_scene* scene, int mesh, long long* counts, double* vertices, double* normals,
+                             int* facets);
+
 /* GGX brdf f and pdf of material `material` (src/shading/ggx/brdf.h:146-194) */
 int nbpt_scene_brdf(
         nbpt_scene* scene, int material, const double* n, const double* v, const double* l, float* f, double* pdf);
@@ -347,6 +374,10 @@ int nbpt_scene_light_sample(
         nbpt_scene* scene, int light, int kind, const unsigned* seed, int seed_words, const double* point,
         double* out, float* radiance);
 
+/* test hook: the next `count` renders the server creates at admission fail as
+ * if cudaMalloc had run out of device memory (the server puts them back at the
+ * head of its queue in arrival order) */
+int nbpt_test_server_fail_allocations(nbpt_server* server, int count);
 /* raw PCG32 draws and uniform [0, 1) draws of a seed_seq stream, computed on the GPU */
 int nbpt_test_pcg(const unsigned* seed, int seed_words, int count, unsigned* out);
 int nbpt_test_canonical(const unsigned* seed, int seed_words, int count, int use_double, double* out);

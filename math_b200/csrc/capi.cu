@@ -1121,6 +1121,17 @@ int nbpt_scene_trace_noalloc(
                 });
 }
 
+int nbpt_scene_ingested_mesh(nbpt_scene* scene, const int mesh, long long* counts, double* vertices, double* normals,
+                             int* facets)
+{
+        return guarded(
+                [&]
+                {
+                        scene_of(scene).ingested_mesh(mesh, counts, vertices, normals, facets);
+                        return 0;
+                });
+}
+
 int nbpt_scene_mesh_export(
         nbpt_scene* scene,
         const int mesh,

@@ -117,6 +117,11 @@ public:
                                   double* point) const = 0;
         virtual void mesh_export(int mesh, long long* counts, double* planes, double* node_lo, double* node_hi,
                                  unsigned* node_info, unsigned* indices, int* normal_info) = 0;
+        // the ingested mesh `mesh` on the host (no GPU needed): counts =
+        // (vertices, facets, normals); vertices and normals [V][N] as the
+        // painter keeps them, facets [F][N]; any pointer may be NULL
+        virtual void ingested_mesh(int mesh, long long* counts, double* vertices, double* normals,
+                                   int* facets) const = 0;
         virtual void brdf(int material, const double* n, const double* v, const double* l, float* f,
                           double* pdf) = 0;
         virtual void brdf_sample(int material, const double* n, const double* v, const std::uint32_t* seed,

@@ -161,59 +161,119 @@ NBPT_HD Vec<N, T> to_vec(const double* p)
         return v;
 }
 
-// Gauss-Jordan inverse with partial pivoting of an M x M matrix in T.
+// Inverse of an M x M matrix (row major) in T as the reference computes it
+// (src/numerical/solve.h:159-172): for M <= 3 the adjugate over the
+// determinant (Leon, Linear Algebra with Applications, 2.3), for M >= 4
+// Gaussian elimination with partial pivoting on [A | I] and back substitution
+// (Karniadakis and Kirby, Parallel Scientific Computing in C++ and MPI;
+// src/numerical/gauss.h:142-280), with the same operation order.
 template <int M, typename T>
 std::array<T, M * M> inverse(std::array<T, M * M> a)
 {
+        const auto at = [&](const int r, const int c) -> T&
+        {
+                return a[r * M + c];
+        };
         std::array<T, M * M> b{};
-        for (int i = 0; i < M; ++i)
+        if constexpr (M == 1)
         {
-                b[i * M + i] = 1;
+                b[0] = T{1} / a[0];
         }
-        for (int c = 0; c < M; ++c)
+        else if constexpr (M == 2)
         {
-                int pivot = c;
-                for (int r = c + 1; r < M; ++r)
+                const T d = at(0, 0) * at(1, 1) - at(0, 1) * at(1, 0);
+                b[0] = at(1, 1) / d;
+                b[1] = -at(0, 1) / d;
+                b[2] = -at(1, 0) / d;
+                b[3] = at(0, 0) / d;
+        }
+        else if constexpr (M == 3)
+        {
+                const T c00 = at(1, 1) * at(2, 2) - at(1, 2) * at(2, 1);
+                const T c10 = at(0, 2) * at(2, 1) - at(0, 1) * at(2, 2);
+                const T c20 = at(0, 1) * at(1, 2) - at(0, 2) * at(1, 1);
+                const T d = at(0, 0) * c00 + at(1, 0) * c10 + at(2, 0) * c20;
+                b[0] = c00 / d;
+                b[1] = c10 / d;
+                b[2] = c20 / d;
+                b[3] = (at(1, 2) * at(2, 0) - at(1, 0) * at(2, 2)) / d;
+                b[4] = (at(0, 0) * at(2, 2) - at(0, 2) * at(2, 0)) / d;
+                b[5] = (at(0, 2) * at(1, 0) - at(0, 0) * at(1, 2)) / d;
+                b[6] = (at(1, 0) * at(2, 1) - at(1, 1) * at(2, 0)) / d;
+                b[7] = (at(0, 1) * at(2, 0) - at(0, 0) * at(2, 1)) / d;
+                b[8] = (at(0, 0) * at(1, 1) - at(0, 1) * at(1, 0)) / d;
+        }
+        else
+        {
+                for (int i = 0; i < M; ++i)
                 {
-                        if (abs_value(a[r * M + c]) > abs_value(a[pivot * M + c]))
+                        b[i * M + i] = 1;
+                }
+                // rows are exchanged whole, which is what exchanging the
+                // reference's row pointers does
+                const auto swap_rows = [](std::array<T, M * M>& m, const int r0, const int r1)
+                {
+                        for (int c = 0; c < M; ++c)
                         {
-                                pivot = r;
+                                std::swap(m[r0 * M + c], m[r1 * M + c]);
+                        }
+                };
+                for (int k = 0; k < M - 1; ++k)
+                {
+                        T largest = abs_value(at(k, k));
+                        int pivot = k;
+                        for (int r = k + 1; r < M; ++r)
+                        {
+                                const T v = abs_value(at(r, k));
+                                if (v > largest)
+                                {
+                                        largest = v;
+                                        pivot = r;
+                                }
+                        }
+                        if (pivot != k)
+                        {
+                                swap_rows(a, pivot, k);
+                                swap_rows(b, pivot, k);
+                        }
+                        for (int i = k + 1; i < M; ++i)
+                        {
+                                const T l_ik = at(i, k) / at(k, k);
+                                for (int j = k; j < M; ++j)
+                                {
+                                        at(i, j) -= l_ik * at(k, j);
+                                }
+                                for (int m = 0; m < M; ++m)
+                                {
+                                        b[i * M + m] -= l_ik * b[k * M + m];
+                                }
                         }
                 }
-                if (a[pivot * M + c] == 0)
+                for (int m = 0; m < M; ++m)
+                {
+                        b[(M - 1) * M + m] /= at(M - 1, M - 1);
+                }
+                for (int k = M - 2; k >= 0; --k)
+                {
+                        for (int j = k + 1; j < M; ++j)
+                        {
+                                const T u = -at(k, j);
+                                for (int m = 0; m < M; ++m)
+                                {
+                                        b[k * M + m] += b[j * M + m] * u;
+                                }
+                        }
+                        for (int m = 0; m < M; ++m)
+                        {
+                                b[k * M + m] /= at(k, k);
+                        }
+                }
+        }
+        for (const T x : b)
+        {
+                if (!std::isfinite(x))
                 {
                         throw std::runtime_error("mesh matrix is singular");
-                }
-                if (pivot != c)
-                {
-                        for (int k = 0; k < M; ++k)
-                        {
-                                std::swap(a[c * M + k], a[pivot * M + k]);
-                                std::swap(b[c * M + k], b[pivot * M + k]);
-                        }
-                }
-                const T d = a[c * M + c];
-                for (int k = 0; k < M; ++k)
-                {
-                        a[c * M + k] /= d;
-                        b[c * M + k] /= d;
-                }
-                for (int r = 0; r < M; ++r)
-                {
-                        if (r == c)
-                        {
-                                continue;
-                        }
-                        const T f = a[r * M + c];
-                        if (f == 0)
-                        {
-                                continue;
-                        }
-                        for (int k = 0; k < M; ++k)
-                        {
-                                a[r * M + k] -= f * a[c * M + k];
-                                b[r * M + k] -= f * b[c * M + k];
-                        }
                 }
         }
         return b;
@@ -233,20 +293,38 @@ void parallel_ranges(const std::size_t count, const F& f, const std::size_t grai
         std::vector<std::thread> threads;
         threads.reserve(parts - 1);
         const std::size_t step = (count + parts - 1) / parts;
+        std::exception_ptr error;
+        std::mutex error_mutex;
+        const auto run = [&](const std::size_t b, const std::size_t e)
+        {
+                try
+                {
+                        f(b, e);
+                }
+                catch (...)
+                {
+                        const std::lock_guard lock(error_mutex);
+                        error = std::current_exception();
+                }
+        };
         for (std::size_t p = 1; p < parts; ++p)
         {
                 const std::size_t b = std::min(count, p * step);
                 const std::size_t e = std::min(count, b + step);
                 threads.emplace_back(
-                        [&f, b, e]
+                        [&run, b, e]
                         {
-                                f(b, e);
+                                run(b, e);
                         });
         }
-        f(std::size_t{0}, std::min(count, step));
+        run(std::size_t{0}, std::min(count, step));
         for (std::thread& t : threads)
         {
                 t.join();
+        }
+        if (error)
+        {
+                std::rethrow_exception(error);
         }
 }
 
@@ -325,11 +403,205 @@ public:
         Stopwatch& operator=(const Stopwatch&) = delete;
 };
 
-// Vertex normals of a simplex mesh: per vertex, the facet normals around it
-// weighted by the facet's solid angle at the vertex (n = 3, 4) or 1
-// (n >= 5), oriented consistently and averaged
-// (after src/model/mesh/normals.cpp:46-195).  Facet normals and angles are
-// computed in parallel; the sums run over the facets in order.
+// The normal of a point set as the reference computes it for a vertex's
+// vicinity (src/numerical/normal.h:46-103): the eigenvector of the smallest
+// eigenvalue of the point set's covariance, found as the orthogonal
+// complement of the other N - 1 eigenvectors.  The eigenvectors come from
+// the cyclic Jacobi method with a threshold (Kiusalaas, Numerical Methods in
+// Engineering with Python 3, section 9.2; src/numerical/eigen.h), on the
+// upper triangle, with the reference's tolerance and at most 20 sweeps.
+// Only the sign of this normal reaches the mesh (the vertex normal is the
+// sum of its facets' normals, each turned towards it), but that sign decides
+// which way a facet's geometric normal faces (facet.cpp:104-117), so the
+// steps follow the reference's for the same eigenvector signs.
+template <int N>
+Vec<N, double> point_normal(const std::vector<Vec<N, double>>& points)
+{
+        if (points.size() < static_cast<std::size_t>(N))
+        {
+                throw std::runtime_error("At least " + std::to_string(N) + " points are required for point normal");
+        }
+        // covariance (numerical/covariance.h:38-66), upper triangle
+        Vec<N, double> average = Vec<N, double>::filled(0);
+        for (const Vec<N, double>& p : points)
+        {
+                average = average + p;
+        }
+        average = average / static_cast<double>(points.size());
+        double a[N][N] = {};
+        for (const Vec<N, double>& p : points)
+        {
+                const Vec<N, double> v = p - average;
+                for (int i = 0; i < N; ++i)
+                {
+                        for (int j = i; j < N; ++j)
+                        {
+                                a[i][j] += v[i] * v[j];
+                        }
+                }
+        }
+        double largest = std::numeric_limits<double>::lowest();
+        for (int i = 0; i < N - 1; ++i)
+        {
+                for (int j = i + 1; j < N; ++j)
+                {
+                        largest = std::max(largest, std::abs(a[i][j]));
+                }
+        }
+        const double tolerance = largest * (100 * std::numeric_limits<double>::epsilon());
+        // eigenvectors as rows, from the identity
+        Vec<N, double> vectors[N];
+        for (int i = 0; i < N; ++i)
+        {
+                vectors[i] = Vec<N, double>::filled(0);
+                vectors[i][i] = 1;
+        }
+        const auto rotate = [&](const int k, const int l)
+        {
+                const double diff = a[l][l] - a[k][k];
+                const double phi = diff / (2 * a[k][l]);
+                const double phi_s = phi * phi + 1;
+                double t;
+                if (phi_s <= std::numeric_limits<double>::max())
+                {
+                        t = std::copysign(1 / (std::abs(phi) + std::sqrt(phi_s)), phi);
+                }
+                else
+                {
+                        t = 1 / (2 * phi);
+                }
+                const double c = 1 / std::sqrt(t * t + 1);
+                const double s = t * c;
+                const double tau = s / (1 + c);
+                const double a_kl = a[k][l];
+                a[k][l] = 0;
+                a[k][k] = a[k][k] - t * a_kl;
+                a[l][l] = a[l][l] + t * a_kl;
+                for (int i = 0; i < k; ++i)
+                {
+                        const double a_ik = a[i][k];
+                        const double a_il = a[i][l];
+                        a[i][k] = a_ik - s * (a_il + tau * a_ik);
+                        a[i][l] = a_il + s * (a_ik - tau * a_il);
+                }
+                for (int i = k + 1; i < l; ++i)
+                {
+                        const double a_ki = a[k][i];
+                        const double a_il = a[i][l];
+                        a[k][i] = a_ki - s * (a_il + tau * a_ki);
+                        a[i][l] = a_il + s * (a_ki - tau * a_il);
+                }
+                for (int i = l + 1; i < N; ++i)
+                {
+                        const double a_ki = a[k][i];
+                        const double a_li = a[l][i];
+                        a[k][i] = a_ki - s * (a_li + tau * a_ki);
+                        a[l][i] = a_li + s * (a_ki - tau * a_li);
+                }
+                for (int i = 0; i < N; ++i)
+                {
+                        const double p_ik = vectors[k][i];
+                        const double p_il = vectors[l][i];
+                        vectors[k][i] = p_ik - s * (p_il + tau * p_ik);
+                        vectors[l][i] = p_il + s * (p_ik - tau * p_il);
+                }
+        };
+        bool converged = false;
+        for (int sweep = 0; sweep < 20 && !converged; ++sweep)
+        {
+                double sum = 0;
+                for (int i = 0; i < N - 1; ++i)
+                {
+                        for (int j = i + 1; j < N; ++j)
+                        {
+                                sum += std::abs(a[i][j]);
+                        }
+                }
+                const double mu = 0.5 * sum / (N * (N - 1));
+                for (int k = 0; k < N - 1; ++k)
+                {
+                        for (int l = k + 1; l < N; ++l)
+                        {
+                                if (std::abs(a[k][l]) >= mu)
+                                {
+                                        rotate(k, l);
+                                }
+                        }
+                }
+                converged = mu <= tolerance;
+        }
+        if (!converged)
+        {
+                throw std::runtime_error("Jacobi method did not converge");
+        }
+        int smallest = 0;
+        for (int i = 1; i < N; ++i)
+        {
+                if (a[i][i] < a[smallest][smallest])
+                {
+                        smallest = i;
+                }
+        }
+        Vec<N, double> others[N - 1];
+        for (int i = 0, k = 0; i < N; ++i)
+        {
+                if (i != smallest)
+                {
+                        others[k++] = vectors[i];
+                }
+        }
+        return orthogonal_complement(others).normalized();
+}
+
+// Solid angle at a facet's corner for the corner's weight (3-space: the
+// angle; 4-space: the spherical triangle's excess, src/geometry/shapes/
+// sphere_simplex.h:88-156), 0 for a degenerate corner.
+template <int N>
+double corner_weight(Vec<N, double> (&e)[N - 1])
+{
+        double norm[N - 1];
+        for (int j = 0; j < N - 1; ++j)
+        {
+                norm[j] = e[j].norm();
+                if (norm[j] == 0)
+                {
+                        return 0;
+                }
+        }
+        if constexpr (N == 3)
+        {
+                const double cosine = dot(e[0] / norm[0], e[1] / norm[1]);
+                return std::acos(std::clamp(cosine, -1.0, 1.0));
+        }
+        else
+        {
+                static_assert(N == 4);
+                const Vec<N, double> a = e[0] / norm[0];
+                const Vec<N, double> b = e[1] / norm[1];
+                const Vec<N, double> c = e[2] / norm[2];
+                const double cos_a = dot(b, c);
+                const double cos_b = dot(a, c);
+                const double cos_c = dot(a, b);
+                const double sin_a_2 = 1 - cos_a * cos_a;
+                const double sin_b_2 = 1 - cos_b * cos_b;
+                const double sin_c_2 = 1 - cos_c * cos_c;
+                const double dihedral_cosine_a = (cos_a - cos_b * cos_c) / std::sqrt(sin_b_2 * sin_c_2);
+                const double dihedral_cosine_b = (cos_b - cos_a * cos_c) / std::sqrt(sin_a_2 * sin_c_2);
+                const double dihedral_cosine_c = (cos_c - cos_a * cos_b) / std::sqrt(sin_a_2 * sin_b_2);
+                const double dihedral_a = std::acos(std::clamp(dihedral_cosine_a, -1.0, 1.0));
+                const double dihedral_b = std::acos(std::clamp(dihedral_cosine_b, -1.0, 1.0));
+                const double dihedral_c = std::acos(std::clamp(dihedral_cosine_c, -1.0, 1.0));
+                const double area = dihedral_a + dihedral_b + dihedral_c - 3.141592653589793238462643383279502884;
+                return std::max(0.0, area);
+        }
+}
+
+// Vertex normals of a simplex mesh as src/model/mesh/normals.cpp:46-195
+// computes them: per vertex, the facet normals around it weighted by the
+// facet's solid angle at the vertex (n = 3, 4) or 1 (n >= 5), each turned
+// towards the normal of the vertex's vicinity (point_normal), summed in facet
+// order and normalised, then rounded to float.  Facet normals and angles are
+// computed in parallel, and so are the vertices.
 template <int N>
 std::vector<float> vertex_normals(const std::vector<float>& points, const std::vector<int>& facets,
                                   const bool parallel = true)
@@ -358,6 +630,8 @@ std::vector<float> vertex_normals(const std::vector<float>& points, const std::v
                                 fn[f] = orthogonal_complement(e).normalized();
                                 if constexpr (N == 3 || N == 4)
                                 {
+                                        // normals.cpp:46-72: the corner's edges in the facet's
+                                        // cyclic order from the corner
                                         for (int k = 0; k < N; ++k)
                                         {
                                                 const int v = facets[f * N + k];
@@ -370,25 +644,8 @@ std::vector<float> vertex_normals(const std::vector<float>& points, const std::v
                                                                 a[j][d] = static_cast<double>(points[o * static_cast<std::size_t>(N) + d]) -
                                                                           static_cast<double>(points[v * static_cast<std::size_t>(N) + d]);
                                                         }
-                                                        a[j] = a[j].normalized();
                                                 }
-                                                if constexpr (N == 3)
-                                                {
-                                                        weight[f * N + k] = std::acos(std::fmax(-1.0, std::fmin(1.0, dot(a[0], a[1]))));
-                                                }
-                                                else
-                                                {
-                                                        // solid angle of the spherical triangle
-                                                        // (Van Oosterom-Strackee); |det| of the three unit
-                                                        // vectors within their 3-space is the norm of their
-                                                        // orthogonal complement
-                                                        Vec<N, double> c3[N - 1] = {a[0], a[1], a[2]};
-                                                        const double det = orthogonal_complement(c3).norm();
-                                                        const double d01 = dot(a[0], a[1]);
-                                                        const double d02 = dot(a[0], a[2]);
-                                                        const double d12 = dot(a[1], a[2]);
-                                                        weight[f * N + k] = 2 * std::atan2(det, 1 + d01 + d02 + d12);
-                                                }
+                                                weight[f * N + k] = corner_weight<N>(a);
                                         }
                                 }
                         }
@@ -459,13 +716,44 @@ std::vector<float> vertex_normals(const std::vector<float>& points, const std::v
                 parallel, vcount,
                 [&](const std::size_t begin, const std::size_t end)
                 {
+                        std::vector<int> vicinity_ids;
+                        std::vector<Vec<N, double>> vicinity;
                         for (std::size_t v = begin; v < end; ++v)
                         {
                                 if (first[v] == first[v + 1])
                                 {
                                         continue;
                                 }
-                                const Vec<N, double> reference = fn[corners[first[v]] / N];
+                                // the vicinity: every vertex of the vertex's facets, in
+                                // increasing index (normals.cpp:98-135)
+                                vicinity_ids.clear();
+                                for (int i = first[v]; i < first[v + 1]; ++i)
+                                {
+                                        const std::size_t f = static_cast<std::size_t>(corners[i]) / N;
+                                        for (int k = 0; k < N; ++k)
+                                        {
+                                                vicinity_ids.push_back(facets[f * N + k]);
+                                        }
+                                }
+                                std::sort(vicinity_ids.begin(), vicinity_ids.end());
+                                vicinity_ids.erase(std::unique(vicinity_ids.begin(), vicinity_ids.end()),
+                                                   vicinity_ids.end());
+                                if (vicinity_ids.size() < static_cast<std::size_t>(N))
+                                {
+                                        throw std::runtime_error("Vertex has " + std::to_string(vicinity_ids.size()) +
+                                                                 " vertices in its vicinity, required minimum is " +
+                                                                 std::to_string(N) + " vertices");
+                                }
+                                vicinity.resize(vicinity_ids.size());
+                                for (std::size_t i = 0; i < vicinity_ids.size(); ++i)
+                                {
+                                        for (int d = 0; d < N; ++d)
+                                        {
+                                                vicinity[i][d] = static_cast<double>(
+                                                        points[static_cast<std::size_t>(vicinity_ids[i]) * N + d]);
+                                        }
+                                }
+                                const Vec<N, double> reference = point_normal<N>(vicinity);
                                 Vec<N, double> sum = Vec<N, double>::filled(0);
                                 for (int i = first[v]; i < first[v + 1]; ++i)
                                 {
@@ -1936,6 +2224,34 @@ public:
                           double* point) const override;
         void mesh_export(int mesh, long long* counts, double* planes, double* node_lo, double* node_hi,
                          unsigned* node_info, unsigned* indices, int* normal_info) override;
+
+        void ingested_mesh(const int mesh, long long* counts, double* vertices, double* normals,
+                           int* facets) const override
+        {
+                if (mesh < 0 || mesh >= static_cast<int>(meshes_.size()))
+                {
+                        throw std::runtime_error("no mesh " + std::to_string(mesh));
+                }
+                const MeshHost& m = meshes_[mesh];
+                if (counts)
+                {
+                        counts[0] = static_cast<long long>(m.vertices.size() / N);
+                        counts[1] = static_cast<long long>(m.facets.size() / N);
+                        counts[2] = static_cast<long long>(m.normals.size() / N);
+                }
+                if (vertices)
+                {
+                        std::copy(m.vertices.begin(), m.vertices.end(), vertices);
+                }
+                if (normals)
+                {
+                        std::copy(m.normals.begin(), m.normals.end(), normals);
+                }
+                if (facets)
+                {
+                        std::copy(m.facets.begin(), m.facets.end(), facets);
+                }
+        }
         void brdf(int material, const double* n, const double* v, const double* l, float* f, double* pdf) override;
         void brdf_sample(int material, const double* n, const double* v, const std::uint32_t* seed, int seed_words,
                          double* l, double* pdf, float* f) override;

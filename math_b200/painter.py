@@ -123,6 +123,7 @@ SIGNATURES = [
     ("nbpt_scene_trace", ctypes.c_int, [_P, _D, ctypes.c_longlong, ctypes.c_int, _I, _I, _D, _D]),
     ("nbpt_scene_trace_noalloc", ctypes.c_int, [_P, _D, ctypes.c_longlong, ctypes.c_int, _I, _I, _D, _D]),
     ("nbpt_scene_mesh_export", ctypes.c_int, [_P, ctypes.c_int, _L, _D, _D, _D, _U, _U, _I]),
+    ("nbpt_scene_ingested_mesh", ctypes.c_int, [_P, ctypes.c_int, _L, _D, _D, _I]),
     ("nbpt_scene_brdf", ctypes.c_int, [_P, ctypes.c_int, _D, _D, _D, _F, _D]),
     ("nbpt_scene_brdf_sample", ctypes.c_int, [_P, ctypes.c_int, _D, _D, _U, ctypes.c_int, _D, _D, _F]),
     ("nbpt_scene_light_sample", ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, _U, ctypes.c_int, _D, _D, _F]),
