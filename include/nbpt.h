@@ -198,6 +198,20 @@ nbpt_painter* nbpt_painter_create(nbpt_scene* scene, int samples_per_pixel, int 
 #define NBPT_INTEGRATOR_PT 1
 nbpt_painter* nbpt_painter_create_integrator(
         nbpt_scene* scene, int integrator, int samples_per_pixel, int max_depth, unsigned seed);
+/* A painter of one slab of the screen, for renders split across GPUs: the
+ * rows [slab_begin, slab_end) of the last screen axis.  No reference function
+ * (the reference's painter threads share one screen; its pixel order is
+ * src/painter/painting/paintbrush.h:162-205).  A pass renders the paths of
+ * the slab and of the row on either side (the pixel filter reaches one
+ * pixel) and accumulates the slab's own pixels; every path's stream is fixed
+ * by (seed, pass, pixel, sample), so the slab's pixels are bit for bit those
+ * of the whole-screen painter, and the slabs of a split put together are its
+ * image.  Images and samples cover the slab (samples: the slab with its
+ * halo rows); sample_count counts every path rendered.  slab_end < 0: the
+ * whole screen. */
+nbpt_painter* nbpt_painter_create_slab(
+        nbpt_scene* scene, int integrator, int samples_per_pixel, int max_depth, unsigned seed, int slab_begin,
+        int slab_end);
 void nbpt_painter_destroy(nbpt_painter* painter);
 
 /* ---- passes on a worker thread (the reference painter's thread and its

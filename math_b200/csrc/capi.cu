@@ -642,6 +642,18 @@ nbpt_painter* nbpt_painter_create_integrator(
         const int max_depth,
         const unsigned seed)
 {
+        return nbpt_painter_create_slab(scene, integrator, samples_per_pixel, max_depth, seed, 0, -1);
+}
+
+nbpt_painter* nbpt_painter_create_slab(
+        nbpt_scene* scene,
+        const int integrator,
+        const int samples_per_pixel,
+        const int max_depth,
+        const unsigned seed,
+        const int slab_begin,
+        const int slab_end)
+{
         nbpt_painter* out = nullptr;
         guarded(
                 [&]
@@ -652,7 +664,8 @@ nbpt_painter* nbpt_painter_create_integrator(
                         }
                         auto p = std::make_unique<nbpt_painter>();
                         p->impl = scene_of(scene).create_painter(samples_per_pixel, max_depth, seed,
-                                                                 static_cast<nbpt::Integrator>(integrator));
+                                                                 static_cast<nbpt::Integrator>(integrator), slab_begin,
+                                                                 slab_end);
                         out = p.release();
                         return 0;
                 });

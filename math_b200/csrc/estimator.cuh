@@ -576,9 +576,15 @@ template <int N>
 struct Screen final
 {
         int size[N - 1];
+        // a slab of the screen: the receiving pixels are [first, first +
+        // pixel_count) in global index, and the sample arrays hold the pixels
+        // from source_first on (0 and 0 for the whole screen)
+        long long first = 0;
+        long long source_first = 0;
 };
 
-// Merge one pass's samples of the 3^(n-1) neighbours into receiving pixel t.
+// Merge one pass's samples of the 3^(n-1) neighbours into receiving pixel t
+// (global index).
 template <int N, typename T, int C>
 NBPT_HD void accumulate_pixel(
         const Screen<N>& screen,
@@ -646,7 +652,7 @@ NBPT_HD void accumulate_pixel(
                 int nbg = 0;
                 for (int j = 0; j < spp; ++j)
                 {
-                        const long long sidx = p * spp + j;
+                        const long long sidx = (p - screen.source_first) * spp + j;
                         const T x0 = (static_cast<T>(tc[0] - pc[0]) + T(0.5)) - points[sidx * (N - 1)];
                         T weight = max_value(T(0), exp(alpha * x0 * x0) - exp_radius);
 #pragma unroll
@@ -675,7 +681,7 @@ NBPT_HD void accumulate_pixel(
                 if (nc > 0)
                 {
                         order_group(color_order, nc, [&](const int i) { return contribution[i]; });
-                        const ColorGroup<C> g{colors + p * spp * C, w, contribution, color_order, nc, C, 1, 0};
+                        const ColorGroup<C> g{colors + (p - screen.source_first) * spp * C, w, contribution, color_order, nc, C, 1, 0};
                         float g_sum[C];
                         float g_wsum = 0;
 #pragma unroll 8
@@ -738,7 +744,7 @@ __global__ void __launch_bounds__(128) accumulate_kernel(
                 return;
         }
         PixelState<C> st = state[t];
-        accumulate_pixel<N, T, C>(screen, t, spp, points, colors, lum, valid, alpha, exp_radius, st);
+        accumulate_pixel<N, T, C>(screen, screen.first + t, spp, points, colors, lum, valid, alpha, exp_radius, st);
         state[t] = st;
 }
 
@@ -812,7 +818,7 @@ __global__ void __launch_bounds__(128) accumulate_warp_kernel(
 
         int tc[N - 1];
         {
-                long long rest = t;
+                long long rest = screen.first + t;
 #pragma unroll
                 for (int d = 0; d < N - 1; ++d)
                 {
@@ -853,7 +859,7 @@ __global__ void __launch_bounds__(128) accumulate_warp_kernel(
                 // weights and selection (pixel_filter.h:57-69, com/select.h:28-47)
                 for (int j = lane; j < spp; j += 32)
                 {
-                        const long long sidx = p * spp + j;
+                        const long long sidx = (p - screen.source_first) * spp + j;
                         const T x0 = (static_cast<T>(tc[0] - pc[0]) + T(0.5)) - points[sidx * (N - 1)];
                         T weight = max_value(T(0), exp(alpha * x0 * x0) - exp_radius);
 #pragma unroll
@@ -923,7 +929,7 @@ __global__ void __launch_bounds__(128) accumulate_warp_kernel(
                 const int nbg = s_counts[warp][1];
                 if (nc > 0)
                 {
-                        const ColorGroup<K> g{colors + p * spp * C, w, contribution, order, nc, C, 32, lane};
+                        const ColorGroup<K> g{colors + (p - screen.source_first) * spp * C, w, contribution, order, nc, C, 32, lane};
                         float g_sum[K];
                         float g_wsum = 0;
 #pragma unroll
@@ -1022,7 +1028,7 @@ __global__ void __launch_bounds__(128) accumulate_warp_small_kernel(
 
         int tc[N - 1];
         {
-                long long rest = t;
+                long long rest = screen.first + t;
 #pragma unroll
                 for (int d = 0; d < N - 1; ++d)
                 {
@@ -1065,7 +1071,7 @@ __global__ void __launch_bounds__(128) accumulate_warp_small_kernel(
                         continue;
                 }
                 const int j = lane;
-                const long long sidx = p * spp + j;
+                const long long sidx = (p - screen.source_first) * spp + j;
                 const T x0 = (static_cast<T>(tc[0] - pc[0]) + T(0.5)) - points[sidx * (N - 1)];
                 T weight = max_value(T(0), exp(alpha * x0 * x0) - exp_radius);
 #pragma unroll
@@ -1184,7 +1190,7 @@ __global__ void __launch_bounds__(128) accumulate_warp_small_kernel(
                 __syncwarp();
                 if (nc > 0)
                 {
-                        const ColorGroup<K> g{colors + p * spp * C, w, s_contribution[warp][nb], order, nc, C, 32, lane};
+                        const ColorGroup<K> g{colors + (p - screen.source_first) * spp * C, w, s_contribution[warp][nb], order, nc, C, 32, lane};
                         float g_sum[K];
                         float g_wsum = 0;
 #pragma unroll

@@ -101,8 +101,12 @@ public:
 
         // max_depth bounds the BPT subpaths; the PT integrator ends its paths
         // by Russian roulette and ignores it
+        // slab_end >= 0: a painter of the rows [slab_begin, slab_end) of the
+        // last screen axis only (its paths, those of the rows either side,
+        // and the estimator of its own pixels); its images are the slab's
         virtual std::unique_ptr<Painter> create_painter(int samples_per_pixel, int max_depth, std::uint32_t seed,
-                                                        Integrator integrator = Integrator::BPT) = 0;
+                                                        Integrator integrator = Integrator::BPT, int slab_begin = 0,
+                                                        int slab_end = -1) = 0;
         // device bytes create_painter would allocate
         virtual long long painter_bytes(int samples_per_pixel, int max_depth,
                                         Integrator integrator = Integrator::BPT) const = 0;

@@ -2216,7 +2216,7 @@ public:
         }
 
         std::unique_ptr<Painter> create_painter(int spp, int max_depth, std::uint32_t seed,
-                                                Integrator integrator) override;
+                                                Integrator integrator, int slab_begin, int slab_end) override;
         long long painter_bytes(int spp, int max_depth, Integrator integrator) const override;
 
         void trace(const double* rays, long long count, int any, int* kind, int* index, double* t, double* point) override;
@@ -2415,7 +2415,10 @@ class PainterT final : public Painter
         std::uint32_t seed_;
         Integrator integrator_;
         int device_ = 0;
-        long long pixels_;
+        long long pixels_;      // receiving pixels: the screen, or a slab of it
+        long long first_ = 0;   // global index of the first receiving pixel
+        long long sources_ = 0; // pixels whose paths a pass renders: the slab and its one-row halo
+        long long source_first_ = 0;
         long long pass_ = 0;
         long long passes_done_ = 0;
         cudaStream_t stream_ = nullptr;
@@ -2497,8 +2500,12 @@ public:
                        chunk;
         }
 
+        // slab_end < 0: the whole screen; else the rows [slab_begin, slab_end)
+        // of the last screen axis, with their paths, the paths of the rows
+        // either side (the filter reaches one pixel) and the estimator of the
+        // slab's own pixels
         PainterT(const SceneT<N, T, C>* scene, const int spp, const int max_depth, const std::uint32_t seed,
-                 const Integrator integrator)
+                 const Integrator integrator, const int slab_begin = 0, const int slab_end = -1)
                 : scene_(scene),
                   spp_request_(spp),
                   max_depth_(max_depth),
@@ -2527,6 +2534,24 @@ public:
                                 + std::to_string(MAX_GROUP) + " of one pass");
                 }
                 pixels_ = scene_->pixel_count();
+                sources_ = pixels_;
+                if (slab_end >= 0)
+                {
+                        const int rows = scene_->device().projector.size[N - 2];
+                        if (slab_begin < 0 || slab_begin >= slab_end || slab_end > rows)
+                        {
+                                throw std::runtime_error("slab rows [" + std::to_string(slab_begin) + ", " +
+                                                         std::to_string(slab_end) + ") outside the screen's " +
+                                                         std::to_string(rows) + " rows");
+                        }
+                        const long long row = pixels_ / rows;
+                        const int source_begin = std::max(0, slab_begin - 1);
+                        const int source_end = std::min(rows, slab_end + 1);
+                        first_ = slab_begin * row;
+                        pixels_ = (slab_end - slab_begin) * row;
+                        source_first_ = source_begin * row;
+                        sources_ = (source_end - source_begin) * row;
+                }
 
                 NBPT_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
 
@@ -2541,7 +2566,7 @@ public:
                 offsets[strata_] = 1;
                 offsets_.upload_on(offsets, stream_);
 
-                const long long samples = pixels_ * spp_;
+                const long long samples = sources_ * spp_;
                 points_.allocate(samples * (N - 1));
                 colors_.allocate(samples * C);
                 lum_.allocate(samples);
@@ -2558,7 +2583,7 @@ public:
                 NBPT_CUDA(cudaGetDevice(&device));
                 device_ = device;
                 NBPT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-                chunk_pixels_ = chunk_pixels(pixels_, spp_, max_depth_, integrator_);
+                chunk_pixels_ = chunk_pixels(sources_, spp_, max_depth_, integrator_);
                 if (integrator_ == Integrator::PT)
                 {
                         next_path_.allocate(1);
@@ -2660,25 +2685,27 @@ public:
                         // painter's life
                         NBPT_CUDA(cudaMemsetAsync(stats_.get(), 0, offsetof(PathStats, overflows), stream_));
                         NBPT_CUDA(cudaEventRecord(ev_start_, stream_));
-                        sj_points_kernel<N - 1, T><<<blocks_for(pixels_, 128), 128, 0, stream_>>>(
-                                0, pixels_, seed_, pass, strata_, offsets_.get(), points_.get());
+                        sj_points_kernel<N - 1, T><<<blocks_for(sources_, 128), 128, 0, stream_>>>(
+                                source_first_, source_first_ + sources_, seed_, pass, strata_, offsets_.get(),
+                                points_.get());
                         NBPT_CUDA(cudaGetLastError());
                         NBPT_CUDA(cudaEventRecord(ev_paths_, stream_));
                         long long launches = 2;
                         if (integrator_ == Integrator::PT)
                         {
                                 // one launch per chunk: whole paths (pt.cuh)
-                                for (long long b = 0; b < pixels_; b += chunk_pixels_)
+                                for (long long b = source_first_; b < source_first_ + sources_; b += chunk_pixels_)
                                 {
-                                        const long long e = std::min(pixels_, b + chunk_pixels_);
+                                        const long long e = std::min(source_first_ + sources_, b + chunk_pixels_);
+                                        const long long o = b - source_first_; // the chunk in the sample arrays
                                         const long long n = (e - b) * spp_;
                                         NBPT_CUDA(cudaMemsetAsync(next_path_.get(), 0, sizeof(unsigned), stream_));
                                         pt_paths_kernel<N, T, C>
                                                 <<<std::min<long long>(connect_blocks_, blocks_for(n, 128)), 128, 0, stream_>>>(
                                                         scene_->device_channel_0(), scene_->device_materials(),
                                                         scene_->device_lights(), b, e, spp_, seed_, pass,
-                                                        points_.get() + b * spp_ * (N - 1), colors_.get() + b * spp_ * C,
-                                                        lum_.get() + b * spp_, valid_.get() + b * spp_,
+                                                        points_.get() + o * spp_ * (N - 1), colors_.get() + o * spp_ * C,
+                                                        lum_.get() + o * spp_, valid_.get() + o * spp_,
                                                         pt_estimates_.get(), next_path_.get(), stats_.get(),
                                                         scene_->cie() + 64, cancel_.get());
                                         NBPT_CUDA(cudaGetLastError());
@@ -2690,9 +2717,10 @@ public:
                                 // per chunk of pixels: subpaths, strategies, the s = 1
                                 // strategies, then the colours (kernels.cuh)
                                 const DeviceScene<N, T, 1>& scene_1 = scene_->device_channel_0();
-                                for (long long b = 0; b < pixels_; b += chunk_pixels_)
+                                for (long long b = source_first_; b < source_first_ + sources_; b += chunk_pixels_)
                                 {
-                                        const long long e = std::min(pixels_, b + chunk_pixels_);
+                                        const long long e = std::min(source_first_ + sources_, b + chunk_pixels_);
+                                        const long long o = b - source_first_; // the chunk in the sample arrays
                                         const long long n = (e - b) * spp_;
                                         NBPT_CUDA(cudaMemsetAsync(task_count_.get(), 0, 3 * sizeof(unsigned), stream_));
                                         // queue regions: s >= 2, then s = 1 and s = 0 (at most
@@ -2707,8 +2735,8 @@ public:
                                         NBPT_CUDA(cudaMemsetAsync(next_path_.get(), 0, sizeof(unsigned), stream_));
                                         paths_walk_kernel<N, T><<<std::min<long long>(connect_blocks_, blocks_for(n, 128)), 128, 0,
                                                                   stream_>>>(
-                                                scene_1, b, e, spp_, max_depth_, seed_, pass, points_.get() + b * spp_ * (N - 1),
-                                                vertices_.get(), rng_.get(), tape_.get(), tape_words_, valid_.get() + b * spp_,
+                                                scene_1, b, e, spp_, max_depth_, seed_, pass, points_.get() + o * spp_ * (N - 1),
+                                                vertices_.get(), rng_.get(), tape_.get(), tape_words_, valid_.get() + o * spp_,
                                                 queues, next_path_.get(), stats_.get(), cancel_.get());
                                         NBPT_CUDA(cudaGetLastError());
                                         paths_light_kernel<N, T><<<blocks_for(n, 128), 128, 0, stream_>>>(
@@ -2723,7 +2751,7 @@ public:
                                         paths_replay_kernel<N, T, C, LANES><<<blocks_for(n * LANES, 128), 128, 0, stream_>>>(
                                                 scene_->device_materials(), scene_->device_lights(),
                                                 scene.shading.fresnel_a, scene.shading.fresnel_b, max_depth_, n, tape_.get(),
-                                                tape_words_, colors_.get() + b * spp_ * C, lum_.get() + b * spp_,
+                                                tape_words_, colors_.get() + o * spp_ * C, lum_.get() + o * spp_,
                                                 scene_->cie() + 64, stats_.get(), cancel_.get());
                                         NBPT_CUDA(cudaGetLastError());
                                         launches += 4;
@@ -2735,6 +2763,8 @@ public:
                         {
                                 screen.size[i] = scene.projector.size[i];
                         }
+                        screen.first = first_;
+                        screen.source_first = source_first_;
                         const T radius = T(1.5);
                         const T width = radius / T(2.5);
                         const T alpha = -1 / (2 * width * width);
@@ -2789,7 +2819,7 @@ public:
                 NBPT_CUDA(cudaEventElapsedTime(&paths_ms, ev_paths_, ev_paths_end_));
                 statistics_.pass_number = passes_done_;
                 statistics_.ray_count = static_cast<long long>(s.queries);
-                statistics_.sample_count = pixels_ * spp_;
+                statistics_.sample_count = sources_ * spp_;
                 statistics_.previous_pass_duration = ms * 1e-3;
                 statistics_.paths_seconds = paths_ms * 1e-3;
                 statistics_.nodes = s.nodes;
@@ -2847,7 +2877,7 @@ public:
         void samples(double* points, float* colors, unsigned char* valid) override
         {
                 NBPT_CUDA(cudaStreamSynchronize(stream_));
-                const long long samples = pixels_ * spp_;
+                const long long samples = sources_ * spp_;
                 if (points)
                 {
                         std::vector<T> p(samples * (N - 1));
@@ -2878,9 +2908,11 @@ std::unique_ptr<Painter> SceneT<N, T, C>::create_painter(
         const int spp,
         const int max_depth,
         const std::uint32_t seed,
-        const Integrator integrator)
+        const Integrator integrator,
+        const int slab_begin,
+        const int slab_end)
 {
-        return std::make_unique<PainterT<N, T, C>>(this, spp, max_depth, seed, integrator);
+        return std::make_unique<PainterT<N, T, C>>(this, spp, max_depth, seed, integrator, slab_begin, slab_end);
 }
 
 template <int N, typename T, int C>

@@ -97,6 +97,7 @@ SIGNATURES = [
     ("nbpt_scene_set_bvh_builder", ctypes.c_int, [_P, ctypes.c_int]),
     ("nbpt_painter_create", _P, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_uint]),
     ("nbpt_painter_create_integrator", _P, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint]),
+    ("nbpt_painter_create_slab", _P, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.c_int, ctypes.c_int]),
     ("nbpt_painter_destroy", None, [_P]),
     ("nbpt_painter_start", ctypes.c_int, [_P, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, _P]),
     ("nbpt_painter_stop", ctypes.c_int, [_P]),
@@ -301,8 +302,9 @@ class Scene:
         return dict(zip(("ingest", "bvh", "upload", "total"), (float(x) for x in out)))
 
     def painter(self, samples_per_pixel: int, max_depth: int, seed: int = 1,
-                integrator: str = "bpt") -> "Painter":
-        return Painter(self, samples_per_pixel, max_depth, seed, integrator)
+                integrator: str = "bpt", slab: tuple[int, int] | None = None) -> "Painter":
+        """slab: rows [begin, end) of the last screen axis (nbpt_painter_create_slab)"""
+        return Painter(self, samples_per_pixel, max_depth, seed, integrator, slab)
 
     def trace(self, rays: np.ndarray, any_hit: bool = False):
         rays = _d(rays).reshape(-1, 2 * self.n)
@@ -373,16 +375,25 @@ class Painter:
     tracing with next-event estimation; max_depth is not used)."""
 
     def __init__(self, scene: Scene, samples_per_pixel: int, max_depth: int, seed: int = 1,
-                 integrator: str = "bpt"):
+                 integrator: str = "bpt", slab: tuple[int, int] | None = None):
         if integrator not in INTEGRATORS:
             raise PainterError(f"Unknown integrator {integrator!r}")
         self.scene = scene
         self.integrator = integrator
         self.spp = scene.actual_spp(samples_per_pixel)
-        self.h = lib().nbpt_painter_create_integrator(scene.h, INTEGRATORS[integrator], samples_per_pixel,
-                                                      max_depth, seed)
+        begin, end = slab if slab is not None else (0, -1)
+        self.h = lib().nbpt_painter_create_slab(scene.h, INTEGRATORS[integrator], samples_per_pixel,
+                                                max_depth, seed, begin, end)
         if not self.h:
             raise PainterError(lib().nbpt_last_error().decode())
+        # receiving pixels (the slab) and the pixels whose paths a pass renders
+        rows = scene.size[-1]
+        row = scene.pixels // rows
+        if slab is None:
+            self.pixels = self.sources = scene.pixels
+        else:
+            self.pixels = (end - begin) * row
+            self.sources = (min(rows, end + 1) - max(0, begin - 1)) * row
 
     def close(self):
         h = getattr(self, "h", None)
@@ -437,13 +448,13 @@ class Painter:
         self.wait()
 
     def images(self):
-        rgb = np.zeros((self.scene.pixels, 3), np.float32)
-        rgba = np.zeros((self.scene.pixels, 4), np.float32)
+        rgb = np.zeros((self.pixels, 3), np.float32)
+        rgba = np.zeros((self.pixels, 4), np.float32)
         _check(lib().nbpt_painter_images(self.h, _p(rgb, _F), _p(rgba, _F)))
         return rgb, rgba
 
     def samples(self):
-        P, S, n = self.scene.pixels, self.spp, self.scene.n
+        P, S, n = self.sources, self.spp, self.scene.n
         points = np.zeros((P, S, n - 1))
         colors = np.zeros((P, S, self.scene.channels), np.float32)
         valid = np.zeros((P, S), np.uint8)

@@ -370,7 +370,7 @@ struct SceneBase
         virtual int actual_spp(int) const = 0;
         virtual void set_integrator(int) = 0;
         virtual void render_samples(int, int, unsigned, unsigned, long long, long long, int, double*, float*, unsigned char*) = 0;
-        virtual void render_image(int, int, unsigned, int, int, float*, float*) = 0;
+        virtual void render_image(int, int, unsigned, int, int, long long, long long, float*, float*) = 0;
         virtual void paint(int, int, int, int, double*, float*) = 0;
         virtual void mesh_info(int, long long*) = 0;
         virtual void mesh_dump(int, double*, double*, int*, int*, double*, float*, double*, double*, unsigned*, unsigned*) = 0;
@@ -780,17 +780,22 @@ public:
         // Seeded passes accumulated by the reference's pixels::Pixels.
         // Samples are added pixel by pixel in index order, so the result does
         // not depend on the thread count.
+        // the samples of the pixels [source_begin, source_end) (all of them
+        // when source_end < 0) added to one pixels::Pixels in increasing pixel
+        // order, which is the order a receiving pixel takes its sources in
         void render_image(
                 const int spp,
                 const int max_depth,
                 const unsigned seed,
                 const int passes,
                 const int threads,
+                const long long source_begin,
+                const long long source_end,
                 float* const rgb_out,
                 float* const rgba_out) override
         {
                 const painter::Scene<N, T, Color>& sc = scene();
-                const long long pixels_count = pixel_count();
+                const long long pixels_count = source_end < 0 ? pixel_count() : source_end;
                 const int count = actual_spp(spp);
                 CollectNotifier<N - 1> notifier;
                 painter::pixels::Pixels<N - 1, T, Color> pixels(
@@ -802,7 +807,7 @@ public:
                 std::vector<unsigned char> valid(CHUNK * count);
                 for (int pass = 0; pass < passes; ++pass)
                 {
-                        for (long long b = 0; b < pixels_count; b += CHUNK)
+                        for (long long b = source_begin; b < pixels_count; b += CHUNK)
                         {
                                 const long long e = std::min(pixels_count, b + CHUNK);
                                 render_samples(
@@ -1631,7 +1636,27 @@ int oracle_render_image(
         return guarded(
                 [&]
                 {
-                        as_scene(scene)->render_image(spp, max_depth, seed, passes, threads, rgb, rgba);
+                        as_scene(scene)->render_image(spp, max_depth, seed, passes, threads, 0, -1, rgb, rgba);
+                });
+}
+
+int oracle_render_image_range(
+        void* const scene,
+        const int spp,
+        const int max_depth,
+        const unsigned seed,
+        const int passes,
+        const int threads,
+        const long long source_begin,
+        const long long source_end,
+        float* const rgb,
+        float* const rgba)
+{
+        return guarded(
+                [&]
+                {
+                        as_scene(scene)->render_image(
+                                spp, max_depth, seed, passes, threads, source_begin, source_end, rgb, rgba);
                 });
 }
 

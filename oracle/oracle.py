@@ -61,6 +61,7 @@ def lib():
             "oracle_scene_set_integrator": (ctypes.c_int, [_P, ctypes.c_int]),
             "oracle_render_samples": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.c_uint, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_int, _D, _F, _B]),
             "oracle_render_image": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.c_int, ctypes.c_int, _F, _F]),
+            "oracle_render_image_range": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.c_int, ctypes.c_int, ctypes.c_longlong, ctypes.c_longlong, _F, _F]),
             "oracle_paint": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _F]),
             "oracle_mesh_info": (ctypes.c_int, [_P, ctypes.c_int, _L]),
             "oracle_mesh_dump": (ctypes.c_int, [_P, ctypes.c_int, _D, _D, _I, _I, _D, _F, _D, _D, _U, _U]),
@@ -221,6 +222,16 @@ class Scene:
         rgba = np.zeros((self.pixels, 4), np.float32)
         _check(lib().oracle_render_image(self.h, spp, max_depth, seed, passes, threads or os.cpu_count(),
                                          ptr(rgb, _F), ptr(rgba, _F)))
+        return rgb, rgba
+
+    def render_image_range(self, spp: int, max_depth: int, seed: int, begin: int, end: int, passes: int = 1,
+                           threads: int | None = None):
+        """render_image from the samples of pixels [begin, end) only: pixels
+        whose every source lies in the range are complete."""
+        rgb = np.zeros((self.pixels, 3), np.float32)
+        rgba = np.zeros((self.pixels, 4), np.float32)
+        _check(lib().oracle_render_image_range(self.h, spp, max_depth, seed, passes, threads or os.cpu_count(),
+                                               begin, end, ptr(rgb, _F), ptr(rgba, _F)))
         return rgb, rgba
 
     def paint(self, spp: int, max_depth: int, passes: int = 1, threads: int | None = None):

@@ -61,3 +61,75 @@ def test_one_rank_is_its_own_time():
 
     assert bench.slowest_rank(3.0, 1, "cpu") == 3.0
     assert bench.job_throughput(10.0, 1, 2.0) == 5.0
+
+
+# --------------------------------------------------------------------------
+# One scene split across ranks by slabs of the screen (math_b200/tiles.py),
+# with the reference painter (the oracle) rendering each slab.
+
+
+def test_slab_rows_cover_the_screen_once():
+    from math_b200 import tiles
+
+    for rows in (1, 2, 7, 64, 96):
+        for world in range(1, min(rows, 9) + 1):
+            slabs = [tiles.slab_rows(rows, r, world) for r in range(world)]
+            assert slabs[0][0] == 0 and slabs[-1][1] == rows
+            assert all(a[1] == b[0] for a, b in zip(slabs, slabs[1:]))
+            sizes = [e - b for b, e in slabs]
+            assert max(sizes) - min(sizes) <= 1
+            for b, e in slabs:
+                sb, se = tiles.source_rows(rows, b, e)
+                assert sb == max(0, b - 1) and se == min(rows, e + 1)
+    with pytest.raises(ValueError):
+        tiles.slab_rows(3, 0, 4)
+
+
+def tile_rank(rank: int, world: int, port: int, out):
+    import sys
+
+    sys.path.insert(0, str(ROOT))
+    import numpy as np
+
+    from math_b200 import scenes, tiles
+    from oracle import oracle
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        desc = scenes.cornell_3d(size=(12, 10), subdivisions=2)
+        s = oracle.Scene(desc, "double", False)
+        size = desc["projector"]["size"]
+        rows = size[-1]
+        b, e = tiles.slab_rows(rows, rank, world)
+        sb, se = tiles.source_rows(rows, b, e)
+        # the slab's paths and those of its halo rows, accumulated; only the
+        # slab's own pixels are complete
+        first, last = tiles.pixel_range(size, sb, se)
+        rgb, _ = s.render_image_range(16, 5, 1, first, last, threads=2)
+        lo, hi = tiles.pixel_range(size, b, e)
+        whole = tiles.gather_image(np.ascontiguousarray(rgb[lo:hi]), rank, world, rows, size)
+        if rank == 0:
+            out["image"] = whole
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(300)
+@pytest.mark.parametrize("world", [2, 3])
+def test_slabs_rendered_on_ranks_make_the_whole_image(oracle_lib, world):
+    """Each gloo rank renders its slab with the reference painter (per-pixel
+    seeded streams, the halo rows recomputed); rank 0 gathers the slabs and
+    the result equals the one-rank image bit for bit."""
+    from math_b200 import scenes
+
+    port = free_port()
+    manager = mp.get_context("spawn").Manager()
+    out = manager.dict()
+    mp.start_processes(tile_rank, args=(world, port, out), nprocs=world, start_method="spawn", join=True)
+    desc = scenes.cornell_3d(size=(12, 10), subdivisions=2)
+    ref, _ = oracle_lib.Scene(desc, "double", False).render_image(16, 5, 1, threads=2)
+    import numpy as np
+
+    assert np.array_equal(out["image"], ref)
