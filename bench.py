@@ -287,9 +287,14 @@ def run_nbpt(args, rank: int, world: int, local: int):
     t0 = time.perf_counter()
     scene = P.Scene(desc, args.precision, spectrum)
     build_s = time.perf_counter() - t0
-    # every rank renders its own pass sequence of the whole screen
-    # (independent samples: weak scaling, no data-path collective)
-    painter = scene.painter(w["spp"], w["max_depth"], seed=1 + rank, integrator=args.integrator)
+    # one render split across the ranks by slabs of the screen (math_b200/
+    # tiles.py): each rank renders its slab's paths and its halo rows', no
+    # collective while rendering, one gather of the slab images at the end
+    from math_b200 import tiles
+
+    rows = desc["projector"]["size"][-1]
+    slab = tiles.slab_rows(rows, rank, world) if world > 1 else None
+    painter = scene.painter(w["spp"], w["max_depth"], seed=1, integrator=args.integrator, slab=slab)
     stream = torch.cuda.ExternalStream(painter_stream(painter))
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
 
@@ -326,15 +331,17 @@ def run_nbpt(args, rank: int, world: int, local: int):
     torch.cuda.synchronize()
     clock_info = clocks.stop()
 
+    # the screen's paths per step, all ranks together (the halo rows' second
+    # rendering is not counted)
     paths_per_step = scene.pixels * painter.spp
     ms = slowest_rank(float(np.sum(step_ms)), world, "cuda")
-    value = job_throughput(paths_per_step * args.steps, world, ms / 1000)
+    value = paths_per_step * args.steps / (ms / 1000)
 
     # end to end through the C ABI, every step a whole job: the scene built
     # from host arrays (host->device copies, BVH build, facet setup on the
     # device), one pass, and the image read back to host memory
-    rgb = np.zeros((scene.pixels, 3), np.float32)
-    rgba = np.zeros((scene.pixels, 4), np.float32)
+    rgb = np.zeros((painter.pixels, 3), np.float32)
+    rgba = np.zeros((painter.pixels, 4), np.float32)
     torch.cuda.synchronize()
     e2e_times = []
     h2d = 0
@@ -342,16 +349,19 @@ def run_nbpt(args, rank: int, world: int, local: int):
     for _ in range(args.steps):
         e0 = time.perf_counter()
         job_scene = P.Scene(desc, args.precision, spectrum)
-        job = job_scene.painter(w["spp"], w["max_depth"], seed=1 + rank, integrator=args.integrator)
+        job = job_scene.painter(w["spp"], w["max_depth"], seed=1, integrator=args.integrator, slab=slab)
         job.run(1)
         P._check(P.lib().nbpt_painter_images(job.h, P._p(rgb, P._F), P._p(rgba, P._F)))
+        if world > 1:
+            # the slab images gathered into the whole image on rank 0
+            tiles.gather_image(rgb, rank, world, rows, desc["projector"]["size"])
         e2e_times.append(time.perf_counter() - e0)
         h2d = job_scene.upload_bytes()
         build = job_scene.build_seconds()
         job.close()
         job_scene.close()
     e2e_s = slowest_rank(float(np.sum(e2e_times)), world, "cuda")
-    e2e = job_throughput(paths_per_step * args.steps, world, e2e_s)
+    e2e = paths_per_step * args.steps / e2e_s
 
     # scene resident: one pass through the C ABI plus the image read back
     torch.cuda.synchronize()
@@ -405,7 +415,7 @@ def run_nbpt(args, rank: int, world: int, local: int):
         line = {
             "metric": f"{args.integrator}_paths_per_second", "value": value, "unit": "paths/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "f32" if args.precision == "float" else "f64",
             "data": "synthetic (seeded generators)",
             "config": {"workload": f"{args.workload} {w['label']} ({scene.pixels} pixels), {w['spp']} spp "
@@ -421,9 +431,9 @@ def run_nbpt(args, rank: int, world: int, local: int):
                     "scene_build_seconds": build,
                     "note": "every step a whole job through the C ABI: scene from host arrays (copies, BVH "
                             "build, facet setup), one pass, RGB and RGBA images read back to host memory"},
-            "resident": {"value": paths_per_step * args.steps / resident_s, "unit": "paths/s",
+            "resident": {"value": painter.pixels * painter.spp * args.steps / resident_s, "unit": "paths/s",
                          "note": "scene resident; one pass through the C ABI plus the image read back"},
-            "streamed": {"value": paths_per_step * len(delivered) / streamed_s, "unit": "paths/s",
+            "streamed": {"value": painter.pixels * painter.spp * len(delivered) / streamed_s, "unit": "paths/s",
                          "note": "scene resident; passes on the painter's worker thread (nbpt_painter_start), "
                                  "each pass's RGB and RGBA images copied to pinned host memory and handed to a "
                                  "callback while the next pass renders"},
@@ -732,8 +742,9 @@ def run_batch(args, rank: int, world: int, local: int):
     build_s = time.perf_counter() - t0
     paths_per_batch = sum(j["paths"] for j in jobs)
     # the rank's jobs in waves of about equal paths; a step renders one wave
-    waves = [[jobs[k] for k in w] for w in rank_jobs([j["paths"] for j in jobs], min(args.waves, len(jobs)))]
-    wave_scenes = [[fp32[jobs.index(j)] for j in w] for w in waves]
+    groups = rank_jobs([j["paths"] for j in jobs], min(args.waves, len(jobs)))
+    waves = [[jobs[k] for k in g] for g in groups]
+    wave_scenes = [[fp32[k] for k in g] for g in groups]
     wave_paths = [sum(j["paths"] for j in w) for w in waves]
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
 
@@ -811,7 +822,7 @@ def run_batch(args, rank: int, world: int, local: int):
         line = {
             "metric": "batched_fp32_paths_per_second", "value": value, "unit": "paths/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * step_seconds / args.steps,
-            "higher_is_better": True, "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded generators)",
             "config": {"workload": BATCH_LABEL, "jobs": args.jobs, "jobs_this_rank": len(jobs),
                        "dims": {str(n): dims.count(n) for n in (3, 4, 5)}, "paths_per_batch": sum(all_paths),

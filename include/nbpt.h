@@ -347,6 +347,9 @@ int nbpt_scene_trace(
  * needs to start at zero.  The first call on each device looks up the
  * scratch's device address (cudaGetSymbolAddress), which can initialise the
  * CUDA context; make that first call before any stream capture begins.
+ * The address is kept for the life of the process: calls after the caller
+ * has run cudaDeviceReset on that device are not supported (the reset
+ * unloads the module the address belongs to).
  * Calls share the scratch: two calls that overlap on one device, from two
  * host threads, race on it and corrupt each other's results, so serialise
  * them.  The call returns when the results are in the host arrays. */

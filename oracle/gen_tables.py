@@ -12,7 +12,7 @@ from the reference sources by oracle/Makefile), and written as C++ arrays:
     Smits basis spectra (src/color/color.h:156-210).
 
 Run from the repository root when the oracle is built:
-    python -m math_b200.csrc.gen_tables
+    python -m oracle.gen_tables
 """
 
 from __future__ import annotations
@@ -22,7 +22,7 @@ from pathlib import Path
 
 import numpy as np
 
-ROOT = Path(__file__).resolve().parents[2]
+ROOT = Path(__file__).resolve().parents[1]
 sys.path.insert(0, str(ROOT))
 
 from oracle import oracle  # noqa: E402
@@ -41,7 +41,7 @@ def fmt(values, kind: str) -> str:
 
 def main() -> None:
     out = []
-    out.append("// Generated by math_b200/csrc/gen_tables.py from the reference painter's own")
+    out.append("// Generated by oracle/gen_tables.py from the reference painter's own")
     out.append("// tables (read through the CPU oracle).  Do not edit by hand.")
     out.append("// clang-format off")
     out.append("#pragma once")
@@ -78,7 +78,7 @@ def main() -> None:
     out.append("};")
     out.append("}")
     out.append("// clang-format on")
-    (Path(__file__).parent / "tables.inc").write_text("\n".join(out) + "\n")
+    (ROOT / "math_b200" / "csrc" / "tables.inc").write_text("\n".join(out) + "\n")
 
 
 if __name__ == "__main__":
