@@ -13,6 +13,7 @@
 #include <cooperative_groups.h>
 #include <cooperative_groups/scan.h>
 #include <cstdint>
+#include <type_traits>
 
 namespace nbpt
 {
@@ -186,10 +187,23 @@ __global__ void sj_points_kernel(
 }
 
 // Minimum resident blocks of 128 threads per SM asked of the compiler for
-// the path kernels (caps their registers); set from launch-shape sweeps.
-#ifndef NBPT_PATHS_MIN_BLOCKS
-#define NBPT_PATHS_MIN_BLOCKS 16
+// the path kernels, which caps their registers (65536 / (128 * blocks)), per
+// dimension and precision, from launch-bound sweeps of the mixed-scene
+// batch's jobs on a B200 (one pass each, best of three):
+//   float: 16 blocks (32 registers) in 3-, 4- and 5-space; 12 and 8 blocks
+//          were 1-8 % slower;
+//   double: 8 blocks (64 registers) in 4- and 5-space, 7-8 % faster than 16;
+//          12 blocks in 3-space, 5 % faster than 16.
+// NBPT_PATHS_MIN_BLOCKS, when defined, sets every kernel's (for sweeps).
+template <int N, typename T>
+struct PathsMinBlocks final
+{
+#ifdef NBPT_PATHS_MIN_BLOCKS
+        static constexpr int value = NBPT_PATHS_MIN_BLOCKS;
+#else
+        static constexpr int value = std::is_same_v<T, double> ? (N == 3 ? 12 : 8) : 16;
 #endif
+};
 
 // ---------------------------------------------------------------------------
 // Paths: one per pixel sample, with the random stream seed_seq{seed, pass,
@@ -351,7 +365,7 @@ __device__ inline unsigned reserve_together(unsigned* const counter, const unsig
 // reference's sequential order (camera subpath, light sample, light
 // subpath).
 template <int N, typename T>
-__global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_walk_kernel(
+__global__ void __launch_bounds__(128, (PathsMinBlocks<N, T>::value)) paths_walk_kernel(
         const DeviceScene<N, T, 1> scene,
         const long long begin,
         const long long end,
@@ -495,7 +509,7 @@ struct Arrival final
 
 // Persistent: the grid strides over the queued strategies.
 template <int N, typename T>
-__global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_connect_kernel(
+__global__ void __launch_bounds__(128, (PathsMinBlocks<N, T>::value)) paths_connect_kernel(
         const DeviceScene<N, T, 1> scene,
         const int max_depth,
         PathVertex<N, T, 1>* __restrict__ vertices,
@@ -553,7 +567,7 @@ __global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_connect_kern
 // t order from the path's stream where the light subpath left it; each
 // usable sample is kept and its strategy queued for the connect kernel.
 template <int N, typename T>
-__global__ void __launch_bounds__(128, NBPT_PATHS_MIN_BLOCKS) paths_light_kernel(
+__global__ void __launch_bounds__(128, (PathsMinBlocks<N, T>::value)) paths_light_kernel(
         const DeviceScene<N, T, 1> scene,
         const long long paths,
         const int max_depth,

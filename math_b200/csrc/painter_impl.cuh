@@ -2603,7 +2603,7 @@ public:
                         task_count_.allocate(3);
                         next_path_.allocate(1);
                         arrivals_.allocate(paths * max_depth_);
-                        connect_blocks_ = sms * NBPT_PATHS_MIN_BLOCKS;
+                        connect_blocks_ = sms * PathsMinBlocks<N, T>::value;
                 }
 
                 NBPT_CUDA(cudaEventCreate(&ev_start_));
