@@ -50,6 +50,9 @@ WORKLOADS = {
     "sphere4d": {"screen": [96, 96, 96], "spp": 8, "max_depth": 8, "spectrum": False, "precision": "float",
                  "label": "4-space hull of 150000 noisy points on S^3 (about 1M facets), ball light, "
                           "parallel projection, RGB"},
+    "mixed5d": {"screen": [12, 12, 12, 12], "spp": 16, "max_depth": 8, "spectrum": False, "precision": "float",
+                "label": "a 5-space job of the mixed batch's shape: box, ceiling light, hull of 24000 points on S^4 "
+                         "(739,994 facets), RGB (for kernel profiles)"},
 }
 
 
@@ -69,7 +72,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--screen", type=int, default=None,
                    help="edge of the voxel screen (default: the workload's 64), for smaller profiling runs")
-    p.add_argument("--workload", default="batch", choices=["batch", "cornell4d", "cornell3d", "sphere4d", "serve", "meshfile"],
+    p.add_argument("--workload", default="batch", choices=["batch", "cornell4d", "cornell3d", "sphere4d", "mixed5d", "serve", "meshfile"],
                    help="batch (the headline): the 64-scene mixed batch, FP32 through the job server against "
                         "plain FP64 one job at a time, with a served stream beside it; cornell4d, cornell3d, "
                         "sphere4d: single-scene workloads; serve: Poisson arrivals of renders into the job server "
@@ -119,6 +122,8 @@ def scene_desc(small: bool, screen: int | None = None, name: str = "cornell4d"):
         return scenes.cornell_4d(size=size, points=2000 if small else 20000)
     if name == "cornell3d":
         return scenes.cornell_3d(size=size, subdivisions=3 if small else 5)
+    if name == "mixed5d":
+        return scenes.mixed_scene(5, 2400 if small else 24000, list(size), 4056)
     return scenes.sphere_4d(size=size, points=15000 if small else 150000)
 
 

@@ -212,6 +212,23 @@ nbpt_painter* nbpt_painter_create_integrator(
 nbpt_painter* nbpt_painter_create_slab(
         nbpt_scene* scene, int integrator, int samples_per_pixel, int max_depth, unsigned seed, int slab_begin,
         int slab_end);
+/* Every painter argument at once: create_painter's integrator, samples per
+ * pixel and flat_shading (src/painter/painter.h:149-157; flat shading shades
+ * with the geometric normal instead of the facets' interpolated vertex
+ * normals, src/painter/integrators/com/normals.h:45-64), the BPT maximum
+ * depth, the random streams' seed, and the slab as nbpt_painter_create_slab
+ * (slab_end < 0: the whole screen). */
+typedef struct nbpt_painter_options
+{
+        int integrator; /* NBPT_INTEGRATOR_BPT or NBPT_INTEGRATOR_PT */
+        int samples_per_pixel;
+        int max_depth;
+        unsigned seed;
+        int flat_shading; /* 0 or 1 */
+        int slab_begin;
+        int slab_end;
+} nbpt_painter_options;
+nbpt_painter* nbpt_painter_create_options(nbpt_scene* scene, const nbpt_painter_options* options);
 void nbpt_painter_destroy(nbpt_painter* painter);
 
 /* ---- passes on a worker thread (the reference painter's thread and its

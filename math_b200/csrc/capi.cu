@@ -645,6 +645,28 @@ nbpt_painter* nbpt_painter_create_integrator(
         return nbpt_painter_create_slab(scene, integrator, samples_per_pixel, max_depth, seed, 0, -1);
 }
 
+nbpt_painter* nbpt_painter_create_options(nbpt_scene* scene, const nbpt_painter_options* options)
+{
+        nbpt_painter* out = nullptr;
+        guarded(
+                [&]
+                {
+                        require(options, "options");
+                        const nbpt_painter_options& o = *options;
+                        if (o.integrator != NBPT_INTEGRATOR_BPT && o.integrator != NBPT_INTEGRATOR_PT)
+                        {
+                                throw std::runtime_error("Unknown integrator " + std::to_string(o.integrator));
+                        }
+                        auto p = std::make_unique<nbpt_painter>();
+                        p->impl = scene_of(scene).create_painter(o.samples_per_pixel, o.max_depth, o.seed,
+                                                                 static_cast<nbpt::Integrator>(o.integrator),
+                                                                 o.slab_begin, o.slab_end, o.flat_shading != 0);
+                        out = p.release();
+                        return 0;
+                });
+        return out;
+}
+
 nbpt_painter* nbpt_painter_create_slab(
         nbpt_scene* scene,
         const int integrator,
@@ -665,7 +687,7 @@ nbpt_painter* nbpt_painter_create_slab(
                         auto p = std::make_unique<nbpt_painter>();
                         p->impl = scene_of(scene).create_painter(samples_per_pixel, max_depth, seed,
                                                                  static_cast<nbpt::Integrator>(integrator), slab_begin,
-                                                                 slab_end);
+                                                                 slab_end, false);
                         out = p.release();
                         return 0;
                 });

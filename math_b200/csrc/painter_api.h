@@ -106,7 +106,7 @@ public:
         // and the estimator of its own pixels); its images are the slab's
         virtual std::unique_ptr<Painter> create_painter(int samples_per_pixel, int max_depth, std::uint32_t seed,
                                                         Integrator integrator = Integrator::BPT, int slab_begin = 0,
-                                                        int slab_end = -1) = 0;
+                                                        int slab_end = -1, bool flat_shading = false) = 0;
         // device bytes create_painter would allocate
         virtual long long painter_bytes(int samples_per_pixel, int max_depth,
                                         Integrator integrator = Integrator::BPT) const = 0;

@@ -2216,7 +2216,8 @@ public:
         }
 
         std::unique_ptr<Painter> create_painter(int spp, int max_depth, std::uint32_t seed,
-                                                Integrator integrator, int slab_begin, int slab_end) override;
+                                                Integrator integrator, int slab_begin, int slab_end,
+                                                bool flat_shading) override;
         long long painter_bytes(int spp, int max_depth, Integrator integrator) const override;
 
         void trace(const double* rays, long long count, int any, int* kind, int* index, double* t, double* point) override;
@@ -2408,6 +2409,7 @@ template <int N, typename T, int C>
 class PainterT final : public Painter
 {
         const SceneT<N, T, C>* scene_;
+        bool flat_shading_;
         int spp_request_;
         int spp_;
         int strata_;
@@ -2505,8 +2507,10 @@ public:
         // either side (the filter reaches one pixel) and the estimator of the
         // slab's own pixels
         PainterT(const SceneT<N, T, C>* scene, const int spp, const int max_depth, const std::uint32_t seed,
-                 const Integrator integrator, const int slab_begin = 0, const int slab_end = -1)
+                 const Integrator integrator, const int slab_begin = 0, const int slab_end = -1,
+                 const bool flat_shading = false)
                 : scene_(scene),
+                  flat_shading_(flat_shading),
                   spp_request_(spp),
                   max_depth_(max_depth),
                   seed_(seed),
@@ -2691,6 +2695,8 @@ public:
                         NBPT_CUDA(cudaGetLastError());
                         NBPT_CUDA(cudaEventRecord(ev_paths_, stream_));
                         long long launches = 2;
+                        DeviceScene<N, T, 1> scene_1 = scene_->device_channel_0();
+                        scene_1.flat_shading = flat_shading_ ? 1 : 0;
                         if (integrator_ == Integrator::PT)
                         {
                                 // one launch per chunk: whole paths (pt.cuh)
@@ -2702,7 +2708,7 @@ public:
                                         NBPT_CUDA(cudaMemsetAsync(next_path_.get(), 0, sizeof(unsigned), stream_));
                                         pt_paths_kernel<N, T, C>
                                                 <<<std::min<long long>(connect_blocks_, blocks_for(n, 128)), 128, 0, stream_>>>(
-                                                        scene_->device_channel_0(), scene_->device_materials(),
+                                                        scene_1, scene_->device_materials(),
                                                         scene_->device_lights(), b, e, spp_, seed_, pass,
                                                         points_.get() + o * spp_ * (N - 1), colors_.get() + o * spp_ * C,
                                                         lum_.get() + o * spp_, valid_.get() + o * spp_,
@@ -2716,7 +2722,6 @@ public:
                         {
                                 // per chunk of pixels: subpaths, strategies, the s = 1
                                 // strategies, then the colours (kernels.cuh)
-                                const DeviceScene<N, T, 1>& scene_1 = scene_->device_channel_0();
                                 for (long long b = source_first_; b < source_first_ + sources_; b += chunk_pixels_)
                                 {
                                         const long long e = std::min(source_first_ + sources_, b + chunk_pixels_);
@@ -2910,9 +2915,11 @@ std::unique_ptr<Painter> SceneT<N, T, C>::create_painter(
         const std::uint32_t seed,
         const Integrator integrator,
         const int slab_begin,
-        const int slab_end)
+        const int slab_end,
+        const bool flat_shading)
 {
-        return std::make_unique<PainterT<N, T, C>>(this, spp, max_depth, seed, integrator, slab_begin, slab_end);
+        return std::make_unique<PainterT<N, T, C>>(this, spp, max_depth, seed, integrator, slab_begin, slab_end,
+                                                   flat_shading);
 }
 
 template <int N, typename T, int C>

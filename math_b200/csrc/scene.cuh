@@ -170,6 +170,9 @@ struct DeviceScene final
         int light_count;
         Projector<N, T> projector;
         ShadingConstants<T> shading;
+        // create_painter's flat_shading: shade with the geometric normal, not
+        // the facets' interpolated vertex normals (a painter's copy sets it)
+        int flat_shading = 0;
 };
 
 // ---------------------------------------------------------------------------
@@ -569,7 +572,10 @@ struct SceneQueries final
                 return h.kind == static_cast<int>(HitKind::FLAT) ? s.flat[h.index].light : -1;
         }
 
-        // integrators/com/normals.h:45-64 (smooth shading)
+        // integrators/com/normals.h:45-64; with flat shading the shading
+        // normal is the geometric one, which also ends scene_intersect at its
+        // first hit (visibility.h:187-190: the flipped geometric normal never
+        // faces the ray)
         __device__ Normals<N, T> compute_normals(const Hit<N, T>& h, const Vec<N, T>& ray_dir) const
         {
                 const Vec<N, T> g = geometric_normal(h);
@@ -577,7 +583,7 @@ struct SceneQueries final
                 Normals<N, T> r;
                 r.geometric = flip ? -g : g;
                 Vec<N, T> sn;
-                if (shading_normal(h, sn))
+                if (s.flat_shading == 0 && shading_normal(h, sn))
                 {
                         r.shading = flip ? -sn : sn;
                 }

@@ -48,6 +48,18 @@ class JobInfo(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class PainterOptions(ctypes.Structure):
+    _fields_ = [
+        ("integrator", ctypes.c_int),
+        ("samples_per_pixel", ctypes.c_int),
+        ("max_depth", ctypes.c_int),
+        ("seed", ctypes.c_uint),
+        ("flat_shading", ctypes.c_int),
+        ("slab_begin", ctypes.c_int),
+        ("slab_end", ctypes.c_int),
+    ]
+
+
 class Statistics(ctypes.Structure):
     _fields_ = [
         ("pass_number", ctypes.c_longlong),
@@ -98,6 +110,7 @@ SIGNATURES = [
     ("nbpt_painter_create", _P, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_uint]),
     ("nbpt_painter_create_integrator", _P, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint]),
     ("nbpt_painter_create_slab", _P, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.c_int, ctypes.c_int]),
+    ("nbpt_painter_create_options", _P, [_P, ctypes.POINTER(PainterOptions)]),
     ("nbpt_painter_destroy", None, [_P]),
     ("nbpt_painter_start", ctypes.c_int, [_P, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, _P]),
     ("nbpt_painter_stop", ctypes.c_int, [_P]),
@@ -302,9 +315,11 @@ class Scene:
         return dict(zip(("ingest", "bvh", "upload", "total"), (float(x) for x in out)))
 
     def painter(self, samples_per_pixel: int, max_depth: int, seed: int = 1,
-                integrator: str = "bpt", slab: tuple[int, int] | None = None) -> "Painter":
-        """slab: rows [begin, end) of the last screen axis (nbpt_painter_create_slab)"""
-        return Painter(self, samples_per_pixel, max_depth, seed, integrator, slab)
+                integrator: str = "bpt", slab: tuple[int, int] | None = None,
+                flat_shading: bool = False) -> "Painter":
+        """slab: rows [begin, end) of the last screen axis (nbpt_painter_create_slab);
+        flat_shading: create_painter's flat_shading"""
+        return Painter(self, samples_per_pixel, max_depth, seed, integrator, slab, flat_shading)
 
     def trace(self, rays: np.ndarray, any_hit: bool = False):
         rays = _d(rays).reshape(-1, 2 * self.n)
@@ -375,15 +390,16 @@ class Painter:
     tracing with next-event estimation; max_depth is not used)."""
 
     def __init__(self, scene: Scene, samples_per_pixel: int, max_depth: int, seed: int = 1,
-                 integrator: str = "bpt", slab: tuple[int, int] | None = None):
+                 integrator: str = "bpt", slab: tuple[int, int] | None = None, flat_shading: bool = False):
         if integrator not in INTEGRATORS:
             raise PainterError(f"Unknown integrator {integrator!r}")
         self.scene = scene
         self.integrator = integrator
         self.spp = scene.actual_spp(samples_per_pixel)
         begin, end = slab if slab is not None else (0, -1)
-        self.h = lib().nbpt_painter_create_slab(scene.h, INTEGRATORS[integrator], samples_per_pixel,
-                                                max_depth, seed, begin, end)
+        options = PainterOptions(INTEGRATORS[integrator], samples_per_pixel, max_depth, seed,
+                                 1 if flat_shading else 0, begin, end)
+        self.h = lib().nbpt_painter_create_options(scene.h, ctypes.byref(options))
         if not self.h:
             raise PainterError(lib().nbpt_last_error().decode())
         # receiving pixels (the slab) and the pixels whose paths a pass renders

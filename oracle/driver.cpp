@@ -369,6 +369,7 @@ struct SceneBase
         virtual long long pixel_count() const = 0;
         virtual int actual_spp(int) const = 0;
         virtual void set_integrator(int) = 0;
+        virtual void set_flat_shading(bool) = 0;
         virtual void render_samples(int, int, unsigned, unsigned, long long, long long, int, double*, float*, unsigned char*) = 0;
         virtual void render_image(int, int, unsigned, int, int, long long, long long, float*, float*) = 0;
         virtual void paint(int, int, int, int, double*, float*) = 0;
@@ -698,6 +699,14 @@ public:
         }
 
         int integrator_ = 0;
+        bool flat_shading_ = false;
+
+        // create_painter's flat_shading: bpt<true> / pt<true>, which shade
+        // with the geometric normal (integrators/com/normals.h:45-64)
+        void set_flat_shading(const bool flat) override
+        {
+                flat_shading_ = flat;
+        }
 
         void set_integrator(const int integrator) override
         {
@@ -760,9 +769,13 @@ public:
                                         const numerical::Ray<N, T> ray = sc.projector().ray(pixel_org + points[i]);
                                         const std::optional<Color> color =
                                                 integrator_ == 1
-                                                        ? painter::integrators::pt::pt<false>(sc, ray, *engine)
-                                                        : painter::integrators::bpt::bpt<false>(
-                                                                  sc, ray, *distribution, *engine);
+                                                        ? (flat_shading_
+                                                                   ? painter::integrators::pt::pt<true>(sc, ray, *engine)
+                                                                   : painter::integrators::pt::pt<false>(sc, ray, *engine))
+                                                        : (flat_shading_ ? painter::integrators::bpt::bpt<true>(
+                                                                                   sc, ray, *distribution, *engine)
+                                                                         : painter::integrators::bpt::bpt<false>(
+                                                                                   sc, ray, *distribution, *engine));
                                         const long long s = k * count + i;
                                         for (std::size_t d = 0; d < N - 1; ++d)
                                         {
@@ -870,7 +883,7 @@ public:
                 const auto start = std::chrono::steady_clock::now();
                 std::unique_ptr<painter::Painter> p = painter::create_painter<N, T, Color>(
                         integrator_ == 1 ? painter::Integrator::PT : painter::Integrator::BPT, &notifier, spp, passes,
-                        &sc, threads, false);
+                        &sc, threads, flat_shading_);
                 p->wait();
                 const double wall =
                         std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
@@ -1591,6 +1604,15 @@ int oracle_scene_actual_spp(void* const scene, const int spp)
                         res = as_scene(scene)->actual_spp(spp);
                 });
         return res;
+}
+
+int oracle_scene_set_flat_shading(void* const scene, const int flat)
+{
+        return guarded(
+                [&]
+                {
+                        as_scene(scene)->set_flat_shading(flat != 0);
+                });
 }
 
 int oracle_scene_set_integrator(void* const scene, const int integrator)

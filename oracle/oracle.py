@@ -59,6 +59,7 @@ def lib():
             "oracle_scene_pixel_count": (ctypes.c_longlong, [_P]),
             "oracle_scene_actual_spp": (ctypes.c_int, [_P, ctypes.c_int]),
             "oracle_scene_set_integrator": (ctypes.c_int, [_P, ctypes.c_int]),
+            "oracle_scene_set_flat_shading": (ctypes.c_int, [_P, ctypes.c_int]),
             "oracle_render_samples": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.c_uint, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_int, _D, _F, _B]),
             "oracle_render_image": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.c_int, ctypes.c_int, _F, _F]),
             "oracle_render_image_range": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.c_int, ctypes.c_int, ctypes.c_longlong, ctypes.c_longlong, _F, _F]),
@@ -193,6 +194,10 @@ class Scene:
 
     def actual_spp(self, spp: int) -> int:
         return _check(lib().oracle_scene_actual_spp(self.h, spp))
+
+    def set_flat_shading(self, flat: bool):
+        """create_painter's flat_shading for render_samples, render_image and paint."""
+        _check(lib().oracle_scene_set_flat_shading(self.h, 1 if flat else 0))
 
     def set_integrator(self, integrator: str):
         """'bpt' (the default) or 'pt' for render_samples, render_image and paint."""

@@ -284,3 +284,27 @@ def test_build_seconds(painter):
     assert all(v >= 0 for v in b.values())
     assert b["bvh"] > 0 and b["total"] > 0
     assert abs(b["ingest"] + b["bvh"] + b["upload"] - b["total"]) < 1e-9
+
+
+@pytest.mark.parametrize("name", list(SMALL))
+@pytest.mark.parametrize("integrator", ["bpt", "pt"])
+def test_flat_shading_paths_bit_exact(painter, oracle_lib, name, integrator):
+    """create_painter's flat_shading (bpt<true> / pt<true>: the geometric
+    normal shades, src/painter/integrators/com/normals.h:45-64): every sample
+    equals the reference's, and differs from smooth shading where the
+    sphere's interpolated normals were used."""
+    make, spectrum = SMALL[name]
+    desc = make()
+    o = oracle_lib.Scene(desc, "double", spectrum)
+    o.set_integrator(integrator)
+    o.set_flat_shading(True)
+    s = painter.Scene(desc, "double", spectrum)
+    p = s.painter(16, 5, seed=1, integrator=integrator, flat_shading=True)
+    p.run(1)
+    _, colors, valid = p.samples()
+    _, ref, ref_valid = o.render_samples(16, 5, seed=1)
+    assert np.array_equal(valid, ref_valid)
+    assert np.array_equal(colors, ref)
+    smooth = s.painter(16, 5, seed=1, integrator=integrator)
+    smooth.run(1)
+    assert not np.array_equal(smooth.samples()[1], colors)
