@@ -2459,7 +2459,11 @@ class PainterT final : public Painter
         Statistics statistics_{};
 
         // device memory for the per-path buffers of one chunk
+#ifdef NBPT_CHUNK_BUDGET_GB
+        static constexpr long long CHUNK_BUDGET = static_cast<long long>(NBPT_CHUNK_BUDGET_GB) << 30;
+#else
         static constexpr long long CHUNK_BUDGET = 4LL << 30;
+#endif
 
         // device bytes of one path's buffers in a chunk (vertices, tape,
         // random stream state, strategy tasks)
