@@ -412,6 +412,8 @@ int nbpt_scene_light_sample(
  * if cudaMalloc had run out of device memory (the server puts them back at the
  * head of its queue in arrival order) */
 int nbpt_test_server_fail_allocations(nbpt_server* server, int count);
+/* test hook: while hold is 1 the server admits no job (queued jobs wait) */
+int nbpt_test_server_hold(nbpt_server* server, int hold);
 /* raw PCG32 draws and uniform [0, 1) draws of a seed_seq stream, computed on the GPU */
 int nbpt_test_pcg(const unsigned* seed, int seed_words, int count, unsigned* out);
 int nbpt_test_canonical(const unsigned* seed, int seed_words, int count, int use_double, double* out);

@@ -985,6 +985,16 @@ int nbpt_server_cancel(nbpt_server* server, const long long job)
                 });
 }
 
+int nbpt_test_server_hold(nbpt_server* server, const int hold)
+{
+        return guarded(
+                [&]
+                {
+                        server_of(server).hold_admission(hold != 0);
+                        return 0;
+                });
+}
+
 int nbpt_test_server_fail_allocations(nbpt_server* server, const int count)
 {
         return guarded(

@@ -56,6 +56,11 @@ public:
         // takes no more passes.
         virtual void cancel() = 0;
         virtual bool cancelled() const = 0;
+        // After the passes enqueued so far (it waits for them): gives the
+        // per-chunk path buffers back to the library's buffer cache and
+        // returns their bytes; the next enqueue_passes allocates them again.
+        // Images, samples and statistics stay.
+        virtual long long release_scratch() = 0;
 };
 
 class Scene

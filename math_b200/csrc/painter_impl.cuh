@@ -67,6 +67,15 @@ public:
         DeviceArray(const DeviceArray&) = delete;
         DeviceArray& operator=(const DeviceArray&) = delete;
 
+        // gives the buffer back to the library's cache; returns its bytes
+        std::size_t free()
+        {
+                const std::size_t b = ptr_ ? size_ * sizeof(X) : 0;
+                release();
+                size_ = 0;
+                return b;
+        }
+
         ~DeviceArray()
         {
                 release();
@@ -2437,6 +2446,7 @@ class PainterT final : public Painter
         DeviceArray<PixelState<C>> state_;
         DeviceArray<PathStats> stats_;
         DeviceArray<unsigned> cancel_; // nonzero: the passes take no more paths
+        bool scratch_ready_ = false;   // the per-chunk path buffers are allocated
         cudaStream_t cancel_stream_ = nullptr;
         std::mutex cancel_mutex_;
         std::atomic<bool> cancelled_{false};
@@ -2629,14 +2639,9 @@ public:
                 else
                 {
                         tape_words_ = tape_words(max_depth_);
-                        const long long paths = chunk_pixels_ * spp_;
-                        tape_.allocate(paths * tape_words_);
-                        vertices_.allocate(paths * 2 * (max_depth_ + 1));
-                        rng_.allocate(paths);
-                        tasks_.allocate(paths * tape_slot_count(max_depth_));
+                        allocate_scratch();
                         task_count_.allocate(3);
                         next_path_.allocate(1);
-                        arrivals_.allocate(paths * max_depth_);
                         connect_blocks_ = sms * PathsMinBlocks<N, T>::value;
                 }
 
@@ -2684,6 +2689,30 @@ public:
                 return stream_;
         }
 
+        // the per-chunk buffers of the BPT path kernels
+        void allocate_scratch()
+        {
+                const long long paths = chunk_pixels_ * spp_;
+                tape_.allocate(paths * tape_words_);
+                vertices_.allocate(paths * 2 * (max_depth_ + 1));
+                rng_.allocate(paths);
+                tasks_.allocate(paths * tape_slot_count(max_depth_));
+                arrivals_.allocate(paths * max_depth_);
+                scratch_ready_ = true;
+        }
+
+        long long release_scratch() override
+        {
+                NBPT_CUDA(cudaStreamSynchronize(stream_));
+                if (integrator_ == Integrator::PT || !scratch_ready_)
+                {
+                        return 0;
+                }
+                scratch_ready_ = false;
+                return static_cast<long long>(tape_.free() + vertices_.free() + rng_.free() + tasks_.free() +
+                                              arrivals_.free());
+        }
+
         void cancel() override
         {
                 const std::lock_guard lock(cancel_mutex_);
@@ -2710,6 +2739,10 @@ public:
                 if (cancelled_)
                 {
                         throw std::runtime_error("the painter was cancelled");
+                }
+                if (integrator_ == Integrator::BPT && !scratch_ready_)
+                {
+                        allocate_scratch();
                 }
                 const DeviceScene<N, T, C>& scene = scene_->device();
                 for (int k = 0; k < passes; ++k)

@@ -6,6 +6,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cstdlib>
@@ -61,6 +62,9 @@ struct Server::Job final
         bool pass_in_flight = false;
         std::atomic<bool> cancel_requested{false};
         bool cancel_sent = false;
+        // budget bytes a finished job keeps until it is released: a render the
+        // server created keeps its images and pixel state
+        long long held = 0;
 };
 
 Server::Server(const int max_jobs, const long long memory_budget)
@@ -282,12 +286,15 @@ void Server::release(const long long job)
                         throw std::runtime_error("job " + std::to_string(job) + " is not finished");
                 }
                 jobs_.erase(job);
+                used_ -= j->held;
+                j->held = 0;
         }
         if (j->owned)
         {
                 cudaSetDevice(j->device);
                 j->owned.reset();
         }
+        changed_.notify_all();
 }
 
 JobInfo Server::wait(const long long job)
@@ -307,6 +314,10 @@ JobInfo Server::wait(const long long job)
 bool Server::admit_locked()
 {
         bool any = false;
+        if (hold_)
+        {
+                return false;
+        }
         while (!queue_.empty() && static_cast<int>(running_.size()) < max_jobs_)
         {
                 const std::shared_ptr<Job>& j = queue_.front();
@@ -329,9 +340,25 @@ void Server::finish_locked(Job& job, const JobState state, const std::string& er
         job.info.state = state;
         job.info.error = error;
         job.info.finished = now();
-        used_ -= job.info.footprint;
-        budget_ = initial_budget_; // memory freed: admit by the estimate again
         cudaSetDevice(job.device);
+        // a render the server created keeps its images until it is released:
+        // its per-chunk path buffers go back now, the rest stays counted
+        long long freed = job.info.footprint;
+        if (job.owned)
+        {
+                try
+                {
+                        freed = std::min(job.info.footprint, job.owned->release_scratch());
+                }
+                catch (const std::exception&)
+                {
+                        cudaGetLastError();
+                        freed = 0;
+                }
+        }
+        job.held = job.info.footprint - freed;
+        used_ -= freed;
+        budget_ = initial_budget_; // memory freed: admit by the estimate again
         if (state == JobState::DONE && job.first && job.done)
         {
                 const cudaEvent_t reference = static_cast<cudaEvent_t>(reference_event_);
@@ -390,6 +417,15 @@ void Server::fail_next_creations(const int count)
 {
         const std::lock_guard lock(mutex_);
         fail_creations_ = count;
+}
+
+void Server::hold_admission(const bool hold)
+{
+        {
+                const std::lock_guard lock(mutex_);
+                hold_ = hold;
+        }
+        changed_.notify_all();
 }
 
 // The worker keeps one pass of every running job in flight, on the job's own

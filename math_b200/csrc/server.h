@@ -79,6 +79,8 @@ public:
         // test hook: the next `count` renders the server creates fail as if
         // cudaMalloc had run out of device memory
         void fail_next_creations(int count);
+        // test hook: while held, the server admits no job
+        void hold_admission(bool hold);
         double now() const;
         // finishes the running jobs, fails the queued ones and stops the
         // worker; the destructor calls it, and so does process exit for a
@@ -106,6 +108,7 @@ private:
         long long next_id_ = 0;
         bool stop_ = false;
         int fail_creations_ = 0;
+        bool hold_ = false;
         void* reference_event_ = nullptr; // cudaEvent_t recorded at construction
         std::thread worker_;
 };

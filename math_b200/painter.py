@@ -142,6 +142,7 @@ SIGNATURES = [
     ("nbpt_scene_brdf_sample", ctypes.c_int, [_P, ctypes.c_int, _D, _D, _U, ctypes.c_int, _D, _D, _F]),
     ("nbpt_scene_light_sample", ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, _U, ctypes.c_int, _D, _D, _F]),
     ("nbpt_test_server_fail_allocations", ctypes.c_int, [_P, ctypes.c_int]),
+    ("nbpt_test_server_hold", ctypes.c_int, [_P, ctypes.c_int]),
     ("nbpt_test_pcg", ctypes.c_int, [_U, ctypes.c_int, ctypes.c_int, _U]),
     ("nbpt_test_canonical", ctypes.c_int, [_U, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D]),
     ("nbpt_test_sj_points", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _U, ctypes.c_int, _D]),
@@ -568,6 +569,10 @@ class Server:
         d = info.as_dict()
         d["error"] = lib().nbpt_last_error().decode() if r < 0 else None
         return d
+
+    def hold_admission(self, hold: bool):
+        """test hook: while held the server admits no job"""
+        _check(lib().nbpt_test_server_hold(self.h, 1 if hold else 0))
 
     def fail_next_allocations(self, count: int):
         """test hook: the next `count` renders created at admission fail as out of device memory"""

@@ -122,9 +122,14 @@ def test_out_of_memory_at_admission_keeps_arrival_order(painter):
     blocker = server.submit_render(big, 16, 6, seed=1, passes=1000)
     while server.job(blocker)["state"] != 1:
         time.sleep(0.001)
-    server.fail_next_allocations(2)
+    # the four renders queue while admission is held; when it resumes the
+    # first two are admitted together and both find the device full
+    server.hold_admission(True)
     ids = [server.submit_render(s, j["spp"], j["max_depth"], seed=6) for s, j in zip(built, jobs)]
+    server.fail_next_allocations(2)
+    server.hold_admission(False)
     time.sleep(0.2)
+    assert all(server.job(i)["state"] == 0 for i in ids)  # all queued again: nothing admitted since
     server.cancel(blocker)
     assert "cancelled" in server.try_wait(blocker)["error"]
     infos = [server.try_wait(i) for i in ids]
