@@ -5,7 +5,9 @@
 
 #include <cuda_runtime.h>
 
+#include <iterator>
 #include <map>
+#include <unordered_map>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -20,6 +22,8 @@ struct Cache final
         std::mutex mutex;
         // device -> (rounded size -> free buffers)
         std::map<int, std::multimap<std::size_t, void*>> free;
+        // buffers handed out for a smaller request than their size
+        std::unordered_map<void*, std::size_t> larger;
         std::size_t bytes = 0;
 };
 
@@ -72,23 +76,42 @@ void* allocate(const std::size_t bytes, int* const device)
         {
                 const std::lock_guard lock(c.mutex);
                 auto& blocks = c.free[d];
-                const auto i = blocks.find(size);
-                if (i != blocks.end())
+                // small sizes: the same power of two; large ones: the smallest
+                // cached buffer that holds the request with at most a quarter
+                // to spare (jobs of similar sizes reuse one another's buffers)
+                const auto i = blocks.lower_bound(size);
+                if (i != blocks.end() && (i->first == size || (size > (std::size_t{1} << 20) &&
+                                                               i->first <= size + size / 4)))
                 {
                         void* const p = i->second;
+                        const std::size_t have = i->first;
                         blocks.erase(i);
-                        c.bytes -= size;
+                        c.bytes -= have;
+                        if (have != size)
+                        {
+                                c.larger[p] = have;
+                        }
                         return p;
                 }
         }
         void* p = nullptr;
         e = cudaMalloc(&p, size);
-        if (e == cudaErrorMemoryAllocation)
+        while (e == cudaErrorMemoryAllocation)
         {
+                // give cached buffers back to the driver, the largest first,
+                // until the request fits (each cudaFree waits for the device)
                 cudaGetLastError();
                 {
                         const std::lock_guard lock(c.mutex);
-                        c.bytes -= free_device(c.free[d]);
+                        auto& blocks = c.free[d];
+                        if (blocks.empty())
+                        {
+                                break;
+                        }
+                        const auto last = std::prev(blocks.end());
+                        cudaFree(last->second);
+                        c.bytes -= last->first;
+                        blocks.erase(last);
                 }
                 e = cudaMalloc(&p, size);
         }
@@ -108,7 +131,13 @@ void release(void* const p, const std::size_t bytes, const int device)
         }
         Cache& c = cache();
         const std::lock_guard lock(c.mutex);
-        const std::size_t size = rounded(bytes);
+        std::size_t size = rounded(bytes);
+        const auto l = c.larger.find(p);
+        if (l != c.larger.end())
+        {
+                size = l->second;
+                c.larger.erase(l);
+        }
         c.free[device].emplace(size, p);
         c.bytes += size;
 }

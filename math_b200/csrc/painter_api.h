@@ -111,10 +111,15 @@ public:
         // and the estimator of its own pixels); its images are the slab's
         virtual std::unique_ptr<Painter> create_painter(int samples_per_pixel, int max_depth, std::uint32_t seed,
                                                         Integrator integrator = Integrator::BPT, int slab_begin = 0,
-                                                        int slab_end = -1, bool flat_shading = false) = 0;
-        // device bytes create_painter would allocate
+                                                        int slab_end = -1, bool flat_shading = false,
+                                                        long long chunk_budget = 0) = 0;
+        // device bytes create_painter would allocate.  chunk_budget: bytes
+        // for the buffers of one chunk of paths (0: a fifth of the device's
+        // memory within [4, 32] GiB); the job server gives each of its slots
+        // a share of its memory budget
         virtual long long painter_bytes(int samples_per_pixel, int max_depth,
-                                        Integrator integrator = Integrator::BPT) const = 0;
+                                        Integrator integrator = Integrator::BPT,
+                                        long long chunk_budget = 0) const = 0;
 
         // verification: closest hit (any == 0) or any hit of rays [n][2N]
         virtual void trace(const double* rays, long long count, int any, int* kind, int* index, double* t,

@@ -2226,8 +2226,8 @@ public:
 
         std::unique_ptr<Painter> create_painter(int spp, int max_depth, std::uint32_t seed,
                                                 Integrator integrator, int slab_begin, int slab_end,
-                                                bool flat_shading) override;
-        long long painter_bytes(int spp, int max_depth, Integrator integrator) const override;
+                                                bool flat_shading, long long chunk_budget) override;
+        long long painter_bytes(int spp, int max_depth, Integrator integrator, long long chunk_budget) const override;
 
         void trace(const double* rays, long long count, int any, int* kind, int* index, double* t, double* point) override;
         void trace_device(const double* rays, long long count, int any, int* kind, int* index, double* t,
@@ -2419,6 +2419,7 @@ class PainterT final : public Painter
 {
         const SceneT<N, T, C>* scene_;
         bool flat_shading_;
+        long long chunk_budget_; // bytes for the chunk buffers, 0: chunk_budget()
         int spp_request_;
         int spp_;
         int strata_;
@@ -2514,29 +2515,31 @@ class PainterT final : public Painter
         // 32-bit path counter
         static constexpr long long PT_CHUNK_PATHS = 1LL << 30;
 
+        // budget: bytes for the chunk buffers, 0 for chunk_budget()
         static long long chunk_pixels(const long long pixels, const int spp, const int max_depth,
-                                      const Integrator integrator)
+                                      const Integrator integrator, const long long budget = 0)
         {
                 if (integrator == Integrator::PT)
                 {
                         return std::max(1LL, std::min(pixels, PT_CHUNK_PATHS / spp));
                 }
                 const long long per_pixel = chunk_path_bytes(max_depth) * spp;
-                long long c = std::max(1LL, std::min(pixels, chunk_budget() / per_pixel));
+                const long long b = budget > 0 ? std::min(budget, chunk_budget()) : chunk_budget();
+                long long c = std::max(1LL, std::min(pixels, b / per_pixel));
                 return std::min(c, (TASK_MAX_PATHS - 1) / spp);
         }
 
 public:
         // device bytes a painter of these parameters allocates
         static long long estimate_bytes(const long long pixels, const int spp, const int max_depth, const int strata,
-                                        const Integrator integrator)
+                                        const Integrator integrator, const long long budget = 0)
         {
                 const long long samples = pixels * spp;
                 const long long per_sample = (N - 1) * sizeof(T) + C * 4 + 4 + 1;
                 const long long per_pixel = sizeof(PixelState<C>) + 12 + 16;
                 const long long chunk = integrator == Integrator::PT
                                                 ? 4 // the path counter; the direct-lighting records are small
-                                                : chunk_pixels(pixels, spp, max_depth, integrator) * spp *
+                                                : chunk_pixels(pixels, spp, max_depth, integrator, budget) * spp *
                                                           chunk_path_bytes(max_depth);
                 return (strata + 1) * sizeof(T) + samples * per_sample + pixels * per_pixel + sizeof(PathStats) +
                        chunk;
@@ -2548,9 +2551,10 @@ public:
         // slab's own pixels
         PainterT(const SceneT<N, T, C>* scene, const int spp, const int max_depth, const std::uint32_t seed,
                  const Integrator integrator, const int slab_begin = 0, const int slab_end = -1,
-                 const bool flat_shading = false)
+                 const bool flat_shading = false, const long long chunk_budget = 0)
                 : scene_(scene),
                   flat_shading_(flat_shading),
+                  chunk_budget_(chunk_budget),
                   spp_request_(spp),
                   max_depth_(max_depth),
                   seed_(seed),
@@ -2627,7 +2631,7 @@ public:
                 NBPT_CUDA(cudaGetDevice(&device));
                 device_ = device;
                 NBPT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-                chunk_pixels_ = chunk_pixels(sources_, spp_, max_depth_, integrator_);
+                chunk_pixels_ = chunk_pixels(sources_, spp_, max_depth_, integrator_, chunk_budget_);
                 if (integrator_ == Integrator::PT)
                 {
                         next_path_.allocate(1);
@@ -2979,20 +2983,23 @@ std::unique_ptr<Painter> SceneT<N, T, C>::create_painter(
         const Integrator integrator,
         const int slab_begin,
         const int slab_end,
-        const bool flat_shading)
+        const bool flat_shading,
+        const long long chunk_budget)
 {
         return std::make_unique<PainterT<N, T, C>>(this, spp, max_depth, seed, integrator, slab_begin, slab_end,
-                                                   flat_shading);
+                                                   flat_shading, chunk_budget);
 }
 
 template <int N, typename T, int C>
-long long SceneT<N, T, C>::painter_bytes(const int spp, const int max_depth, const Integrator integrator) const
+long long SceneT<N, T, C>::painter_bytes(const int spp, const int max_depth, const Integrator integrator,
+                                         const long long chunk_budget) const
 {
         if (spp < 1 || (integrator == Integrator::BPT && max_depth < 1))
         {
                 throw std::runtime_error("painter samples per pixel and maximum depth must be positive");
         }
-        return PainterT<N, T, C>::estimate_bytes(pixel_count(), actual_spp(spp), max_depth, strata(spp), integrator);
+        return PainterT<N, T, C>::estimate_bytes(pixel_count(), actual_spp(spp), max_depth, strata(spp), integrator,
+                                                 chunk_budget);
 }
 
 template <int N, typename T, int C>

@@ -210,7 +210,8 @@ long long Server::submit_render(Scene* const scene, const int spp, const int max
         job->info.state = JobState::QUEUED;
         job->info.passes = passes;
         job->info.passes_done = 0;
-        job->info.footprint = scene->painter_bytes(spp, max_depth) + scene->device_bytes();
+        job->info.footprint =
+                scene->painter_bytes(spp, max_depth, Integrator::BPT, slot_chunk_budget()) + scene->device_bytes();
         job->info.submitted = now();
         job->info.started = -1;
         job->info.finished = -1;
@@ -419,6 +420,15 @@ void Server::fail_next_creations(const int count)
         fail_creations_ = count;
 }
 
+// The chunk buffers of a render the server creates: an equal share of the
+// memory budget per slot, so that max_jobs renders fit at once, and at least
+// 4 GiB.  Running jobs overlap one another's chunk tails, so smaller chunks
+// cost less here than in a render alone.
+long long Server::slot_chunk_budget() const
+{
+        return std::max(4LL << 30, initial_budget_ / std::max(1, max_jobs_));
+}
+
 void Server::hold_admission(const bool hold)
 {
         {
@@ -495,7 +505,9 @@ void Server::run()
                                                         throw CudaError("cudaMalloc (a failure the test asked for)",
                                                                         cudaErrorMemoryAllocation);
                                                 }
-                                                j->owned = j->scene->create_painter(j->spp, j->max_depth, j->seed);
+                                                j->owned = j->scene->create_painter(j->spp, j->max_depth, j->seed,
+                                                                                    Integrator::BPT, 0, -1, false,
+                                                                                    slot_chunk_budget());
                                         }
                                         catch (const CudaError& e)
                                         {

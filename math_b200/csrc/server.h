@@ -93,6 +93,7 @@ private:
 
         void run();
         bool admit_locked();
+        long long slot_chunk_budget() const;
         void finish_locked(Job& job, JobState state, const std::string& error);
 
         int max_jobs_;

@@ -137,7 +137,7 @@ def test_out_of_memory_at_admission_keeps_arrival_order(painter):
     # head of the queue, and admission kept the arrival order
     assert all(i["state"] == 2 for i in infos), infos
     started = [i["started"] for i in infos]
-    assert started == sorted(started)
+    assert started == sorted(started), [(i["submitted"], i["started"], i["finished"]) for i in infos]
     for k, i in enumerate(ids):
         rgb, _ = server.images(i, built[k].pixels)
         assert np.array_equal(rgb, alone[k])
