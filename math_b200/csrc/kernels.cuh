@@ -408,17 +408,21 @@ __global__ void __launch_bounds__(128, (PathsMinBlocks<N, T>::value)) paths_walk
                         {
                                 break;
                         }
-                        const long long local_pixel = i / spp;
-                        const int sample = static_cast<int>(i - local_pixel * spp);
-                        const long long p = begin + local_pixel;
+                        // 32-bit index arithmetic: a chunk's path index and a
+                        // screen's pixel index fit in 31 bits (the painter's chunk
+                        // limits and its screen check), and a 64-bit division costs
+                        // several times a 32-bit one
+                        const unsigned local_pixel = static_cast<unsigned>(i) / static_cast<unsigned>(spp);
+                        const int sample = static_cast<int>(static_cast<unsigned>(i) - local_pixel * spp);
+                        const unsigned p = static_cast<unsigned>(begin) + local_pixel;
                         Vec<N - 1, T> point;
                         {
-                                long long rest = p;
+                                unsigned rest = p;
 #pragma unroll
                                 for (int d = 0; d < N - 1; ++d)
                                 {
-                                        const int size = scene.projector.size[d];
-                                        const long long r = rest / size;
+                                        const unsigned size = static_cast<unsigned>(scene.projector.size[d]);
+                                        const unsigned r = rest / size;
                                         point[d] = static_cast<T>(static_cast<int>(rest - r * size)) +
                                                    points[i * (N - 1) + d];
                                         rest = r;

@@ -2582,6 +2582,11 @@ public:
                                 + std::to_string(MAX_GROUP) + " of one pass");
                 }
                 pixels_ = scene_->pixel_count();
+                if (pixels_ >= (1LL << 31))
+                {
+                        throw std::runtime_error("a screen of " + std::to_string(pixels_) +
+                                                 " pixels: at most 2^31 - 1 are supported");
+                }
                 sources_ = pixels_;
                 if (slab_end >= 0)
                 {
