@@ -216,8 +216,21 @@ nbpt_painter* nbpt_painter_create_slab(
  * pixel and flat_shading (src/painter/painter.h:149-157; flat shading shades
  * with the geometric normal instead of the facets' interpolated vertex
  * normals, src/painter/integrators/com/normals.h:45-64), the BPT maximum
- * depth, the random streams' seed, and the slab as nbpt_painter_create_slab
- * (slab_end < 0: the whole screen). */
+ * depth, the random streams' seed, the slab as nbpt_painter_create_slab
+ * (slab_end < 0: the whole screen), and the type of the per-pixel radiance
+ * and weight sums of the estimator (src/painter/pixels/pixels.cpp:83-95,
+ * samples/com/merge.h:199-233):
+ *   NBPT_PIXEL_SUMS_FLOAT   float, as the reference's Color keeps them
+ *                           (src/color/color.h:416-417): the images of a
+ *                           double-precision scene are the reference's;
+ *   NBPT_PIXEL_SUMS_DOUBLE  double; held-out samples stay float;
+ *   NBPT_PIXEL_SUMS_DEFAULT float for a double-precision scene, double for a
+ *                           single-precision one (the single-precision trace
+ *                           keeps its radiance sums in double).
+ * The other painter constructors take NBPT_PIXEL_SUMS_DEFAULT. */
+#define NBPT_PIXEL_SUMS_DEFAULT 0
+#define NBPT_PIXEL_SUMS_FLOAT 1
+#define NBPT_PIXEL_SUMS_DOUBLE 2
 typedef struct nbpt_painter_options
 {
         int integrator; /* NBPT_INTEGRATOR_BPT or NBPT_INTEGRATOR_PT */
@@ -227,6 +240,7 @@ typedef struct nbpt_painter_options
         int flat_shading; /* 0 or 1 */
         int slab_begin;
         int slab_end;
+        int pixel_sums; /* NBPT_PIXEL_SUMS_* */
 } nbpt_painter_options;
 nbpt_painter* nbpt_painter_create_options(nbpt_scene* scene, const nbpt_painter_options* options);
 void nbpt_painter_destroy(nbpt_painter* painter);

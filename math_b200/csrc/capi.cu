@@ -660,7 +660,8 @@ nbpt_painter* nbpt_painter_create_options(nbpt_scene* scene, const nbpt_painter_
                         auto p = std::make_unique<nbpt_painter>();
                         p->impl = scene_of(scene).create_painter(o.samples_per_pixel, o.max_depth, o.seed,
                                                                  static_cast<nbpt::Integrator>(o.integrator),
-                                                                 o.slab_begin, o.slab_end, o.flat_shading != 0);
+                                                                 o.slab_begin, o.slab_end, o.flat_shading != 0, 0,
+                                                                 o.pixel_sums);
                         out = p.release();
                         return 0;
                 });

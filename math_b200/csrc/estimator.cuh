@@ -19,6 +19,11 @@
 // them.  From the same samples the image is therefore the reference's, bit
 // for bit.  One thread gathers for one receiving pixel, so no atomics are
 // needed.
+//
+// The same merges run with the radiance and weight sums in double (the sum
+// type S of the sets): the single-precision trace keeps its per-pixel sums
+// in double, so that long renders do not lose the small late contributions
+// to float rounding.  Held-out samples are float in both forms.
 #pragma once
 
 #include "core.cuh"
@@ -35,11 +40,14 @@ inline constexpr int MAX_GROUP = 256;
 // ---------------------------------------------------------------------------
 // sample sets (samples/color.h, samples/background.h)
 
-template <int C>
+// S is the type of the sums: float as the reference keeps them (the
+// bit-exact mode), or double (the radiance sums of the single-precision
+// trace kept in double); held-out entries are float samples in both.
+template <int C, typename S = float>
 struct ColorSet final
 {
-        float color_sum[C];
-        float weight_sum;
+        S color_sum[C];
+        S weight_sum;
         float colors[HELD_OUT][C];
         float weights[HELD_OUT];
         float contributions[HELD_OUT];
@@ -47,19 +55,20 @@ struct ColorSet final
         int full;  // more than HELD_OUT samples seen: the sums are valid
 };
 
+template <typename S = float>
 struct BackgroundSet final
 {
-        float weight_sum;
+        S weight_sum;
         float weights[HELD_OUT];
         int count;
         int full;
 };
 
-template <int C>
+template <int C, typename S = float>
 struct PixelState final
 {
-        ColorSet<C> color;
-        BackgroundSet background;
+        ColorSet<C, S> color;
+        BackgroundSet<S> background;
 };
 
 // A group of one source pixel's samples for one receiving pixel: sample
@@ -90,10 +99,10 @@ struct ColorGroup final
 // ---- merges (com/merge.h) ------------------------------------------------
 
 // Entry accessor over a set or a group, in the set's (sorted) order.
-template <int C>
+template <int C, typename S>
 struct SetView final
 {
-        const ColorSet<C>* s;
+        const ColorSet<C, S>* s;
         const ColorGroup<C>* g; // when merging a fresh group
         int g_full;
         // group held-out positions: 0, 1 -> order[0], order[1]; 2, 3 -> order[n-2], order[n-1]
@@ -144,8 +153,8 @@ struct SetView final
         }
 };
 
-template <int C>
-NBPT_HD void copy_entry(ColorSet<C>& out, const int to, const SetView<C>& from, const int k)
+template <int C, typename S>
+NBPT_HD void copy_entry(ColorSet<C, S>& out, const int to, const SetView<C, S>& from, const int k)
 {
 #pragma unroll 8
         for (int c = 0; c < C; ++c)
@@ -156,8 +165,8 @@ NBPT_HD void copy_entry(ColorSet<C>& out, const int to, const SetView<C>& from, 
         out.contributions[to] = from.contribution(k);
 }
 
-template <int C>
-NBPT_HD void sum_entry(float* color_sum, float& weight_sum, const SetView<C>& from, const int k)
+template <int C, typename S>
+NBPT_HD void sum_entry(S* color_sum, S& weight_sum, const SetView<C, S>& from, const int k)
 {
 #pragma unroll 8
         for (int c = 0; c < C; ++c)
@@ -168,14 +177,14 @@ NBPT_HD void sum_entry(float* color_sum, float& weight_sum, const SetView<C>& fr
 }
 
 // merge_with_sum (com/merge.h:199-233, samples/merge.cpp:109-145)
-template <int C>
-NBPT_HD void merge_colors_with_sum(const SetView<C>& a, const SetView<C>& b, const float* a_sum, float a_wsum,
-                                   const float* b_sum, float b_wsum, const bool a_full, const bool b_full,
-                                   ColorSet<C>& out)
+template <int C, typename S>
+NBPT_HD void merge_colors_with_sum(const SetView<C, S>& a, const SetView<C, S>& b, const S* a_sum, S a_wsum,
+                                   const S* b_sum, S b_wsum, const bool a_full, const bool b_full,
+                                   ColorSet<C, S>& out)
 {
         // samples_color_sum / samples_weight_sum (samples/merge.cpp:37-76)
-        float sum[C];
-        float wsum;
+        S sum[C];
+        S wsum;
         if (a_full && b_full)
         {
 #pragma unroll 8
@@ -215,7 +224,7 @@ NBPT_HD void merge_colors_with_sum(const SetView<C>& a, const SetView<C>& b, con
 
         const int a_size = a.count();
         const int b_size = b.count();
-        ColorSet<C> r;
+        ColorSet<C, S> r;
         if (a_size == HELD_OUT && b_size == HELD_OUT)
         {
                 int ai = 0;
@@ -330,12 +339,12 @@ NBPT_HD void merge_colors_with_sum(const SetView<C>& a, const SetView<C>& b, con
 }
 
 // Merge a fresh group into a pixel's colour set (samples/merge.cpp:198-223).
-template <int C>
-NBPT_HD void merge_color_group(ColorSet<C>& s, const ColorGroup<C>& g, const float* g_sum, const float g_wsum,
+template <int C, typename S>
+NBPT_HD void merge_color_group(ColorSet<C, S>& s, const ColorGroup<C>& g, const S* g_sum, const S g_wsum,
                                const bool g_full)
 {
-        const SetView<C> a{&s, nullptr, 0};
-        const SetView<C> b{nullptr, &g, g_full ? 1 : 0};
+        const SetView<C, S> a{&s, nullptr, 0};
+        const SetView<C, S> b{nullptr, &g, g_full ? 1 : 0};
         const int a_count = a.count();
         const int b_count = b.count();
         if (a_count + b_count > HELD_OUT)
@@ -350,7 +359,7 @@ NBPT_HD void merge_color_group(ColorSet<C>& s, const ColorGroup<C>& g, const flo
         if (a_count == 0)
         {
                 // the group as created, held-out entries and sums
-                ColorSet<C> r;
+                ColorSet<C, S> r;
                 for (int k = 0; k < b_count; ++k)
                 {
                         copy_entry(r, k, b, k);
@@ -358,16 +367,16 @@ NBPT_HD void merge_color_group(ColorSet<C>& s, const ColorGroup<C>& g, const flo
 #pragma unroll 8
                 for (int c = 0; c < C; ++c)
                 {
-                        r.color_sum[c] = g_full ? g_sum[c] : 0.0f;
+                        r.color_sum[c] = g_full ? g_sum[c] : S(0);
                 }
-                r.weight_sum = g_full ? g_wsum : 0.0f;
+                r.weight_sum = g_full ? g_wsum : S(0);
                 r.count = b_count;
                 r.full = g_full ? 1 : 0;
                 s = r;
                 return;
         }
         // merge (com/merge.h:235-271): sorted merge of two small sets
-        ColorSet<C> r;
+        ColorSet<C, S> r;
         int i = 0;
         int ai = 0;
         int bi = 0;
@@ -396,12 +405,13 @@ NBPT_HD void merge_color_group(ColorSet<C>& s, const ColorGroup<C>& g, const flo
 }
 
 // Background sets: the same merges on weights only.
-NBPT_HD void merge_background_group(BackgroundSet& s, const float* gw, const int n)
+template <typename S>
+NBPT_HD void merge_background_group(BackgroundSet<S>& s, const float* gw, const int n)
 {
         // gw: the group's weights, already ordered (order_group on values)
         const bool g_full = n > HELD_OUT;
         float held[HELD_OUT];
-        float g_sum = 0;
+        S g_sum = 0;
         int g_count = n;
         if (g_full)
         {
@@ -425,7 +435,7 @@ NBPT_HD void merge_background_group(BackgroundSet& s, const float* gw, const int
         const int a_count = s.full ? HELD_OUT : s.count;
         if (a_count + g_count > HELD_OUT)
         {
-                float wsum;
+                S wsum;
                 if (s.full && g_full)
                 {
                         wsum = s.weight_sum + g_sum;
@@ -540,7 +550,7 @@ NBPT_HD void merge_background_group(BackgroundSet& s, const float* gw, const int
                 {
                         s.weights[k] = held[k];
                 }
-                s.weight_sum = g_full ? g_sum : 0.0f;
+                s.weight_sum = g_full ? g_sum : S(0);
                 s.count = g_count;
                 s.full = g_full ? 1 : 0;
                 return;
@@ -585,7 +595,7 @@ struct Screen final
 
 // Merge one pass's samples of the 3^(n-1) neighbours into receiving pixel t
 // (global index).
-template <int N, typename T, int C>
+template <int N, typename T, int C, typename S>
 NBPT_HD void accumulate_pixel(
         const Screen<N>& screen,
         const long long t,
@@ -596,7 +606,7 @@ NBPT_HD void accumulate_pixel(
         const unsigned char* __restrict__ valid,
         const T alpha,
         const T exp_radius,
-        PixelState<C>& st)
+        PixelState<C, S>& st)
 {
         int tc[N - 1];
         {
@@ -682,8 +692,8 @@ NBPT_HD void accumulate_pixel(
                 {
                         order_group(color_order, nc, [&](const int i) { return contribution[i]; });
                         const ColorGroup<C> g{colors + (p - screen.source_first) * spp * C, w, contribution, color_order, nc, C, 1, 0};
-                        float g_sum[C];
-                        float g_wsum = 0;
+                        S g_sum[C];
+                        S g_wsum = 0;
 #pragma unroll 8
                         for (int c = 0; c < C; ++c)
                         {
@@ -725,7 +735,7 @@ NBPT_HD void accumulate_pixel(
 }
 
 // accumulation kernel: one thread per receiving pixel, no atomics
-template <int N, typename T, int C>
+template <int N, typename T, int C, typename S>
 __global__ void __launch_bounds__(128) accumulate_kernel(
         const Screen<N> screen,
         const long long pixel_count,
@@ -736,15 +746,15 @@ __global__ void __launch_bounds__(128) accumulate_kernel(
         const unsigned char* __restrict__ valid,
         const T alpha,
         const T exp_radius,
-        PixelState<C>* __restrict__ state)
+        PixelState<C, S>* __restrict__ state)
 {
         const long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
         if (t >= pixel_count)
         {
                 return;
         }
-        PixelState<C> st = state[t];
-        accumulate_pixel<N, T, C>(screen, screen.first + t, spp, points, colors, lum, valid, alpha, exp_radius, st);
+        PixelState<C, S> st = state[t];
+        accumulate_pixel<N, T, C, S>(screen, screen.first + t, spp, points, colors, lum, valid, alpha, exp_radius, st);
         state[t] = st;
 }
 
@@ -754,7 +764,7 @@ __global__ void __launch_bounds__(128) accumulate_kernel(
 // the same merge on the same scalars for its own channels (lane, lane + 32,
 // ...), so the merge decisions are the single-thread kernel's and each
 // channel's sums are formed in the same order.
-template <int N, typename T, int C>
+template <int N, typename T, int C, typename S>
 __global__ void __launch_bounds__(128) accumulate_warp_kernel(
         const Screen<N> screen,
         const long long pixel_count,
@@ -765,7 +775,7 @@ __global__ void __launch_bounds__(128) accumulate_warp_kernel(
         const unsigned char* __restrict__ valid,
         const T alpha,
         const T exp_radius,
-        PixelState<C>* __restrict__ state)
+        PixelState<C, S>* __restrict__ state)
 {
         static_assert(C % 32 == 0);
         constexpr int K = C / 32;
@@ -793,8 +803,8 @@ __global__ void __launch_bounds__(128) accumulate_warp_kernel(
         float* const sorted = s_sorted[warp];
 
         // this lane's channels of the pixel state, and its scalars
-        PixelState<C>& global = state[t];
-        ColorSet<K> cs;
+        PixelState<C, S>& global = state[t];
+        ColorSet<K, S> cs;
 #pragma unroll
         for (int k = 0; k < K; ++k)
         {
@@ -814,7 +824,7 @@ __global__ void __launch_bounds__(128) accumulate_warp_kernel(
         }
         cs.count = global.color.count;
         cs.full = global.color.full;
-        BackgroundSet bs = global.background;
+        BackgroundSet<S> bs = global.background;
 
         int tc[N - 1];
         {
@@ -930,8 +940,8 @@ __global__ void __launch_bounds__(128) accumulate_warp_kernel(
                 if (nc > 0)
                 {
                         const ColorGroup<K> g{colors + (p - screen.source_first) * spp * C, w, contribution, order, nc, C, 32, lane};
-                        float g_sum[K];
-                        float g_wsum = 0;
+                        S g_sum[K];
+                        S g_wsum = 0;
 #pragma unroll
                         for (int k = 0; k < K; ++k)
                         {
@@ -991,7 +1001,7 @@ __global__ void __launch_bounds__(128) accumulate_warp_kernel(
 // accumulate_warp_kernel merges them.
 inline constexpr int SMALL_GROUP = 32;
 
-template <int N, typename T, int C>
+template <int N, typename T, int C, typename S>
 __global__ void __launch_bounds__(128) accumulate_warp_small_kernel(
         const Screen<N> screen,
         const long long pixel_count,
@@ -1002,7 +1012,7 @@ __global__ void __launch_bounds__(128) accumulate_warp_small_kernel(
         const unsigned char* __restrict__ valid,
         const T alpha,
         const T exp_radius,
-        PixelState<C>* __restrict__ state)
+        PixelState<C, S>* __restrict__ state)
 {
         static_assert(C % 32 == 0);
         constexpr int K = C / 32;
@@ -1143,8 +1153,8 @@ __global__ void __launch_bounds__(128) accumulate_warp_small_kernel(
         __syncwarp();
 
         // this lane's channels of the pixel state, and its scalars
-        PixelState<C>& global = state[t];
-        ColorSet<K> cs;
+        PixelState<C, S>& global = state[t];
+        ColorSet<K, S> cs;
 #pragma unroll
         for (int k = 0; k < K; ++k)
         {
@@ -1164,7 +1174,7 @@ __global__ void __launch_bounds__(128) accumulate_warp_small_kernel(
         }
         cs.count = global.color.count;
         cs.full = global.color.full;
-        BackgroundSet bs = global.background;
+        BackgroundSet<S> bs = global.background;
 
         int* const order = s_order_int[warp];
         float* const sorted = s_sorted[warp];
@@ -1191,8 +1201,8 @@ __global__ void __launch_bounds__(128) accumulate_warp_small_kernel(
                 if (nc > 0)
                 {
                         const ColorGroup<K> g{colors + (p - screen.source_first) * spp * C, w, s_contribution[warp][nb], order, nc, C, 32, lane};
-                        float g_sum[K];
-                        float g_wsum = 0;
+                        S g_sum[K];
+                        S g_wsum = 0;
 #pragma unroll
                         for (int k = 0; k < K; ++k)
                         {
@@ -1249,22 +1259,22 @@ __global__ void __launch_bounds__(128) accumulate_warp_small_kernel(
 // and the RGB of the colour (src/color/color.h rgb32).  The background is
 // black: its colour and contribution are 0.
 
-template <int C>
+template <int C, typename S>
 struct Resolved final
 {
         bool has;
-        float color[C];
-        float color_weight;
-        float background_weight;
+        S color[C];
+        S color_weight;
+        S background_weight;
 };
 
-template <int C>
-NBPT_HD Resolved<C> resolve_pixel(const PixelState<C>& st)
+template <int C, typename S>
+NBPT_HD Resolved<C, S> resolve_pixel(const PixelState<C, S>& st)
 {
-        Resolved<C> res;
+        Resolved<C, S> res;
         res.has = false;
-        const ColorSet<C>& a = st.color;
-        const BackgroundSet& b = st.background;
+        const ColorSet<C, S>& a = st.color;
+        const BackgroundSet<S>& b = st.background;
         const int a_size = a.full ? HELD_OUT : a.count;
         const int b_size = b.full ? HELD_OUT : b.count;
         if (a_size + b_size <= HELD_OUT)
@@ -1287,10 +1297,10 @@ NBPT_HD Resolved<C> resolve_pixel(const PixelState<C>& st)
 #pragma unroll 8
         for (int c = 0; c < C; ++c)
         {
-                res.color[c] = a.full ? a.color_sum[c] : 0.0f;
+                res.color[c] = a.full ? a.color_sum[c] : S(0);
         }
-        res.color_weight = a.full ? a.weight_sum : 0.0f;
-        res.background_weight = b.full ? b.weight_sum : 0.0f;
+        res.color_weight = a.full ? a.weight_sum : S(0);
+        res.background_weight = b.full ? b.weight_sum : S(0);
 
         const auto a_key = [&](const int i)
         {
@@ -1422,21 +1432,23 @@ NBPT_HD Resolved<C> resolve_pixel(const PixelState<C>& st)
         return res;
 }
 
-// The pixel's RGB and premultiplied RGBA (pixel.h:51-88, color.h rgb32).
-template <int C>
-NBPT_HD void resolve_rgb(const PixelState<C>& state, const float* xyz, float* rgb, float* rgba)
+// The pixel's RGB and premultiplied RGBA (pixel.h:51-88, color.h rgb32); with
+// double sums the division by the weight is in double and the colour is then
+// rounded to float.
+template <int C, typename S>
+NBPT_HD void resolve_rgb(const PixelState<C, S>& state, const float* xyz, float* rgb, float* rgba)
 {
-        const Resolved<C> r = resolve_pixel(state);
+        const Resolved<C, S> r = resolve_pixel(state);
         float out[3] = {0.0f, 0.0f, 0.0f};
         float out_a[4] = {0.0f, 0.0f, 0.0f, 0.0f};
         if (r.has)
         {
-                const float sum = r.color_weight + r.background_weight;
+                const S sum = r.color_weight + r.background_weight;
                 float color[C];
 #pragma unroll 8
                 for (int c = 0; c < C; ++c)
                 {
-                        color[c] = r.color[c] / sum;
+                        color[c] = static_cast<float>(r.color[c] / sum);
                 }
                 float c_rgb[3];
                 if constexpr (C == 3)
@@ -1476,7 +1488,7 @@ NBPT_HD void resolve_rgb(const PixelState<C>& state, const float* xyz, float* rg
                         out_a[0] = c_rgb[0];
                         out_a[1] = c_rgb[1];
                         out_a[2] = c_rgb[2];
-                        out_a[3] = r.color_weight / sum;
+                        out_a[3] = static_cast<float>(r.color_weight / sum);
                 }
         }
         rgb[0] = out[0];
@@ -1491,10 +1503,10 @@ NBPT_HD void resolve_rgb(const PixelState<C>& state, const float* xyz, float* rg
         }
 }
 
-template <int C>
+template <int C, typename S>
 __global__ void resolve_kernel(
         const long long pixel_count,
-        const PixelState<C>* __restrict__ state,
+        const PixelState<C, S>* __restrict__ state,
         const float* __restrict__ xyz, // [3][64] colour matching functions (spectrum only)
         float* __restrict__ rgb,
         float* __restrict__ rgba)
@@ -1504,6 +1516,6 @@ __global__ void resolve_kernel(
         {
                 return;
         }
-        resolve_rgb<C>(state[t], xyz, rgb + t * 3, rgba ? rgba + t * 4 : nullptr);
+        resolve_rgb<C, S>(state[t], xyz, rgb + t * 3, rgba ? rgba + t * 4 : nullptr);
 }
 } // namespace nbpt

@@ -31,6 +31,11 @@ enum class Integrator : int
         PT = 1
 };
 
+// the type of a painter's per-pixel sums (create_painter's pixel_sums)
+inline constexpr int PIXEL_SUMS_DEFAULT = 0;
+inline constexpr int PIXEL_SUMS_FLOAT = 1;
+inline constexpr int PIXEL_SUMS_DOUBLE = 2;
+
 class Painter
 {
 public:
@@ -109,17 +114,21 @@ public:
         // slab_end >= 0: a painter of the rows [slab_begin, slab_end) of the
         // last screen axis only (its paths, those of the rows either side,
         // and the estimator of its own pixels); its images are the slab's
+        // pixel_sums: the type of the per-pixel radiance and weight sums,
+        // PIXEL_SUMS_FLOAT (the reference's), PIXEL_SUMS_DOUBLE, or
+        // PIXEL_SUMS_DEFAULT: float for a double-precision scene (its images
+        // are the reference's), double for a single-precision one
         virtual std::unique_ptr<Painter> create_painter(int samples_per_pixel, int max_depth, std::uint32_t seed,
                                                         Integrator integrator = Integrator::BPT, int slab_begin = 0,
                                                         int slab_end = -1, bool flat_shading = false,
-                                                        long long chunk_budget = 0) = 0;
+                                                        long long chunk_budget = 0, int pixel_sums = 0) = 0;
         // device bytes create_painter would allocate.  chunk_budget: bytes
         // for the buffers of one chunk of paths (0: a fifth of the device's
         // memory within [4, 32] GiB); the job server gives each of its slots
         // a share of its memory budget
         virtual long long painter_bytes(int samples_per_pixel, int max_depth,
                                         Integrator integrator = Integrator::BPT,
-                                        long long chunk_budget = 0) const = 0;
+                                        long long chunk_budget = 0, int pixel_sums = 0) const = 0;
 
         // verification: closest hit (any == 0) or any hit of rays [n][2N]
         virtual void trace(const double* rays, long long count, int any, int* kind, int* index, double* t,

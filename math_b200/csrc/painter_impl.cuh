@@ -2226,8 +2226,9 @@ public:
 
         std::unique_ptr<Painter> create_painter(int spp, int max_depth, std::uint32_t seed,
                                                 Integrator integrator, int slab_begin, int slab_end,
-                                                bool flat_shading, long long chunk_budget) override;
-        long long painter_bytes(int spp, int max_depth, Integrator integrator, long long chunk_budget) const override;
+                                                bool flat_shading, long long chunk_budget, int pixel_sums) override;
+        long long painter_bytes(int spp, int max_depth, Integrator integrator, long long chunk_budget,
+                                int pixel_sums) const override;
 
         void trace(const double* rays, long long count, int any, int* kind, int* index, double* t, double* point) override;
         void trace_device(const double* rays, long long count, int any, int* kind, int* index, double* t,
@@ -2444,7 +2445,9 @@ class PainterT final : public Painter
         DeviceArray<float> colors_;
         DeviceArray<float> lum_;
         DeviceArray<unsigned char> valid_;
-        DeviceArray<PixelState<C>> state_;
+        bool double_sums_ = false;
+        DeviceArray<PixelState<C, float>> state_;    // float sums
+        DeviceArray<PixelState<C, double>> state64_; // double sums
         DeviceArray<PathStats> stats_;
         DeviceArray<unsigned> cancel_; // nonzero: the passes take no more paths
         bool scratch_ready_ = false;   // the per-chunk path buffers are allocated
@@ -2530,13 +2533,26 @@ class PainterT final : public Painter
         }
 
 public:
+        static bool double_sums(const int pixel_sums)
+        {
+                if (pixel_sums != PIXEL_SUMS_DEFAULT && pixel_sums != PIXEL_SUMS_FLOAT &&
+                    pixel_sums != PIXEL_SUMS_DOUBLE)
+                {
+                        throw std::runtime_error("Unknown pixel sums " + std::to_string(pixel_sums));
+                }
+                return pixel_sums == PIXEL_SUMS_DOUBLE ||
+                       (pixel_sums == PIXEL_SUMS_DEFAULT && std::is_same_v<T, float>);
+        }
+
         // device bytes a painter of these parameters allocates
         static long long estimate_bytes(const long long pixels, const int spp, const int max_depth, const int strata,
-                                        const Integrator integrator, const long long budget = 0)
+                                        const Integrator integrator, const long long budget = 0,
+                                        const bool sums_in_double = false)
         {
                 const long long samples = pixels * spp;
                 const long long per_sample = (N - 1) * sizeof(T) + C * 4 + 4 + 1;
-                const long long per_pixel = sizeof(PixelState<C>) + 12 + 16;
+                const long long per_pixel =
+                        (sums_in_double ? sizeof(PixelState<C, double>) : sizeof(PixelState<C, float>)) + 12 + 16;
                 const long long chunk = integrator == Integrator::PT
                                                 ? 4 // the path counter; the direct-lighting records are small
                                                 : chunk_pixels(pixels, spp, max_depth, integrator, budget) * spp *
@@ -2551,9 +2567,10 @@ public:
         // slab's own pixels
         PainterT(const SceneT<N, T, C>* scene, const int spp, const int max_depth, const std::uint32_t seed,
                  const Integrator integrator, const int slab_begin = 0, const int slab_end = -1,
-                 const bool flat_shading = false, const long long chunk_budget = 0)
+                 const bool flat_shading = false, const long long chunk_budget = 0, const int pixel_sums = 0)
                 : scene_(scene),
                   flat_shading_(flat_shading),
+                  double_sums_(double_sums(pixel_sums)),
                   chunk_budget_(chunk_budget),
                   spp_request_(spp),
                   max_depth_(max_depth),
@@ -2624,7 +2641,14 @@ public:
                 colors_.allocate(samples * C);
                 lum_.allocate(samples);
                 valid_.allocate(samples);
-                state_.allocate(pixels_);
+                if (double_sums_)
+                {
+                        state64_.allocate(pixels_);
+                }
+                else
+                {
+                        state_.allocate(pixels_);
+                }
                 stats_.allocate(1);
                 NBPT_CUDA(cudaMemsetAsync(stats_.get(), 0, sizeof(PathStats), stream_));
                 cancel_.allocate(1);
@@ -2658,7 +2682,14 @@ public:
                 NBPT_CUDA(cudaEventCreate(&ev_paths_));
                 NBPT_CUDA(cudaEventCreate(&ev_paths_end_));
                 NBPT_CUDA(cudaEventCreate(&ev_end_));
-                NBPT_CUDA(cudaMemsetAsync(state_.get(), 0, state_.bytes(), stream_));
+                if (double_sums_)
+                {
+                        NBPT_CUDA(cudaMemsetAsync(state64_.get(), 0, state64_.bytes(), stream_));
+                }
+                else
+                {
+                        NBPT_CUDA(cudaMemsetAsync(state_.get(), 0, state_.bytes(), stream_));
+                }
                 statistics_.pixel_count = pixels_;
         }
 
@@ -2686,7 +2717,8 @@ public:
         long long device_bytes() const override
         {
                 const std::size_t own = offsets_.bytes() + points_.bytes() + colors_.bytes() + lum_.bytes() +
-                                        valid_.bytes() + state_.bytes() + stats_.bytes() + rgb_.bytes() +
+                                        valid_.bytes() + state_.bytes() + state64_.bytes() + stats_.bytes() +
+                                        rgb_.bytes() +
                                         rgba_.bytes() + vertices_.bytes() + rng_.bytes() + tape_.bytes() +
                                         tasks_.bytes() + task_count_.bytes() + arrivals_.bytes() +
                                         next_path_.bytes() + pt_estimates_.bytes();
@@ -2846,33 +2878,13 @@ public:
                         const T width = radius / T(2.5);
                         const T alpha = -1 / (2 * width * width);
                         const T exp_radius = std::exp(alpha * radius * radius);
-                        if constexpr (C % 32 == 0 && N <= 4)
+                        if (double_sums_)
                         {
-                                if (spp_ <= SMALL_GROUP)
-                                {
-                                        accumulate_warp_small_kernel<N, T, C>
-                                                <<<blocks_for(pixels_ * 32, 128), 128, 0, stream_>>>(
-                                                        screen, pixels_, spp_, points_.get(), colors_.get(), lum_.get(),
-                                                        valid_.get(), alpha, exp_radius, state_.get());
-                                }
-                                else
-                                {
-                                        accumulate_warp_kernel<N, T, C><<<blocks_for(pixels_ * 32, 128), 128, 0, stream_>>>(
-                                                screen, pixels_, spp_, points_.get(), colors_.get(), lum_.get(),
-                                                valid_.get(), alpha, exp_radius, state_.get());
-                                }
-                        }
-                        else if constexpr (C % 32 == 0)
-                        {
-                                accumulate_warp_kernel<N, T, C><<<blocks_for(pixels_ * 32, 128), 128, 0, stream_>>>(
-                                        screen, pixels_, spp_, points_.get(), colors_.get(), lum_.get(), valid_.get(),
-                                        alpha, exp_radius, state_.get());
+                                accumulate(screen, alpha, exp_radius, state64_.get());
                         }
                         else
                         {
-                                accumulate_kernel<N, T, C><<<blocks_for(pixels_, 128), 128, 0, stream_>>>(
-                                        screen, pixels_, spp_, points_.get(), colors_.get(), lum_.get(), valid_.get(),
-                                        alpha, exp_radius, state_.get());
+                                accumulate(screen, alpha, exp_radius, state_.get());
                         }
                         NBPT_CUDA(cudaGetLastError());
                         NBPT_CUDA(cudaEventRecord(ev_end_, stream_));
@@ -2913,10 +2925,55 @@ public:
                 }
         }
 
+        template <typename S>
+        void accumulate(const Screen<N>& screen, const T alpha, const T exp_radius, PixelState<C, S>* const state)
+        {
+                if constexpr (C % 32 == 0 && N <= 4)
+                {
+                        if (spp_ <= SMALL_GROUP)
+                        {
+                                accumulate_warp_small_kernel<N, T, C, S><<<blocks_for(pixels_ * 32, 128), 128, 0, stream_>>>(
+                                        screen, pixels_, spp_, points_.get(), colors_.get(), lum_.get(), valid_.get(),
+                                        alpha, exp_radius, state);
+                        }
+                        else
+                        {
+                                accumulate_warp_kernel<N, T, C, S><<<blocks_for(pixels_ * 32, 128), 128, 0, stream_>>>(
+                                        screen, pixels_, spp_, points_.get(), colors_.get(), lum_.get(), valid_.get(),
+                                        alpha, exp_radius, state);
+                        }
+                }
+                else if constexpr (C % 32 == 0)
+                {
+                        accumulate_warp_kernel<N, T, C, S><<<blocks_for(pixels_ * 32, 128), 128, 0, stream_>>>(
+                                screen, pixels_, spp_, points_.get(), colors_.get(), lum_.get(), valid_.get(), alpha,
+                                exp_radius, state);
+                }
+                else
+                {
+                        accumulate_kernel<N, T, C, S><<<blocks_for(pixels_, 128), 128, 0, stream_>>>(
+                                screen, pixels_, spp_, points_.get(), colors_.get(), lum_.get(), valid_.get(), alpha,
+                                exp_radius, state);
+                }
+        }
+
+        void resolve()
+        {
+                if (double_sums_)
+                {
+                        resolve_kernel<C, double><<<blocks_for(pixels_, 128), 128, 0, stream_>>>(
+                                pixels_, state64_.get(), scene_->cie(), rgb_.get(), rgba_.get());
+                }
+                else
+                {
+                        resolve_kernel<C, float><<<blocks_for(pixels_, 128), 128, 0, stream_>>>(
+                                pixels_, state_.get(), scene_->cie(), rgb_.get(), rgba_.get());
+                }
+        }
+
         void images(float* rgb, float* rgba) override
         {
-                resolve_kernel<C><<<blocks_for(pixels_, 128), 128, 0, stream_>>>(
-                        pixels_, state_.get(), scene_->cie(), rgb_.get(), rgba_.get());
+                resolve();
                 NBPT_CUDA(cudaGetLastError());
                 NBPT_CUDA(cudaStreamSynchronize(stream_));
                 if (rgb)
@@ -2931,8 +2988,7 @@ public:
 
         void enqueue_images(float* rgb, float* rgba) override
         {
-                resolve_kernel<C><<<blocks_for(pixels_, 128), 128, 0, stream_>>>(
-                        pixels_, state_.get(), scene_->cie(), rgb_.get(), rgba_.get());
+                resolve();
                 NBPT_CUDA(cudaGetLastError());
                 if (rgb)
                 {
@@ -2989,22 +3045,23 @@ std::unique_ptr<Painter> SceneT<N, T, C>::create_painter(
         const int slab_begin,
         const int slab_end,
         const bool flat_shading,
-        const long long chunk_budget)
+        const long long chunk_budget,
+        const int pixel_sums)
 {
         return std::make_unique<PainterT<N, T, C>>(this, spp, max_depth, seed, integrator, slab_begin, slab_end,
-                                                   flat_shading, chunk_budget);
+                                                   flat_shading, chunk_budget, pixel_sums);
 }
 
 template <int N, typename T, int C>
 long long SceneT<N, T, C>::painter_bytes(const int spp, const int max_depth, const Integrator integrator,
-                                         const long long chunk_budget) const
+                                         const long long chunk_budget, const int pixel_sums) const
 {
         if (spp < 1 || (integrator == Integrator::BPT && max_depth < 1))
         {
                 throw std::runtime_error("painter samples per pixel and maximum depth must be positive");
         }
         return PainterT<N, T, C>::estimate_bytes(pixel_count(), actual_spp(spp), max_depth, strata(spp), integrator,
-                                                 chunk_budget);
+                                                 chunk_budget, PainterT<N, T, C>::double_sums(pixel_sums));
 }
 
 template <int N, typename T, int C>

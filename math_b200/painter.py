@@ -57,6 +57,7 @@ class PainterOptions(ctypes.Structure):
         ("flat_shading", ctypes.c_int),
         ("slab_begin", ctypes.c_int),
         ("slab_end", ctypes.c_int),
+        ("pixel_sums", ctypes.c_int),
     ]
 
 
@@ -317,10 +318,11 @@ class Scene:
 
     def painter(self, samples_per_pixel: int, max_depth: int, seed: int = 1,
                 integrator: str = "bpt", slab: tuple[int, int] | None = None,
-                flat_shading: bool = False) -> "Painter":
+                flat_shading: bool = False, pixel_sums: str | None = None) -> "Painter":
         """slab: rows [begin, end) of the last screen axis (nbpt_painter_create_slab);
-        flat_shading: create_painter's flat_shading"""
-        return Painter(self, samples_per_pixel, max_depth, seed, integrator, slab, flat_shading)
+        flat_shading: create_painter's flat_shading; pixel_sums: "float",
+        "double" or None (float for a double-precision scene, else double)"""
+        return Painter(self, samples_per_pixel, max_depth, seed, integrator, slab, flat_shading, pixel_sums)
 
     def trace(self, rays: np.ndarray, any_hit: bool = False):
         rays = _d(rays).reshape(-1, 2 * self.n)
@@ -379,6 +381,9 @@ class Scene:
 
 # painter::Integrator (src/painter/painter.h:143-147)
 INTEGRATORS = {"bpt": 0, "pt": 1}
+# NBPT_PIXEL_SUMS_*: the type of the estimator's per-pixel sums; None is the
+# default (float for a double-precision scene, double for a single-precision one)
+PIXEL_SUMS = {None: 0, "float": 1, "double": 2}
 
 PASS_CALLBACK = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_float),
                                  ctypes.POINTER(ctypes.c_float), ctypes.c_longlong)
@@ -391,15 +396,18 @@ class Painter:
     tracing with next-event estimation; max_depth is not used)."""
 
     def __init__(self, scene: Scene, samples_per_pixel: int, max_depth: int, seed: int = 1,
-                 integrator: str = "bpt", slab: tuple[int, int] | None = None, flat_shading: bool = False):
+                 integrator: str = "bpt", slab: tuple[int, int] | None = None, flat_shading: bool = False,
+                 pixel_sums: str | None = None):
         if integrator not in INTEGRATORS:
             raise PainterError(f"Unknown integrator {integrator!r}")
+        if pixel_sums not in PIXEL_SUMS:
+            raise PainterError(f"Unknown pixel sums {pixel_sums!r}")
         self.scene = scene
         self.integrator = integrator
         self.spp = scene.actual_spp(samples_per_pixel)
         begin, end = slab if slab is not None else (0, -1)
         options = PainterOptions(INTEGRATORS[integrator], samples_per_pixel, max_depth, seed,
-                                 1 if flat_shading else 0, begin, end)
+                                 1 if flat_shading else 0, begin, end, PIXEL_SUMS[pixel_sums])
         self.h = lib().nbpt_painter_create_options(scene.h, ctypes.byref(options))
         if not self.h:
             raise PainterError(lib().nbpt_last_error().decode())

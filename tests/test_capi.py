@@ -23,6 +23,20 @@ def test_header_declares_the_binding_signatures():
     assert names == bound
 
 
+@pytest.mark.parametrize("c_name, mirror", [("nbpt_painter_options", painter.PainterOptions),
+                                             ("nbpt_statistics", painter.Statistics),
+                                             ("nbpt_job_info", painter.JobInfo)])
+def test_header_structs_match_the_binding(c_name, mirror):
+    """Every field of the header's struct, in order, in the ctypes mirror."""
+    text = (ROOT / "include" / "nbpt.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    body = re.search(r"typedef struct %s\s*\{(.*?)\}\s*%s;" % (c_name, c_name), text, re.S)
+    assert body, c_name
+    fields = [re.findall(r"(\w+)\s*(?:\[\d+\])?\s*;", line)[0]
+              for line in body.group(1).split("\n") if ";" in line]
+    assert fields == [f[0] for f in mirror._fields_]
+
+
 def test_library_exports_every_declared_symbol():
     lib = ctypes.CDLL(str(painter.LIB_PATH))
     for name in declared_functions():

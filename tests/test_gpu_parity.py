@@ -224,9 +224,9 @@ def test_own_ingestion_paths(painter, oracle_lib, name):
 
 def test_float_path_rmse_against_double_reference(painter, oracle_lib):
     """Single precision (traversal, intersection, BRDF and MIS in float;
-    facet set-up in double; colours and pixel sums in float, as the
-    reference's Color is float in both instantiations) against the double-precision
-    reference image of the same scene: relative RMSE within 1%."""
+    facet set-up and the per-pixel radiance sums in double) against the
+    double-precision reference image of the same scene: relative RMSE
+    within 1%."""
     desc = scenes.cornell_3d(size=(32, 32), subdivisions=3)
     o = oracle_lib.Scene(desc, "double", False)
     ref, _ = o.render_image(64, 5, seed=7, passes=4)
