@@ -645,6 +645,41 @@ def batch_step(server, built: list, jobs: list[dict], seed: int = 1, read_images
     return totals
 
 
+def batch_steps(server, wave_scenes: list, waves: list, steps: int, seed: int = 1,
+                read_images: bool = True) -> dict:
+    """`steps` steps of the batch submitted back to back: step k renders
+    wave k mod len(waves) (each job one pass at its own samples per pixel);
+    all the steps' renders are queued in the job server at once, which
+    admits them as slots and memory free up (continuous batching, no drain
+    between steps).  `span` is the device time from the first job's first
+    kernel to the last job's last (CUDA events on the jobs' streams);
+    `images` holds each job's image of its last step."""
+    work = [(s, j) for k in range(steps) for s, j in zip(wave_scenes[k % len(waves)], waves[k % len(waves)])]
+    ids = [server.submit_render(s, j["spp"], j["max_depth"], seed=seed, passes=1) for s, j in work]
+    first, last = [], []
+    totals = {"paths": 0, "launches": 0, "bytes": 0.0, "rays": 0, "nodes": 0, "facets": 0, "nonfinite": 0}
+    images = {}
+    for (s, j), i in zip(work, ids):
+        info = server.wait(i)
+        st = server.statistics(i)
+        first.append(info["device_started"])
+        last.append(info["device_finished"])
+        size = record_bytes(s.n, s.precision)
+        totals["paths"] += st["sample_count"]
+        totals["launches"] += st["kernel_launches"] + 1  # + the images' resolve kernel
+        totals["bytes"] += st["nodes"] * size["node"] + st["facets"] * size["facet"] + st["shapes"] * size["shape"]
+        totals["rays"] += st["ray_count"]
+        totals["nodes"] += st["nodes"]
+        totals["facets"] += st["facets"]
+        totals["nonfinite"] += st["nonfinite_samples"]
+        if read_images:
+            images[j["index"]] = server.images(i, s.pixels)[0]
+        server.release(i)
+    totals["span"] = max(last) - min(first) if work else 0.0
+    totals["images"] = images
+    return totals
+
+
 def e2e_step(server, jobs: list[dict], precision: str, builders: int = 4) -> dict:
     """One step of the batch end to end through the public API: every
     scene built from host arrays (nbpt_scene_* on `builders` host threads,
@@ -755,36 +790,21 @@ def run_batch(args, rank: int, world: int, local: int):
 
     server = P.Server(max_jobs=args.max_jobs)
     try:
-        for k in range(args.warmup):
-            flush_l2(flush)
-            w = k % len(waves)
-            batch_step(server, wave_scenes[w], waves[w], read_images=False)
+        batch_steps(server, wave_scenes, waves, args.warmup, read_images=False)
+        flush_l2(flush)
+        torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
         clocks = ClockSampler(local)
         clocks.start()
-        spans = [[] for _ in waves]
-        totals = {"launches": 0, "bytes": 0.0, "rays": 0, "nodes": 0, "facets": 0, "nonfinite": 0, "paths": 0}
-        images = {}
-        for k in range(args.steps):
-            flush_l2(flush)
-            w = k % len(waves)
-            r = batch_step(server, wave_scenes[w], waves[w])
-            spans[w].append(r["span"])
-            for key in totals:
-                totals[key] += r[key]
-            for j, img in zip(waves[w], r["images"]):
-                images[j["index"]] = img
+        totals = batch_steps(server, wave_scenes, waves, args.steps)
         clock_info = clocks.stop()
         torch.cuda.synchronize()
-        step_seconds = float(sum(sum(x) for x in spans))
-        if all(spans):
-            # every wave timed: the batch's rate from each wave's mean span
-            # (the plain sum when the steps cover whole batches)
-            batch_seconds = sum(float(np.mean(x)) for x in spans)
-            rank_rate = paths_per_batch / batch_seconds
-        else:
-            rank_rate = totals["paths"] / step_seconds
+        if world > 1:
+            torch.distributed.barrier()
+        images = totals["images"]
+        step_seconds = float(totals["span"])
+        rank_rate = totals["paths"] / step_seconds
         # whole batch over the slowest rank: every rank renders its jobs
         batch_seconds = slowest_rank(paths_per_batch / rank_rate, world, "cuda")
         value = sum(all_paths) / batch_seconds
@@ -835,13 +855,16 @@ def run_batch(args, rank: int, world: int, local: int):
                        "waves": len(waves), "wave_paths": wave_paths,
                        "step": (f"one wave: {len(jobs) // len(waves)} of the batch's jobs (the batch split into "
                                 f"{len(waves)} waves of about equal paths), one pass each at its own samples "
-                                "per pixel, all submitted to the job server at once, images read back; value = "
-                                "paths of the whole batch / the sum of the waves' mean device spans"),
+                                "per pixel, images read back; the steps are submitted back to back, all queued in "
+                                "the job server at once (continuous batching: no drain between steps); value = "
+                                "paths of the timed steps / their device span"),
                        "max_jobs": args.max_jobs, "points_scale": args.points_scale,
                        "screen_scale": args.screen_scale, "generate_s": generate_s, "scene_build_s": build_s,
-                       "l2": "flushed (256 MiB write) before every step; scenes and buffers exceed L2",
-                       "timing": "device span per step: CUDA events on the jobs' streams, from the first kernel of "
-                                 "the wave's first job to the last kernel of its last job"},
+                       "l2": "flushed (256 MiB write) before the timed steps; the steps' scenes (64 meshes of up "
+                             "to 1.5 M facets) and path buffers exceed L2 many times over",
+                       "timing": "device span of the timed steps: CUDA events on the jobs' streams, from the first "
+                                 "kernel of the first step's first job to the last kernel of the last job; "
+                                 "ms_per_step = span / steps"},
             "plain_fp64": plain,
             "speedup_vs_plain_fp64": (value / plain["value"]) if plain else None,
             "e2e": {"value": e2e_value, "unit": "paths/s",
