@@ -9,10 +9,13 @@ convex hull of N points on the unit (n-1)-sphere (N log-uniform in
 5-8, RGB.  Inputs are synthetic, generated from fixed seeds
 (math_b200/scenes.py).
 
-One step is one pass of every job (770 M paths) through the job server in
-FP32, all jobs submitted at once.  `value` is paths/s over the timed steps
-on the device (CUDA events on the jobs' streams, first kernel to last, L2
-flushed between steps); `plain_fp64` the same jobs in FP64 one at a time;
+One step is one wave, a quarter of the batch's jobs (about 192 M of its
+770 M paths), one pass each through the job server in FP32; the steps are
+submitted back to back (continuous batching).  Before the warm-up the
+server's chunk budget is chosen by measurement (math_b200.tuning).  `value`
+is paths/s over the timed steps on the device (CUDA events on the jobs'
+streams, first kernel to last, L2 flushed before them); `plain_fp64` the
+same jobs in FP64 one at a time;
 `e2e` the whole batch through the C ABI from host arrays (scene builds,
 copies, images back); `serve` a Poisson stream of renders into the server
 with its p50/p99 latency.  `--impl reference` runs the reference's own CPU
@@ -88,6 +91,9 @@ def parse():
     p.add_argument("--max-jobs", type=int, default=16, help="batch/serve: jobs the server runs at once")
     p.add_argument("--waves", type=int, default=4,
                    help="batch: the batch is split into this many waves of about equal paths; a step is one wave")
+    p.add_argument("--no-tune", action="store_true",
+                   help="batch: keep the server's default chunk budget instead of choosing it by measurement "
+                        "(math_b200.tuning, one batch per candidate, before the warm-up)")
     p.add_argument("--e2e-steps", type=int, default=0,
                    help="batch: steps (waves) of the end-to-end measurement (0: one whole batch)")
     p.add_argument("--serve-duration", type=float, default=20.0,
@@ -790,6 +796,18 @@ def run_batch(args, rank: int, world: int, local: int):
 
     server = P.Server(max_jobs=args.max_jobs)
     try:
+        tuning = None
+        if not args.no_tune:
+            from math_b200 import tuning as T
+
+            def one_batch():
+                r = batch_steps(server, wave_scenes, waves, len(waves), read_images=False)
+                return r["paths"], r["span"]
+
+            # a first batch at the default allocates the scenes' buffers
+            one_batch()
+            tuning = T.tune_chunk_budget(server, one_batch, T.chunk_budget_candidates(server))
+        server_chunk_budget = server.chunk_budget
         batch_steps(server, wave_scenes, waves, args.warmup, read_images=False)
         flush_l2(flush)
         torch.cuda.synchronize()
@@ -858,7 +876,15 @@ def run_batch(args, rank: int, world: int, local: int):
                                 "per pixel, images read back; the steps are submitted back to back, all queued in "
                                 "the job server at once (continuous batching: no drain between steps); value = "
                                 "paths of the timed steps / their device span"),
-                       "max_jobs": args.max_jobs, "points_scale": args.points_scale,
+                       "max_jobs": args.max_jobs,
+                       "chunk_budget": server_chunk_budget,
+                       "tuning": tuning and {
+                           "what": "the job server's chunk budget per render, chosen before the warm-up by "
+                                   "math_b200.tuning: one batch per candidate, the fastest kept",
+                           "chosen_gib": tuning["chosen"] / 2**30,
+                           "trials": [{"chunk_budget_gib": t["chunk_budget"] / 2**30,
+                                       "paths_per_s": t["paths_per_s"]} for t in tuning["trials"]]},
+                       "points_scale": args.points_scale,
                        "screen_scale": args.screen_scale, "generate_s": generate_s, "scene_build_s": build_s,
                        "l2": "flushed (256 MiB write) before the timed steps; the steps' scenes (64 meshes of up "
                              "to 1.5 M facets) and path buffers exceed L2 many times over",

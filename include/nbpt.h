@@ -343,6 +343,18 @@ int nbpt_server_statistics(nbpt_server* server, long long job, nbpt_statistics* 
  * it; until then a done render keeps its device memory */
 int nbpt_server_release(nbpt_server* server, long long job);
 int nbpt_server_job(nbpt_server* server, long long job, nbpt_job_info* info);
+/* Device bytes of per-chunk path buffers for each render the server creates
+ * from now on (renders already submitted keep theirs); 0 restores the
+ * default, an equal share of the memory budget per job slot and at least
+ * 4 GiB.  A pass's paths run in chunks of as many paths as these buffers
+ * hold, and each chunk ends in a tail where the persistent path kernels run
+ * out of paths; larger chunks shorten the tails, while fewer renders fit in
+ * the memory budget at once.  math_b200.tuning picks it by measurement.
+ * No reference counterpart: the reference's painter keeps one path per
+ * thread (src/painter/painting/painting.cpp:181-206). */
+int nbpt_server_set_chunk_budget(nbpt_server* server, long long bytes);
+/* the chunk budget of the renders submitted next (bytes), -1 on error */
+long long nbpt_server_chunk_budget(const nbpt_server* server);
 /* blocks until the job is done or failed; NBPT_ERROR (with the message) if it failed */
 int nbpt_server_wait(nbpt_server* server, long long job, nbpt_job_info* info);
 /* seconds since the server started, on the clock of nbpt_job_info */

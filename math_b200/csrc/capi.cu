@@ -986,6 +986,28 @@ int nbpt_server_cancel(nbpt_server* server, const long long job)
                 });
 }
 
+int nbpt_server_set_chunk_budget(nbpt_server* server, const long long bytes)
+{
+        return guarded(
+                [&]
+                {
+                        server_of(server).set_chunk_budget(bytes);
+                        return 0;
+                });
+}
+
+long long nbpt_server_chunk_budget(const nbpt_server* server)
+{
+        long long out = -1;
+        guarded(
+                [&]
+                {
+                        out = server_of(const_cast<nbpt_server*>(server)).chunk_budget();
+                        return 0;
+                });
+        return out;
+}
+
 int nbpt_test_server_hold(nbpt_server* server, const int hold)
 {
         return guarded(

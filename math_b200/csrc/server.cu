@@ -54,6 +54,7 @@ struct Server::Job final
         int spp = 0;
         int max_depth = 0;
         std::uint32_t seed = 0;
+        long long chunk_budget = 0; // the server's chunk budget when the render was submitted
         std::unique_ptr<Painter> owned;
         int device;
         JobInfo info;
@@ -210,8 +211,12 @@ long long Server::submit_render(Scene* const scene, const int spp, const int max
         job->info.state = JobState::QUEUED;
         job->info.passes = passes;
         job->info.passes_done = 0;
+        {
+                const std::lock_guard lock(mutex_);
+                job->chunk_budget = slot_chunk_budget();
+        }
         job->info.footprint =
-                scene->painter_bytes(spp, max_depth, Integrator::BPT, slot_chunk_budget()) + scene->device_bytes();
+                scene->painter_bytes(spp, max_depth, Integrator::BPT, job->chunk_budget) + scene->device_bytes();
         job->info.submitted = now();
         job->info.started = -1;
         job->info.finished = -1;
@@ -426,7 +431,27 @@ void Server::fail_next_creations(const int count)
 // cost less here than in a render alone.
 long long Server::slot_chunk_budget() const
 {
+        if (chunk_budget_ > 0)
+        {
+                return chunk_budget_;
+        }
         return std::max(4LL << 30, initial_budget_ / std::max(1, max_jobs_));
+}
+
+void Server::set_chunk_budget(const long long bytes)
+{
+        if (bytes < 0)
+        {
+                throw std::runtime_error("chunk budget " + std::to_string(bytes) + " is negative");
+        }
+        const std::lock_guard lock(mutex_);
+        chunk_budget_ = bytes;
+}
+
+long long Server::chunk_budget() const
+{
+        const std::lock_guard lock(mutex_);
+        return slot_chunk_budget();
 }
 
 void Server::hold_admission(const bool hold)
@@ -507,7 +532,7 @@ void Server::run()
                                                 }
                                                 j->owned = j->scene->create_painter(j->spp, j->max_depth, j->seed,
                                                                                     Integrator::BPT, 0, -1, false,
-                                                                                    slot_chunk_budget());
+                                                                                    j->chunk_budget);
                                         }
                                         catch (const CudaError& e)
                                         {

@@ -81,6 +81,13 @@ public:
         void fail_next_creations(int count);
         // test hook: while held, the server admits no job
         void hold_admission(bool hold);
+        // device bytes of chunk buffers (the per-chunk path buffers of the
+        // BPT kernels) of each render the server creates from now on; 0: an
+        // equal share of the memory budget per slot, at least 4 GiB.  Larger
+        // chunks leave less of each pass to the persistent kernels' tails;
+        // fewer renders then fit in the budget at once.
+        void set_chunk_budget(long long bytes);
+        long long chunk_budget() const;
         double now() const;
         // finishes the running jobs, fails the queued ones and stops the
         // worker; the destructor calls it, and so does process exit for a
@@ -110,6 +117,7 @@ private:
         bool stop_ = false;
         int fail_creations_ = 0;
         bool hold_ = false;
+        long long chunk_budget_ = 0; // set_chunk_budget
         void* reference_event_ = nullptr; // cudaEvent_t recorded at construction
         std::thread worker_;
 };

@@ -135,6 +135,8 @@ SIGNATURES = [
     ("nbpt_server_wait", ctypes.c_int, [_P, ctypes.c_longlong, ctypes.POINTER(JobInfo)]),
     ("nbpt_server_time", ctypes.c_double, [_P]),
     ("nbpt_server_cancel", ctypes.c_int, [_P, ctypes.c_longlong]),
+    ("nbpt_server_set_chunk_budget", ctypes.c_int, [_P, ctypes.c_longlong]),
+    ("nbpt_server_chunk_budget", ctypes.c_longlong, [_P]),
     ("nbpt_scene_trace", ctypes.c_int, [_P, _D, ctypes.c_longlong, ctypes.c_int, _I, _I, _D, _D]),
     ("nbpt_scene_trace_noalloc", ctypes.c_int, [_P, _D, ctypes.c_longlong, ctypes.c_int, _I, _I, _D, _D]),
     ("nbpt_scene_mesh_export", ctypes.c_int, [_P, ctypes.c_int, _L, _D, _D, _D, _U, _U, _I]),
@@ -569,6 +571,14 @@ class Server:
 
     def cancel(self, job: int):
         _check(lib().nbpt_server_cancel(self.h, job))
+
+    def set_chunk_budget(self, nbytes: int):
+        """Chunk-buffer bytes of the renders submitted from now on (0: the default share per slot)."""
+        _check(lib().nbpt_server_set_chunk_budget(self.h, int(nbytes)))
+
+    @property
+    def chunk_budget(self) -> int:
+        return _check(lib().nbpt_server_chunk_budget(self.h))
 
     def try_wait(self, job: int) -> dict:
         """wait() that returns the failed job's info (with "error") instead of raising."""

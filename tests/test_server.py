@@ -94,3 +94,38 @@ def test_server_created_renders_match_renders_alone(painter):
     server.close()
     for s in built:
         s.close()
+
+
+@pytest.mark.gpu
+def test_chunk_budget_changes_no_image(painter):
+    """Renders the server creates with a small chunk budget (many chunks per
+    pass) equal those with the default, bit for bit: every path's stream,
+    tape and strategies are its own, so chunk boundaries change nothing."""
+    jobs = scenes.mixed_batch(3, seed=11, points_scale=0.02, screen_scale=0.1)
+    built = [P.Scene(j["desc"], "float", False) for j in jobs]
+    server = P.Server(max_jobs=3)
+    default = server.chunk_budget
+    assert default >= 4 << 30
+    images = {}
+    launches = {}
+    for budget in (0, 8 << 20):
+        server.set_chunk_budget(budget)
+        assert server.chunk_budget == (budget or default)
+        ids = [server.submit_render(s, j["spp"], j["max_depth"], seed=5, passes=2) for s, j in zip(built, jobs)]
+        out = []
+        for s, i in zip(built, ids):
+            assert server.wait(i)["state"] == 2
+            out.append(server.images(i, s.pixels))
+            launches.setdefault(budget, []).append(server.statistics(i)["kernel_launches"])
+            server.release(i)
+        images[budget] = out
+    # 8 MiB of chunk buffers hold fewer paths than a pass of the larger jobs
+    assert any(b > a for a, b in zip(launches[0], launches[8 << 20]))
+    for a, b in zip(images[0], images[8 << 20]):
+        assert np.array_equal(a[0], b[0])
+        assert np.array_equal(a[1], b[1])
+    with pytest.raises(P.PainterError, match="negative"):
+        server.set_chunk_budget(-1)
+    server.close()
+    for s in built:
+        s.close()
