@@ -51,7 +51,7 @@ WORKLOADS = {
     "cornell3d": {"screen": [256, 256], "spp": 16, "max_depth": 5, "spectrum": False, "precision": "double",
                   "label": "3-space Cornell box, icosphere of 20480 triangles, RGB"},
     "sphere4d": {"screen": [96, 96, 96], "spp": 8, "max_depth": 8, "spectrum": False, "precision": "float",
-                 "label": "4-space hull of 150000 noisy points on S^3 (about 1M facets), ball light, "
+                 "label": "4-space hull of 150000 noisy points on S^3 (321,175 facets), ball light, "
                           "parallel projection, RGB"},
     "mixed5d": {"screen": [12, 12, 12, 12], "spp": 16, "max_depth": 8, "spectrum": False, "precision": "float",
                 "label": "a 5-space job of the mixed batch's shape: box, ceiling light, hull of 24000 points on S^4 "

@@ -99,18 +99,45 @@ def sphere_points(n: int, count: int, seed: int, noise: float = 0.0) -> np.ndarr
     return p.astype(np.float32)
 
 
-def convex_hull_mesh(points: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
-    """Boundary facets ((n-1)-simplices) of the convex hull of `points`.
+def hull_integer_points(points: np.ndarray) -> np.ndarray:
+    """The integer points the reference's convex hull works on
+    (src/geometry/core/convex_hull/source_points.h:40-100): float points
+    shifted by their per-axis minimum and scaled so the largest extent is
+    2^30 - 1, the product taken in double and rounded to the nearest integer
+    (halves away from zero).  Returned as float64 (exact: 30 bits)."""
+    p = np.asarray(points, dtype=np.float32)
+    lo = p.min(axis=0)
+    hi = p.max(axis=0)
+    extent = float(np.max(np.abs(hi - lo)))  # float subtraction, as the reference's Vector<N, float>
+    if not extent != 0:
+        raise ValueError("no distinct points")
+    scale = float((1 << 30) - 1) / extent
+    x = (p - lo).astype(np.float64) * scale  # float difference, double product
+    r = np.floor(x)
+    return r + (x - r >= 0.5)
 
-    The hull of points in general position is unique, so this is the same
-    facet set the reference's own hull (src/geometry/core/convex_hull.h)
-    produces; the vertex order inside a facet does not matter to the painter,
-    which orients normals towards the ray.
-    """
+
+def convex_hull_mesh(points: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """Boundary facets ((n-1)-simplices) of the convex hull of `points`,
+    the facet set of the reference's compute_convex_hull
+    (src/geometry/core/convex_hull.h:95-98).
+
+    The reference computes the hull exactly on the points rounded to a
+    30-bit integer grid (hull_integer_points), keeping the first of points
+    that round to the same integer point.  Qhull on those integer points
+    finds the same facets: a double-precision hull of the unrounded points
+    differs from it by a few facets wherever nearly coplanar points are
+    split the other way by the rounding (tests/test_hull.py checks the
+    3- and 4-space hulls against the reference's own).  Facet vertices are
+    indices into `points`; the vertex order inside a facet does not matter
+    to the painter, which orients normals towards the ray."""
     from scipy.spatial import ConvexHull
 
-    hull = ConvexHull(points.astype(np.float64))
-    return points.astype(np.float32), hull.simplices.astype(np.int32)
+    q = hull_integer_points(points)
+    _, first = np.unique(q, axis=0, return_index=True)
+    first = np.sort(first)
+    hull = ConvexHull(q[first])
+    return np.asarray(points, dtype=np.float32), first[hull.simplices].astype(np.int32)
 
 
 def transform_matrix(n: int, scale: float, center) -> list[list[float]]:
@@ -337,18 +364,8 @@ def stratified_spp(spp: int, dimension: int) -> int:
     return k ** dimension
 
 
-def mixed_batch(count: int = 64, seed: int = 4, points_scale: float = 1.0, screen_scale: float = 1.0,
-                spp=(4, 64), depth=(5, 8), workers: int = 1, select=None) -> list[dict]:
-    """Jobs of the batched mixed-scene workload: dimension uniform in
-    {3, 4, 5}; hull of N points on the unit sphere with N log-uniform in the
-    dimension's range (MIXED_POINTS: 2k-200k, at most 50k in 5-space, where
-    hulls grow fastest); screen edge uniform in MIXED_SCREENS; samples per
-    pixel log-uniform in `spp`; maximum depth uniform in `depth`.  The scale
-    arguments shrink hulls and screens for quick runs.  With `workers` > 1
-    the hulls are computed in that many processes (started with `spawn`, so
-    a process that already uses the GPU can call it); the jobs are the same.
-    `select`: indices of the jobs to build (the others are left out); every
-    job carries "paths", its paths per pass."""
+def _mixed_params(count, seed, points_scale, screen_scale, spp, depth):
+    """((n, points, screen, hull seed), spp, depth, points) of each job of the batch."""
     rng = np.random.default_rng(seed)
     params = []
     for k in range(count):
@@ -361,6 +378,30 @@ def mixed_batch(count: int = 64, seed: int = 4, points_scale: float = 1.0, scree
         job_spp = int(round(math.exp(rng.uniform(math.log(spp[0]), math.log(spp[1])))))
         job_depth = int(rng.integers(depth[0], depth[1] + 1))
         params.append(((n, points, [edge] * (n - 1), seed * 1000 + k), job_spp, job_depth, points))
+    return params
+
+
+def mixed_batch_hulls(count: int = 64, seed: int = 4, points_scale: float = 1.0) -> list[tuple[int, int, int, int]]:
+    """(job index, dimension, points, point seed) of every job's hull in the
+    mixed batch, without building it: the hull is of
+    sphere_points(dimension, points, point seed)."""
+    params = _mixed_params(count, seed, points_scale, 1.0, (4, 64), (5, 8))
+    return [(k, p[0][0], p[0][1], p[0][3]) for k, p in enumerate(params)]
+
+
+def mixed_batch(count: int = 64, seed: int = 4, points_scale: float = 1.0, screen_scale: float = 1.0,
+                spp=(4, 64), depth=(5, 8), workers: int = 1, select=None) -> list[dict]:
+    """Jobs of the batched mixed-scene workload: dimension uniform in
+    {3, 4, 5}; hull of N points on the unit sphere with N log-uniform in the
+    dimension's range (MIXED_POINTS: 2k-200k, at most 50k in 5-space, where
+    hulls grow fastest); screen edge uniform in MIXED_SCREENS; samples per
+    pixel log-uniform in `spp`; maximum depth uniform in `depth`.  The scale
+    arguments shrink hulls and screens for quick runs.  With `workers` > 1
+    the hulls are computed in that many processes (started with `spawn`, so
+    a process that already uses the GPU can call it); the jobs are the same.
+    `select`: indices of the jobs to build (the others are left out); every
+    job carries "paths", its paths per pass."""
+    params = _mixed_params(count, seed, points_scale, screen_scale, spp, depth)
     chosen = list(range(count)) if select is None else sorted(set(select))
     params = [params[i] for i in chosen]
     count = len(params)

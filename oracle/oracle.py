@@ -399,3 +399,41 @@ def mesh_file_arrays(path, n: int) -> dict:
         ptr(out["facet_vertices"], _I), ptr(out["facet_normals"], _I), ptr(out["has_normal"], _B),
         ptr(out["facet_material"], _I)))
     return out
+
+
+# ---------------------------------------------------------------------------
+# the reference's convex hull (oracle/_ref/libnbpt_hull.so, `make -C oracle
+# hull`): 3- and 4-space, whose exact integer arithmetic fits 128 bits
+
+HULL_PATH = HERE / "_ref" / "libnbpt_hull.so"
+_hull = None
+
+
+def hull_available() -> bool:
+    return HULL_PATH.exists()
+
+
+def convex_hull(points: np.ndarray) -> np.ndarray:
+    """Facets [F][n] (vertex indices) of the reference's
+    compute_convex_hull (src/geometry/core/convex_hull.h:95-98) of float
+    points [count][n], n = 3 or 4."""
+    global _hull
+    if _hull is None:
+        if not HULL_PATH.exists():
+            raise FileNotFoundError(f"hull library not built: {HULL_PATH} (run make -C oracle hull)")
+        L = ctypes.CDLL(str(HULL_PATH))
+        L.oracle_convex_hull.restype = ctypes.c_longlong
+        L.oracle_convex_hull.argtypes = [ctypes.c_int, _F, ctypes.c_longlong, _I, ctypes.c_longlong]
+        L.oracle_hull_error.restype = ctypes.c_char_p
+        _hull = L
+    p = np.ascontiguousarray(points, dtype=np.float32)
+    count, n = p.shape
+    cap = 16 * count + 64
+    out = np.zeros((cap, n), np.int32)
+    f = _hull.oracle_convex_hull(n, ptr(p, _F), count, ptr(out, _I), cap)
+    if f < 0:
+        raise OracleError(_hull.oracle_hull_error().decode())
+    if f > cap:
+        out = np.zeros((f, n), np.int32)
+        f = _hull.oracle_convex_hull(n, ptr(p, _F), count, ptr(out, _I), f)
+    return out[:f]

@@ -1,9 +1,10 @@
 /*
  * Declaration-only stand-in for <gmp.h>, used only to compile the reference
- * painter as a CPU test oracle.  The painter's render path never performs
- * multi-precision arithmetic (only the n-D convex-hull generator does, and that
- * is not compiled into the oracle), so nothing here has a definition: any
- * accidental use fails at link time instead of computing a wrong value.
+ * painter and its convex hull as CPU test oracles.  The painter's render path
+ * never performs multi-precision arithmetic, and the hull is built for 3- and
+ * 4-space only, whose exact arithmetic fits 128-bit integers, so nothing here
+ * has a definition: any accidental use fails at link time instead of
+ * computing a wrong value.
  */
 #pragma once
 #include <cstddef>
@@ -17,6 +18,24 @@ struct nbpt_oracle_mpz_struct
 typedef nbpt_oracle_mpz_struct mpz_t[1];
 typedef nbpt_oracle_mpz_struct* mpz_ptr;
 typedef const nbpt_oracle_mpz_struct* mpz_srcptr;
+
+struct nbpt_oracle_mpf_struct
+{
+        int prec;
+        int size;
+        long exp;
+        void* data;
+};
+typedef nbpt_oracle_mpf_struct mpf_t[1];
+typedef nbpt_oracle_mpf_struct* mpf_ptr;
+typedef const nbpt_oracle_mpf_struct* mpf_srcptr;
+
+int mpz_sgn(mpz_srcptr);
+void mpz_gcd(mpz_ptr, mpz_srcptr, mpz_srcptr);
+void mpz_divexact(mpz_ptr, mpz_srcptr, mpz_srcptr);
+void mpz_addmul(mpz_ptr, mpz_srcptr, mpz_srcptr);
+void mpf_sqrt(mpf_ptr, mpf_srcptr);
+void mpf_set_z(mpf_ptr, mpz_srcptr);
 
 void mpz_import(mpz_ptr, std::size_t, int, std::size_t, int, std::size_t, const void*);
 void mpz_neg(mpz_ptr, mpz_srcptr);

@@ -21,6 +21,22 @@ public:
         mpz_srcptr get_mpz_t() const;
 };
 
+bool operator==(const mpz_class&, long);
+bool operator!=(const mpz_class&, long);
+bool operator<(const mpz_class&, long);
+bool operator<=(const mpz_class&, long);
+bool operator>(const mpz_class&, long);
+bool operator>=(const mpz_class&, long);
+
+class mpq_class
+{
+        mpz_t num_;
+        mpz_t den_;
+
+public:
+        mpq_class();
+};
+
 class mpf_class
 {
         double value_;
@@ -28,4 +44,10 @@ class mpf_class
 public:
         mpf_class();
         mpf_class(double);
+        mpf_class(double, unsigned long);
+        mpf_class& operator=(const mpz_class&);
+        mpf_class& operator/=(const mpf_class&);
+        mpf_ptr get_mpf_t();
+        mpf_srcptr get_mpf_t() const;
+        double get_d() const;
 };

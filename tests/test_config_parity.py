@@ -2,7 +2,7 @@
 
 1. Closest hits in FP64 on the full meshes (the 4-space Cornell box's hull of
    20,000 points on S^3, about 135k facets, and the 4-space hull of 150,000
-   noisy points, about 1M facets), against the reference's scene and mesh
+   noisy points, 321,175 facets), against the reference's scene and mesh
    queries (the oracle) on a seeded ray set: camera rays of the projector and
    rays from random points of the scene's box in random directions, as in
    src/painter/shapes/test/spherical_mesh.h:192-240.  Bit-exact.
@@ -114,7 +114,7 @@ CONFIGS = {
     # and at the second measurement)
     "C1 3-space Cornell, 256^2, 16 spp, depth 5, RGB": (lambda: scenes.cornell_3d(), False, 16, 5, (2, 8)),
     "C2 4-space Cornell, 64^3, 16 (27) spp, depth 6, spectrum": (lambda: scenes.cornell_4d(), True, 16, 6, (2, 16)),
-    "C3 4-space 1M facets, 96^3, 8 spp, depth 8, RGB": (lambda: scenes.sphere_4d(), False, 8, 8, (2, 40)),
+    "C3 4-space 321k-facet hull, 96^3, 8 spp, depth 8, RGB": (lambda: scenes.sphere_4d(), False, 8, 8, (2, 40)),
 }
 
 
