@@ -241,6 +241,11 @@ typedef struct nbpt_painter_options
         int slab_begin;
         int slab_end;
         int pixel_sums; /* NBPT_PIXEL_SUMS_* */
+        /* device bytes of the per-chunk path buffers (0: a fifth of the
+         * device's memory within [4, 32] GiB); a pass runs its paths in
+         * chunks of as many as they hold, with the same images whatever the
+         * size */
+        long long chunk_budget;
 } nbpt_painter_options;
 nbpt_painter* nbpt_painter_create_options(nbpt_scene* scene, const nbpt_painter_options* options);
 void nbpt_painter_destroy(nbpt_painter* painter);
@@ -253,6 +258,19 @@ void nbpt_painter_destroy(nbpt_painter* painter);
  * counts from 1 (Notifier::pass_done, Notifier::images) */
 typedef void (*nbpt_pass_callback)(void* user, long long pass, const float* rgb, const float* rgba,
                                    long long pixel_count);
+/* Progress within a pass, the GPU's counterpart of the reference's per-pixel
+ * notifications (Notifier::pixel_set and thread_busy / thread_free,
+ * src/painter/pixels/pixels.cpp:95, painting/thread_notifier.h:27-50): a
+ * pass traces its paths in chunks of pixels and calls this after each chunk
+ * with the pixels traced so far (the pixel estimate of a pass is formed
+ * after all its chunks, so no pixel value changes before the pass's images).
+ * `pass` counts from 1; `pixels` is the pixels whose paths the pass renders.
+ * It runs on a CUDA host-callback thread: it must return quickly and call no
+ * CUDA function. */
+typedef void (*nbpt_progress_callback)(void* user, long long pass, long long pixels_done, long long pixels);
+/* sets (or, with NULL, removes) the painter's progress callback for the
+ * passes enqueued from now on, with nbpt_painter_enqueue or on the worker */
+int nbpt_painter_set_progress(nbpt_painter* painter, nbpt_progress_callback on_chunk, void* user);
 /* called on the worker thread when a pass fails (Notifier::error_message);
  * the worker then ends */
 typedef void (*nbpt_error_callback)(void* user, const char* message);

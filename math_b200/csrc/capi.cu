@@ -657,11 +657,16 @@ nbpt_painter* nbpt_painter_create_options(nbpt_scene* scene, const nbpt_painter_
                         {
                                 throw std::runtime_error("Unknown integrator " + std::to_string(o.integrator));
                         }
+                        if (o.chunk_budget < 0)
+                        {
+                                throw std::runtime_error("chunk budget " + std::to_string(o.chunk_budget) +
+                                                         " is negative");
+                        }
                         auto p = std::make_unique<nbpt_painter>();
                         p->impl = scene_of(scene).create_painter(o.samples_per_pixel, o.max_depth, o.seed,
                                                                  static_cast<nbpt::Integrator>(o.integrator),
-                                                                 o.slab_begin, o.slab_end, o.flat_shading != 0, 0,
-                                                                 o.pixel_sums);
+                                                                 o.slab_begin, o.slab_end, o.flat_shading != 0,
+                                                                 o.chunk_budget, o.pixel_sums);
                         out = p.release();
                         return 0;
                 });
@@ -839,6 +844,16 @@ void* nbpt_painter_stream(nbpt_painter* painter)
                         return 0;
                 });
         return s;
+}
+
+int nbpt_painter_set_progress(nbpt_painter* painter, const nbpt_progress_callback on_chunk, void* const user)
+{
+        return guarded(
+                [&]
+                {
+                        painter_of(painter).set_progress(on_chunk, user);
+                        return 0;
+                });
 }
 
 int nbpt_painter_cancel(nbpt_painter* painter)

@@ -66,6 +66,13 @@ public:
         // returns their bytes; the next enqueue_passes allocates them again.
         // Images, samples and statistics stay.
         virtual long long release_scratch() = 0;
+        // Progress within a pass: after the paths of each chunk of pixels are
+        // traced, `callback(user, pass, pixels_done, pixels)` runs on a CUDA
+        // host-callback thread (pass counted from 1; pixels: the pixels whose
+        // paths the pass renders).  It must return quickly and call no CUDA
+        // function.  nullptr: none.  Applies to the passes enqueued after it.
+        using ProgressCallback = void (*)(void* user, long long pass, long long pixels_done, long long pixels);
+        virtual void set_progress(ProgressCallback callback, void* user) = 0;
 };
 
 class Scene

@@ -31,6 +31,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstring>
+#include <deque>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -2446,6 +2447,47 @@ class PainterT final : public Painter
         DeviceArray<float> lum_;
         DeviceArray<unsigned char> valid_;
         bool double_sums_ = false;
+        // set_progress: the callback and one note per chunk enqueued since
+        // the last wait (a deque: host callbacks hold pointers to its notes)
+        struct ProgressNote
+        {
+                ProgressCallback callback;
+                void* user;
+                long long pass;
+                long long done;
+                long long total;
+                std::atomic<long long>* completed;
+        };
+        ProgressCallback progress_ = nullptr;
+        void* progress_user_ = nullptr;
+        std::deque<ProgressNote> progress_notes_;
+        std::atomic<long long> progress_completed_{0}; // notes whose callback has run, in stream order
+        long long progress_dropped_ = 0;              // notes removed from the front of the deque
+
+        static void CUDART_CB progress_host(void* data)
+        {
+                const ProgressNote* const n = static_cast<const ProgressNote*>(data);
+                n->callback(n->user, n->pass, n->done, n->total);
+                n->completed->fetch_add(1, std::memory_order_release);
+        }
+
+        void note_progress(const std::uint32_t pass, const long long end)
+        {
+                if (!progress_)
+                {
+                        return;
+                }
+                // the notes of callbacks that have run are no longer referenced
+                const long long completed = progress_completed_.load(std::memory_order_acquire);
+                while (!progress_notes_.empty() && progress_dropped_ < completed)
+                {
+                        progress_notes_.pop_front();
+                        ++progress_dropped_;
+                }
+                progress_notes_.push_back({progress_, progress_user_, static_cast<long long>(pass) + 1,
+                                           end - source_first_, sources_, &progress_completed_});
+                NBPT_CUDA(cudaLaunchHostFunc(stream_, &progress_host, &progress_notes_.back()));
+        }
         DeviceArray<PixelState<C, float>> state_;    // float sums
         DeviceArray<PixelState<C, double>> state64_; // double sums
         DeviceArray<PathStats> stats_;
@@ -2820,6 +2862,7 @@ public:
                                                         scene_->cie() + 64, cancel_.get());
                                         NBPT_CUDA(cudaGetLastError());
                                         launches += 1;
+                                        note_progress(pass, e);
                                 }
                         }
                         else
@@ -2864,6 +2907,7 @@ public:
                                                 scene_->cie() + 64, stats_.get(), cancel_.get());
                                         NBPT_CUDA(cudaGetLastError());
                                         launches += 4;
+                                        note_progress(pass, e);
                                 }
                         }
                         NBPT_CUDA(cudaEventRecord(ev_paths_end_, stream_));
@@ -2893,9 +2937,18 @@ public:
                 passes_done_ += passes;
         }
 
+        void set_progress(const ProgressCallback callback, void* const user) override
+        {
+                progress_ = callback;
+                progress_user_ = user;
+        }
+
         void wait() override
         {
                 NBPT_CUDA(cudaStreamSynchronize(stream_));
+                // every host callback has run
+                progress_dropped_ += static_cast<long long>(progress_notes_.size());
+                progress_notes_.clear();
                 if (cancelled_)
                 {
                         throw std::runtime_error("cancelled: the pass in flight ended early and its image is incomplete");

@@ -58,6 +58,7 @@ class PainterOptions(ctypes.Structure):
         ("slab_begin", ctypes.c_int),
         ("slab_end", ctypes.c_int),
         ("pixel_sums", ctypes.c_int),
+        ("chunk_budget", ctypes.c_longlong),
     ]
 
 
@@ -124,6 +125,7 @@ SIGNATURES = [
     ("nbpt_painter_statistics", ctypes.c_int, [_P, ctypes.POINTER(Statistics)]),
     ("nbpt_painter_stream", _P, [_P]),
     ("nbpt_painter_cancel", ctypes.c_int, [_P]),
+    ("nbpt_painter_set_progress", ctypes.c_int, [_P, ctypes.c_void_p, _P]),
     ("nbpt_server_create", _P, [ctypes.c_int, ctypes.c_longlong]),
     ("nbpt_server_destroy", None, [_P]),
     ("nbpt_server_submit", ctypes.c_longlong, [_P, _P, ctypes.c_int]),
@@ -320,11 +322,13 @@ class Scene:
 
     def painter(self, samples_per_pixel: int, max_depth: int, seed: int = 1,
                 integrator: str = "bpt", slab: tuple[int, int] | None = None,
-                flat_shading: bool = False, pixel_sums: str | None = None) -> "Painter":
+                flat_shading: bool = False, pixel_sums: str | None = None, chunk_budget: int = 0) -> "Painter":
         """slab: rows [begin, end) of the last screen axis (nbpt_painter_create_slab);
         flat_shading: create_painter's flat_shading; pixel_sums: "float",
-        "double" or None (float for a double-precision scene, else double)"""
-        return Painter(self, samples_per_pixel, max_depth, seed, integrator, slab, flat_shading, pixel_sums)
+        "double" or None (float for a double-precision scene, else double);
+        chunk_budget: bytes of per-chunk path buffers (0: the default)"""
+        return Painter(self, samples_per_pixel, max_depth, seed, integrator, slab, flat_shading, pixel_sums,
+                       chunk_budget)
 
     def trace(self, rays: np.ndarray, any_hit: bool = False):
         rays = _d(rays).reshape(-1, 2 * self.n)
@@ -390,6 +394,7 @@ PIXEL_SUMS = {None: 0, "float": 1, "double": 2}
 PASS_CALLBACK = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_float),
                                  ctypes.POINTER(ctypes.c_float), ctypes.c_longlong)
 ERROR_CALLBACK = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_char_p)
+PROGRESS_CALLBACK = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong)
 
 
 class Painter:
@@ -399,7 +404,7 @@ class Painter:
 
     def __init__(self, scene: Scene, samples_per_pixel: int, max_depth: int, seed: int = 1,
                  integrator: str = "bpt", slab: tuple[int, int] | None = None, flat_shading: bool = False,
-                 pixel_sums: str | None = None):
+                 pixel_sums: str | None = None, chunk_budget: int = 0):
         if integrator not in INTEGRATORS:
             raise PainterError(f"Unknown integrator {integrator!r}")
         if pixel_sums not in PIXEL_SUMS:
@@ -409,7 +414,7 @@ class Painter:
         self.spp = scene.actual_spp(samples_per_pixel)
         begin, end = slab if slab is not None else (0, -1)
         options = PainterOptions(INTEGRATORS[integrator], samples_per_pixel, max_depth, seed,
-                                 1 if flat_shading else 0, begin, end, PIXEL_SUMS[pixel_sums])
+                                 1 if flat_shading else 0, begin, end, PIXEL_SUMS[pixel_sums], int(chunk_budget))
         self.h = lib().nbpt_painter_create_options(scene.h, ctypes.byref(options))
         if not self.h:
             raise PainterError(lib().nbpt_last_error().decode())
@@ -460,6 +465,18 @@ class Painter:
 
     def cancel(self):
         _check(lib().nbpt_painter_cancel(self.h))
+
+    def set_progress(self, fn):
+        """fn(pass, pixels_done, pixels) after each chunk of a pass's paths
+        (nbpt_painter_set_progress; it runs on a CUDA host-callback thread);
+        None removes it."""
+        if fn is None:
+            _check(lib().nbpt_painter_set_progress(self.h, None, None))
+            self._progress = None
+            return
+        cb = PROGRESS_CALLBACK(lambda user, p, done, total: fn(int(p), int(done), int(total)))
+        _check(lib().nbpt_painter_set_progress(self.h, ctypes.cast(cb, ctypes.c_void_p), None))
+        self._progress = cb
 
     def __del__(self):
         self.close()
