@@ -128,7 +128,7 @@ def convex_hull_mesh(points: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
     finds the same facets: a double-precision hull of the unrounded points
     differs from it by a few facets wherever nearly coplanar points are
     split the other way by the rounding (tests/test_hull.py checks the
-    3- and 4-space hulls against the reference's own).  Facet vertices are
+    3-, 4- and 5-space benchmark hulls against the reference's own).  Facet vertices are
     indices into `points`; the vertex order inside a facet does not matter
     to the painter, which orients normals towards the ray."""
     from scipy.spatial import ConvexHull

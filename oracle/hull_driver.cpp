@@ -44,7 +44,7 @@ long long hull(const float* points, const long long count, int* facets, const lo
 }
 
 extern "C" {
-// facets of the hull of count points [count][n] (n = 3 or 4): returns the
+// facets of the hull of count points [count][n] (n = 3, 4 or 5): returns the
 // facet count (facets written when it is at most capacity), -1 on error
 long long oracle_convex_hull(const int n, const float* points, const long long count, int* facets,
                              const long long capacity)
@@ -59,7 +59,11 @@ long long oracle_convex_hull(const int n, const float* points, const long long c
                 {
                         return hull<4>(points, count, facets, capacity);
                 }
-                g_error = "convex hull: dimension " + std::to_string(n) + " is not built (3 and 4 only)";
+                if (n == 5)
+                {
+                        return hull<5>(points, count, facets, capacity);
+                }
+                g_error = "convex hull: dimension " + std::to_string(n) + " is not built (3, 4 and 5 only)";
         }
         catch (const std::exception& e)
         {

@@ -403,7 +403,7 @@ def mesh_file_arrays(path, n: int) -> dict:
 
 # ---------------------------------------------------------------------------
 # the reference's convex hull (oracle/_ref/libnbpt_hull.so, `make -C oracle
-# hull`): 3- and 4-space, whose exact integer arithmetic fits 128 bits
+# hull`): 3-, 4- and 5-space (5-space with GMP integers)
 
 HULL_PATH = HERE / "_ref" / "libnbpt_hull.so"
 _hull = None
@@ -416,7 +416,7 @@ def hull_available() -> bool:
 def convex_hull(points: np.ndarray) -> np.ndarray:
     """Facets [F][n] (vertex indices) of the reference's
     compute_convex_hull (src/geometry/core/convex_hull.h:95-98) of float
-    points [count][n], n = 3 or 4."""
+    points [count][n], n = 3, 4 or 5."""
     global _hull
     if _hull is None:
         if not HULL_PATH.exists():

@@ -1,10 +1,10 @@
 /*
  * Declaration-only stand-in for <gmp.h>, used only to compile the reference
- * painter and its convex hull as CPU test oracles.  The painter's render path
- * never performs multi-precision arithmetic, and the hull is built for 3- and
- * 4-space only, whose exact arithmetic fits 128-bit integers, so nothing here
- * has a definition: any accidental use fails at link time instead of
- * computing a wrong value.
+ * painter as a CPU test oracle.  The painter's render path never performs
+ * multi-precision arithmetic (the reference's convex hull does, and the
+ * oracle's hull library takes hull_gmp/ and the system's libgmp instead), so
+ * nothing here has a definition: any accidental use fails at link time
+ * instead of computing a wrong value.
  */
 #pragma once
 #include <cstddef>
