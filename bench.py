@@ -11,8 +11,9 @@ convex hull of N points on the unit (n-1)-sphere (N log-uniform in
 
 One step is one wave, a quarter of the batch's jobs (about 192 M of its
 770 M paths), one pass each through the job server in FP32; the steps are
-submitted back to back (continuous batching).  Before the warm-up the
-server's chunk budget is chosen by measurement (math_b200.tuning).  `value`
+submitted back to back (continuous batching).  With `--tune` the
+server's chunk budget is chosen by measurement before the warm-up
+(math_b200.tuning).  `value`
 is paths/s over the timed steps on the device (CUDA events on the jobs'
 streams, first kernel to last, L2 flushed before them); `plain_fp64` the
 same jobs in FP64 one at a time;
@@ -91,9 +92,10 @@ def parse():
     p.add_argument("--max-jobs", type=int, default=16, help="batch/serve: jobs the server runs at once")
     p.add_argument("--waves", type=int, default=4,
                    help="batch: the batch is split into this many waves of about equal paths; a step is one wave")
-    p.add_argument("--no-tune", action="store_true",
-                   help="batch: keep the server's default chunk budget instead of choosing it by measurement "
-                        "(math_b200.tuning, one batch per candidate, before the warm-up)")
+    p.add_argument("--tune", action="store_true",
+                   help="batch: choose the server's chunk budget by measurement (math_b200.tuning, one batch per "
+                        "candidate, before the warm-up) instead of keeping its default; on this batch the "
+                        "candidates differ by less than one batch's run-to-run spread")
     p.add_argument("--e2e-steps", type=int, default=0,
                    help="batch: steps (waves) of the end-to-end measurement (0: one whole batch)")
     p.add_argument("--serve-duration", type=float, default=20.0,
@@ -797,7 +799,7 @@ def run_batch(args, rank: int, world: int, local: int):
     server = P.Server(max_jobs=args.max_jobs)
     try:
         tuning = None
-        if not args.no_tune:
+        if args.tune:
             from math_b200 import tuning as T
 
             def one_batch():
@@ -806,7 +808,10 @@ def run_batch(args, rank: int, world: int, local: int):
 
             # a first batch at the default allocates the scenes' buffers
             one_batch()
-            tuning = T.tune_chunk_budget(server, one_batch, T.chunk_budget_candidates(server))
+            # every candidate starts from an empty buffer cache, and so does
+            # the warm-up after the tuning
+            tuning = T.tune_chunk_budget(server, one_batch, T.chunk_budget_candidates(server),
+                                         reset=P.release_cached_memory)
         server_chunk_budget = server.chunk_budget
         batch_steps(server, wave_scenes, waves, args.warmup, read_images=False)
         flush_l2(flush)

@@ -516,6 +516,11 @@ def painter_stream(p: "Painter") -> int:
     return int(lib().nbpt_painter_stream(p.h) or 0)
 
 
+def release_cached_memory() -> int:
+    """Frees the device buffers the library keeps for reuse (nbpt_release_cached_memory); returns their bytes."""
+    return _check(lib().nbpt_release_cached_memory())
+
+
 def device_count() -> int:
     return lib().nbpt_device_count()
 

@@ -34,16 +34,22 @@ def chunk_budget_candidates(server, factors=(1.0, 1.5, 2.0, 2.75), cap: int = 32
 
 
 def tune_chunk_budget(server, run: Callable[[], tuple[float, float]], candidates: list[int],
-                      log: Callable[[str], None] | None = None) -> dict:
+                      log: Callable[[str], None] | None = None, reset: Callable[[], object] | None = None) -> dict:
     """For each candidate (bytes): set it as the server's chunk budget, call
     `run()`, which renders a representative slice of the workload through the
     server and returns (paths, device seconds), and record paths/s.  The
-    fastest candidate is left set.  Returns {"chosen": bytes, "trials":
-    [{"chunk_budget": bytes, "paths_per_s": r, "wall_s": w}, ...]}."""
+    fastest candidate is left set.  `reset`, called before every trial and
+    once more at the end, puts shared state back (the library's cache of
+    device buffers, whose sizes follow the chunk budget: a cache filled by one
+    candidate would slow the next, and the run after the tuning).  Returns
+    {"chosen": bytes, "trials": [{"chunk_budget": bytes, "paths_per_s": r,
+    "wall_s": w}, ...]}."""
     if not candidates:
         raise ValueError("no candidate chunk budgets")
     trials = []
     for b in candidates:
+        if reset:
+            reset()
         server.set_chunk_budget(b)
         t0 = time.perf_counter()
         paths, seconds = run()
@@ -54,4 +60,6 @@ def tune_chunk_budget(server, run: Callable[[], tuple[float, float]], candidates
             log(f"chunk budget {b / GIB:.2f} GiB: {rate / 1e6:.2f} M paths/s")
     best = max(trials, key=lambda t: t["paths_per_s"])
     server.set_chunk_budget(best["chunk_budget"])
+    if reset:
+        reset()
     return {"chosen": best["chunk_budget"], "trials": trials}

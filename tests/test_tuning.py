@@ -42,8 +42,12 @@ def test_the_fastest_candidate_is_kept():
         seen.append(gib)
         return rates[gib] * 10.0, 10.0
 
-    out = T.tune_chunk_budget(s, run, [9 * T.GIB, 16 * T.GIB, 24 * T.GIB], log=lambda m: None)
+    resets = []
+    out = T.tune_chunk_budget(s, run, [9 * T.GIB, 16 * T.GIB, 24 * T.GIB], log=lambda m: None,
+                              reset=lambda: resets.append(s.budget))
     assert seen == [9, 16, 24]
+    # before every trial (with the previous budget still set) and at the end
+    assert len(resets) == 4 and resets[-1] == 16 * T.GIB
     assert out["chosen"] == 16 * T.GIB
     assert s.budget == 16 * T.GIB
     assert [t["paths_per_s"] for t in out["trials"]] == [60.0, 64.0, 58.0]
