@@ -10,13 +10,12 @@ convex hull of N points on the unit (n-1)-sphere (N log-uniform in
 (math_b200/scenes.py).
 
 One step is one wave, a quarter of the batch's jobs (about 192 M of its
-770 M paths), one pass each through the job server in FP32; the steps are
-submitted back to back (continuous batching).  With `--tune` the
-server's chunk budget is chosen by measurement before the warm-up
-(math_b200.tuning).  `value`
-is paths/s over the timed steps on the device (CUDA events on the jobs'
-streams, first kernel to last, L2 flushed before them); `plain_fp64` the
-same jobs in FP64 one at a time;
+770 M paths), one pass each through the job server in FP32, all submitted
+at once.  With `--tune` the server's chunk budget is chosen by measurement
+before the warm-up (math_b200.tuning).  `value` is paths/s over the timed
+steps on the device (CUDA events on the jobs' streams, each step's first
+kernel to its last, L2 flushed between steps); `plain_fp64` the same jobs in
+FP64 one at a time;
 `e2e` the whole batch through the C ABI from host arrays (scene builds,
 copies, images back); `serve` a Poisson stream of renders into the server
 with its p50/p99 latency.  `--impl reference` runs the reference's own CPU
@@ -56,7 +55,7 @@ WORKLOADS = {
                           "parallel projection, RGB"},
     "mixed5d": {"screen": [12, 12, 12, 12], "spp": 16, "max_depth": 8, "spectrum": False, "precision": "float",
                 "label": "a 5-space job of the mixed batch's shape: box, ceiling light, hull of 24000 points on S^4 "
-                         "(739,994 facets), RGB (for kernel profiles)"},
+                         "(739,992 facets), RGB (for kernel profiles)"},
 }
 
 
@@ -813,21 +812,38 @@ def run_batch(args, rank: int, world: int, local: int):
             tuning = T.tune_chunk_budget(server, one_batch, T.chunk_budget_candidates(server),
                                          reset=P.release_cached_memory)
         server_chunk_budget = server.chunk_budget
-        batch_steps(server, wave_scenes, waves, args.warmup, read_images=False)
-        flush_l2(flush)
+        for k in range(args.warmup):
+            flush_l2(flush)
+            w = k % len(waves)
+            batch_step(server, wave_scenes[w], waves[w], read_images=False)
         torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
         clocks = ClockSampler(local)
         clocks.start()
-        totals = batch_steps(server, wave_scenes, waves, args.steps)
+        spans = [[] for _ in waves]
+        totals = {"launches": 0, "bytes": 0.0, "rays": 0, "nodes": 0, "facets": 0, "nonfinite": 0, "paths": 0}
+        images = {}
+        for k in range(args.steps):
+            flush_l2(flush)
+            w = k % len(waves)
+            r = batch_step(server, wave_scenes[w], waves[w])
+            spans[w].append(r["span"])
+            for key in totals:
+                totals[key] += r[key]
+            for j, img in zip(waves[w], r["images"]):
+                images[j["index"]] = img
         clock_info = clocks.stop()
         torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
-        images = totals["images"]
-        step_seconds = float(totals["span"])
-        rank_rate = totals["paths"] / step_seconds
+        step_seconds = float(sum(sum(x) for x in spans))
+        if all(spans):
+            # every wave timed: the batch's rate from each wave's mean span
+            # (the plain sum when the steps cover whole batches)
+            rank_rate = paths_per_batch / sum(float(np.mean(x)) for x in spans)
+        else:
+            rank_rate = totals["paths"] / step_seconds
         # whole batch over the slowest rank: every rank renders its jobs
         batch_seconds = slowest_rank(paths_per_batch / rank_rate, world, "cuda")
         value = sum(all_paths) / batch_seconds
@@ -878,9 +894,8 @@ def run_batch(args, rank: int, world: int, local: int):
                        "waves": len(waves), "wave_paths": wave_paths,
                        "step": (f"one wave: {len(jobs) // len(waves)} of the batch's jobs (the batch split into "
                                 f"{len(waves)} waves of about equal paths), one pass each at its own samples "
-                                "per pixel, images read back; the steps are submitted back to back, all queued in "
-                                "the job server at once (continuous batching: no drain between steps); value = "
-                                "paths of the timed steps / their device span"),
+                                "per pixel, all submitted to the job server at once, images read back; value = "
+                                "paths of the whole batch / the sum of the waves' mean device spans"),
                        "max_jobs": args.max_jobs,
                        "chunk_budget": server_chunk_budget,
                        "tuning": tuning and {
@@ -891,11 +906,9 @@ def run_batch(args, rank: int, world: int, local: int):
                                        "paths_per_s": t["paths_per_s"]} for t in tuning["trials"]]},
                        "points_scale": args.points_scale,
                        "screen_scale": args.screen_scale, "generate_s": generate_s, "scene_build_s": build_s,
-                       "l2": "flushed (256 MiB write) before the timed steps; the steps' scenes (64 meshes of up "
-                             "to 1.5 M facets) and path buffers exceed L2 many times over",
-                       "timing": "device span of the timed steps: CUDA events on the jobs' streams, from the first "
-                                 "kernel of the first step's first job to the last kernel of the last job; "
-                                 "ms_per_step = span / steps"},
+                       "l2": "flushed (256 MiB write) before every step; scenes and buffers exceed L2",
+                       "timing": "device span per step: CUDA events on the jobs' streams, from the first kernel of "
+                                 "the wave's first job to the last kernel of its last job"},
             "plain_fp64": plain,
             "speedup_vs_plain_fp64": (value / plain["value"]) if plain else None,
             "e2e": {"value": e2e_value, "unit": "paths/s",
