@@ -17,6 +17,7 @@
 #include "mesh_files.h"
 #include "device_pool.h"
 #include "estimator.cuh"
+#include "float_paths.h"
 #include "host_math.h"
 #include "kernels.cuh"
 #include "painter_api.h"
@@ -2772,6 +2773,82 @@ public:
                 return stream_;
         }
 
+        // The path kernels of this precision: single precision's come from
+        // their own unit, compiled with multiply-add contraction
+        // (float_paths.h); double precision's are compiled here, without it.
+        static auto walk_kernel()
+        {
+                if constexpr (std::is_same_v<T, float>)
+                {
+                        return float_path_kernels<N>().walk;
+                }
+                else
+                {
+                        return &paths_walk_kernel<N, T>;
+                }
+        }
+        static auto light_kernel()
+        {
+                if constexpr (std::is_same_v<T, float>)
+                {
+                        return float_path_kernels<N>().light;
+                }
+                else
+                {
+                        return &paths_light_kernel<N, T>;
+                }
+        }
+        static auto connect_kernel()
+        {
+                if constexpr (std::is_same_v<T, float>)
+                {
+                        return float_path_kernels<N>().connect;
+                }
+                else
+                {
+                        return &paths_connect_kernel<N, T>;
+                }
+        }
+        static auto replay_kernel()
+        {
+                constexpr int LANES = C % 32 == 0 ? 32 : 1;
+                if constexpr (std::is_same_v<T, float>)
+                {
+                        static_assert(C == 3 || C == 64);
+                        if constexpr (C == 3)
+                        {
+                                return float_path_kernels<N>().replay_rgb;
+                        }
+                        else
+                        {
+                                return float_path_kernels<N>().replay_spectrum;
+                        }
+                }
+                else
+                {
+                        return &paths_replay_kernel<N, T, C, LANES>;
+                }
+        }
+        static auto pt_kernel()
+        {
+                if constexpr (std::is_same_v<T, float>)
+                {
+                        static_assert(C == 3 || C == 64);
+                        if constexpr (C == 3)
+                        {
+                                return float_path_kernels<N>().pt_rgb;
+                        }
+                        else
+                        {
+                                return float_path_kernels<N>().pt_spectrum;
+                        }
+                }
+                else
+                {
+                        return &pt_paths_kernel<N, T, C>;
+                }
+        }
+
         // the per-chunk buffers of the BPT path kernels
         void allocate_scratch()
         {
@@ -2852,7 +2929,7 @@ public:
                                         const long long o = b - source_first_; // the chunk in the sample arrays
                                         const long long n = (e - b) * spp_;
                                         NBPT_CUDA(cudaMemsetAsync(next_path_.get(), 0, sizeof(unsigned), stream_));
-                                        pt_paths_kernel<N, T, C>
+                                        pt_kernel()
                                                 <<<std::min<long long>(connect_blocks_, blocks_for(n, 128)), 128, 0, stream_>>>(
                                                         scene_1, scene_->device_materials(),
                                                         scene_->device_lights(), b, e, spp_, seed_, pass,
@@ -2885,22 +2962,22 @@ public:
                                                 tasks_.get() + n * (tape_slot_count(max_depth_) - max_depth_);
                                         queues.count = task_count_.get();
                                         NBPT_CUDA(cudaMemsetAsync(next_path_.get(), 0, sizeof(unsigned), stream_));
-                                        paths_walk_kernel<N, T><<<std::min<long long>(connect_blocks_, blocks_for(n, 128)), 128, 0,
+                                        walk_kernel()<<<std::min<long long>(connect_blocks_, blocks_for(n, 128)), 128, 0,
                                                                   stream_>>>(
                                                 scene_1, b, e, spp_, max_depth_, seed_, pass, points_.get() + o * spp_ * (N - 1),
                                                 vertices_.get(), rng_.get(), tape_.get(), tape_words_, valid_.get() + o * spp_,
                                                 queues, next_path_.get(), stats_.get(), cancel_.get());
                                         NBPT_CUDA(cudaGetLastError());
-                                        paths_light_kernel<N, T><<<blocks_for(n, 128), 128, 0, stream_>>>(
+                                        light_kernel()<<<blocks_for(n, 128), 128, 0, stream_>>>(
                                                 scene_1, n, max_depth_, vertices_.get(), rng_.get(), tape_.get(), tape_words_,
                                                 arrivals_.get(), queues, cancel_.get());
                                         NBPT_CUDA(cudaGetLastError());
-                                        paths_connect_kernel<N, T><<<connect_blocks_, 128, 0, stream_>>>(
+                                        connect_kernel()<<<connect_blocks_, 128, 0, stream_>>>(
                                                 scene_1, max_depth_, vertices_.get(), tape_.get(), tape_words_, arrivals_.get(),
                                                 queues, stats_.get());
                                         NBPT_CUDA(cudaGetLastError());
                                         constexpr int LANES = C % 32 == 0 ? 32 : 1;
-                                        paths_replay_kernel<N, T, C, LANES><<<blocks_for(n * LANES, 128), 128, 0, stream_>>>(
+                                        replay_kernel()<<<blocks_for(n * LANES, 128), 128, 0, stream_>>>(
                                                 scene_->device_materials(), scene_->device_lights(),
                                                 scene.shading.fresnel_a, scene.shading.fresnel_b, max_depth_, n, tape_.get(),
                                                 tape_words_, colors_.get() + o * spp_ * C, lum_.get() + o * spp_,
