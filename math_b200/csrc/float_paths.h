@@ -1,9 +1,10 @@
 // The single-precision path kernels, compiled in their own unit
-// (painter_paths_f.cu) with multiply-add contraction.  The library's other
-// units compile without it, so that double precision follows the reference's
-// operation order bit for bit; single precision is checked against the
-// reference statistically (relative RMSE, z-tests), and contraction makes its
-// path kernels about 5 % faster.  The painter launches them through these
+// (painter_paths_f.cu) with multiply-add contraction, denormals flushed to
+// zero and approximate division and square root.  The library's other units
+// compile with none of these, so that double precision follows the
+// reference's operation order bit for bit; single precision is checked
+// against the reference statistically (relative RMSE, z-tests), and these
+// options make its path kernels about 15 % faster.  The painter launches them through these
 // pointers, so no other unit instantiates them.
 #pragma once
 

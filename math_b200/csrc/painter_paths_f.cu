@@ -1,5 +1,7 @@
-// Single-precision path kernels with multiply-add contraction (float_paths.h;
-// the Makefile compiles this unit with -fmad=true).
+// Single-precision path kernels with multiply-add contraction, denormals
+// flushed and approximate division and square root (float_paths.h; the
+// Makefile compiles this unit with -fmad=true -ftz=true -prec-div=false
+// -prec-sqrt=false).
 #include "float_paths.h"
 
 namespace nbpt
