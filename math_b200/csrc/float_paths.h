@@ -4,8 +4,8 @@
 // compile with none of these, so that double precision follows the
 // reference's operation order bit for bit; single precision is checked
 // against the reference statistically (relative RMSE, z-tests), and these
-// options make its path kernels about 15 % faster.  The painter launches them through these
-// pointers, so no other unit instantiates them.
+// options make its path kernels about 15 % faster.  The painter launches them
+// through these pointers, so no other unit instantiates them.
 #pragma once
 
 #include "kernels.cuh"
