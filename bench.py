@@ -202,15 +202,14 @@ def cpu_baseline(small: bool, name: str = "cornell4d", precision: str = "float",
     w = WORKLOADS[name]
     desc = scene_desc(small, None, name)
     slab = desc["projector"]["size"]
-    s = oracle.Scene(desc, precision, w["spectrum"])
-    s.set_integrator(integrator)
     cores = os.cpu_count() or 1
-    stats, _ = s.paint(w["spp"], w["max_depth"], passes=1, threads=cores)
-    value = stats["sample_count"] / stats["pass_duration"]
+    # in a watchdog child: the reference painter can stall at the end of a pass
+    (paths, seconds), = reference_job_passes(desc, w["spp"], w["max_depth"], 1, cores, precision=precision,
+                                             spectrum=w["spectrum"], integrator=integrator)[0]
+    value = paths / seconds
     return {"value": value, "unit": "paths/s", "cores": cores, "kind": "reference",
             "sample": (f"one pass of the reference painter over the whole {'x'.join(map(str, slab))} screen "
-                       f"({stats['sample_count']} paths, {stats['pass_duration']:.2f} s, "
-                       f"ray_count {stats['ray_count']})")}
+                       f"({paths} paths, {seconds:.2f} s)")}
 
 
 # DRAM bytes (read + write) per path of the path kernels (walk, connect,
@@ -239,17 +238,15 @@ def run_reference(args, rank: int):
     w = workload_of(args)
     desc = scene_desc(args.small, args.screen, args.workload if args.workload in WORKLOADS else "cornell4d")
     slab = desc["projector"]["size"]
-    s = oracle.Scene(desc, args.precision, w["spectrum"])
-    s.set_integrator(args.integrator)
     cores = os.cpu_count() or 1
-    for _ in range(args.warmup):
-        s.paint(w["spp"], w["max_depth"], passes=1, threads=cores)
-    samples = 0
-    seconds = 0.0
-    for _ in range(args.steps):
-        st, _ = s.paint(w["spp"], w["max_depth"], passes=1, threads=cores)
-        samples += st["sample_count"]
-        seconds += st["pass_duration"]
+    # warm-up and timed passes in a watchdog child: the reference painter can
+    # stall at the end of a pass (reference_job_passes)
+    passes, _ = reference_job_passes(desc, w["spp"], w["max_depth"], args.warmup + args.steps, cores,
+                                     precision=args.precision, spectrum=w["spectrum"],
+                                     integrator=args.integrator)
+    timed = passes[args.warmup:]
+    samples = sum(p for p, _ in timed)
+    seconds = sum(t for _, t in timed)
     value = samples / seconds
     sample = f"{args.steps} passes over the whole {'x'.join(map(str, slab))} screen"
     print(json.dumps({
@@ -512,12 +509,15 @@ def sample_desc(desc: dict, spp_actual: int, target: int) -> dict:
     return d
 
 
-def _reference_job_worker(conn, desc: dict, spp: int, depth: int, passes: int, threads: int):
+def _reference_job_worker(conn, desc: dict, spp: int, depth: int, passes: int, threads: int,
+                          precision: str = "float", spectrum: bool = False, integrator: str = "bpt"):
     """Child process: the reference painter's scene once, then `passes`
     one-pass paints, each pass's (paths, seconds) sent as it ends."""
     from oracle import oracle
 
-    s = oracle.Scene(desc, "float", False)
+    s = oracle.Scene(desc, precision, spectrum)
+    if integrator != "bpt":
+        s.set_integrator(integrator)
     conn.send(("built", None))
     for _ in range(passes):
         st, _ = s.paint(spp, depth, passes=1, threads=threads)
@@ -526,7 +526,8 @@ def _reference_job_worker(conn, desc: dict, spp: int, depth: int, passes: int, t
 
 
 def reference_job_passes(desc: dict, spp: int, depth: int, passes: int, threads: int,
-                         limit: float = 60.0) -> tuple[list, int]:
+                         limit: float = 60.0, precision: str = "float", spectrum: bool = False,
+                         integrator: str = "bpt") -> tuple[list, int]:
     """`passes` passes of the reference painter on one scene, in a child
     process.  The reference's painter can stop for good at the end of a
     pass: the thread that ends the last pass sets the stop flag
@@ -544,7 +545,8 @@ def reference_job_passes(desc: dict, spp: int, depth: int, passes: int, threads:
     hangs = 0
     while len(out) < passes:
         a, b = ctx.Pipe(duplex=False)
-        p = ctx.Process(target=_reference_job_worker, args=(b, desc, spp, depth, passes - len(out), threads),
+        p = ctx.Process(target=_reference_job_worker,
+                        args=(b, desc, spp, depth, passes - len(out), threads, precision, spectrum, integrator),
                         daemon=True)
         p.start()
         b.close()
